@@ -1,0 +1,305 @@
+"""ctypes front end for the oracle libraries (test infrastructure only).
+
+Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline / reference legs use
+this module. It loads
+  _lib/libnwg_oracle.so  (CPU restatement),
+  _lib/libnwg_tape.so    (GPU draw tapes),
+  _ref/libref_host.so    (reference host code, CPU),
+  _ref/libref_dev.so     (reference device code, GPU).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from functools import lru_cache
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+POLICY_HALFS = 150528
+TAIL_DIM = 38
+
+_u8p = C.POINTER(C.c_uint8)
+_u16p = C.POINTER(C.c_uint16)
+_u32p = C.POINTER(C.c_uint32)
+_i32p = C.POINTER(C.c_int32)
+_f32p = C.POINTER(C.c_float)
+_u64p = C.POINTER(C.c_uint64)
+_sz = C.c_size_t
+
+
+def _ptr(a: np.ndarray | None, t):
+    if a is None:
+        return C.cast(None, t)
+    assert a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(t)
+
+
+def genome_halfs(action_count: int) -> int:
+    return POLICY_HALFS + TAIL_DIM * action_count
+
+
+def stride_bytes(action_count: int) -> int:
+    return 2 * genome_halfs(action_count) if action_count else 0
+
+
+class ShardRecord(C.Structure):
+    """TrainingDataShardRuntime (training_folder/training_data.hpp:35-42), 48 bytes."""
+
+    _fields_ = [
+        ("first_catalog_word_index", C.c_uint64),
+        ("word_count", C.c_uint64),
+        ("center_row", C.c_uint64),
+        ("center_column", C.c_uint64),
+        ("radius", C.c_uint64),
+        ("global_from_outset", C.c_uint8),
+    ]
+
+
+assert C.sizeof(ShardRecord) == 48
+
+
+class DrawTape(C.Structure):
+    _fields_ = [
+        ("raw", _u32p),
+        ("uniform", _f32p),
+        ("normal_pair", _f32p),
+        ("length", _sz),
+        ("position", _sz),
+        ("has_cached_normal", C.c_int),
+        ("cached_normal", C.c_float),
+        ("overflow", C.c_int),
+    ]
+
+
+class BreedConfig(C.Structure):
+    _fields_ = [
+        ("crossover_l1", C.c_float),
+        ("crossover_l2", C.c_float),
+        ("crossover_l3", C.c_float),
+        ("mutation_probability", C.c_float),
+        ("mutation_sigma", C.c_float),
+        ("row_scale_probability", C.c_float),
+    ]
+
+
+@lru_cache(None)
+def lib() -> C.CDLL:
+    path = HERE / "_lib" / "libnwg_oracle.so"
+    if not path.exists():
+        from oracle import build
+
+        build.build_oracle()
+    L = C.CDLL(str(path))
+    L.nwo_genome_stride_bytes.restype = _sz
+    L.nwo_genome_stride_bytes.argtypes = [_sz]
+    L.nwo_set_fma_mode.argtypes = [C.c_int]
+    L.nwo_feedback.argtypes = [_u8p, _u8p, _u8p]
+    L.nwo_encode_turn.argtypes = [_u16p, _u8p, _u8p, _f32p]
+    L.nwo_policy_forward.argtypes = [_u16p, _sz, _u8p, _u8p, C.c_int, _f32p]
+    L.nwo_score_action.restype = C.c_float
+    L.nwo_score_action.argtypes = [_f32p, _u8p, _u16p]
+    L.nwo_evaluate_individual.argtypes = [_u16p, _sz, _u8p, _sz, _u32p, _sz, _f32p, _u64p, _f32p, _i32p, _i32p,
+                                          _f32p]
+    L.nwo_normalize_fitness.restype = C.c_float
+    L.nwo_normalize_fitness.argtypes = [C.c_float, _sz]
+    L.nwo_cell_words_from_shards.restype = _sz
+    L.nwo_cell_words_from_shards.argtypes = [C.POINTER(ShardRecord), _sz, _sz, _sz, _sz, _u32p, _sz]
+    L.nwo_select_parent_pair.argtypes = [_f32p, _u8p, _sz, _sz, _sz, _sz, _sz, _u32p, _f32p, _sz, _u32p, _u32p]
+    L.nwo_breed_and_mutate.argtypes = [_u16p, _u16p, _sz, _u16p, C.POINTER(DrawTape), C.POINTER(BreedConfig)]
+    L.nwo_bootstrap_genome.argtypes = [_u16p, _sz, _f32p, _sz]
+    L.nwo_bootstrap_normals_per_thread.restype = _sz
+    L.nwo_bootstrap_normals_per_thread.argtypes = [_sz, _sz]
+    L.nwo_summarize.argtypes = [_f32p, _sz, _f32p, _f32p, C.POINTER(_sz)]
+    return L
+
+
+def set_fma_mode(on: bool) -> None:
+    lib().nwo_set_fma_mode(1 if on else 0)
+
+
+def word(s: str) -> np.ndarray:
+    return np.frombuffer(s.upper().encode(), dtype=np.uint8) - ord("A")
+
+
+def words_to_letters(words: list[str]) -> np.ndarray:
+    return np.ascontiguousarray(np.stack([word(w) for w in words]).astype(np.uint8))
+
+
+def feedback(guess: np.ndarray, solution: np.ndarray) -> np.ndarray | None:
+    out = np.zeros(5, np.uint8)
+    ok = lib().nwo_feedback(_ptr(np.ascontiguousarray(guess, np.uint8), _u8p),
+                            _ptr(np.ascontiguousarray(solution, np.uint8), _u8p), _ptr(out, _u8p))
+    return out if ok else None
+
+
+def encode_turn(genome: np.ndarray, guess: np.ndarray, fb: np.ndarray) -> np.ndarray:
+    out = np.zeros(64, np.float32)
+    lib().nwo_encode_turn(_ptr(genome, _u16p), _ptr(np.ascontiguousarray(guess, np.uint8), _u8p),
+                          _ptr(np.ascontiguousarray(fb, np.uint8), _u8p), _ptr(out, _f32p))
+    return out
+
+
+def policy_forward(genome: np.ndarray, solution: np.ndarray, guesses: np.ndarray) -> np.ndarray | None:
+    """Policy vector for the grid with `solution` after `guesses` (rows of 5 letters)."""
+    guesses = np.ascontiguousarray(np.asarray(guesses, np.uint8).reshape(-1, 5))
+    fbs = np.zeros_like(guesses)
+    finished = 0
+    for t in range(len(guesses)):
+        fbs[t] = feedback(guesses[t], solution)
+        if np.array_equal(guesses[t], solution):
+            finished = 1
+    if len(guesses) >= 6:
+        finished = 1
+    out = np.zeros(64, np.float32)
+    ok = lib().nwo_policy_forward(_ptr(genome, _u16p), len(guesses), _ptr(guesses, _u8p), _ptr(fbs, _u8p), finished,
+                                  _ptr(out, _f32p))
+    return out if ok else None
+
+
+def score_action(policy: np.ndarray, w: np.ndarray, tail_row: np.ndarray) -> float:
+    return lib().nwo_score_action(_ptr(np.ascontiguousarray(policy, np.float32), _f32p),
+                                  _ptr(np.ascontiguousarray(w, np.uint8), _u8p),
+                                  _ptr(np.ascontiguousarray(tail_row, np.uint16), _u16p))
+
+
+def evaluate_individual(genome: np.ndarray, action_count: int, catalog: np.ndarray, cell_words: np.ndarray,
+                        trace_policy: bool = False) -> dict:
+    w = len(cell_words)
+    scores = np.zeros(3 * w, np.float32)
+    turns = np.zeros(3 * w, np.int32)
+    guesses = np.zeros(3 * w * 6, np.int32)
+    policy = np.zeros(3 * w * 6 * 64, np.float32) if trace_policy else None
+    raw = C.c_float()
+    steps = C.c_uint64()
+    cw = np.ascontiguousarray(cell_words, np.uint32)
+    status = lib().nwo_evaluate_individual(_ptr(genome, _u16p), action_count, _ptr(catalog, _u8p), len(catalog),
+                                           _ptr(cw, _u32p), w, C.byref(raw), C.byref(steps), _ptr(scores, _f32p),
+                                           _ptr(turns, _i32p), _ptr(guesses, _i32p), _ptr(policy, _f32p))
+    return dict(status=status, raw=raw.value, steps=steps.value, scores=scores, turns=turns,
+                guesses=guesses.reshape(3 * w, 6), policy=None if policy is None else policy.reshape(3 * w, 6, 64))
+
+
+def normalize_fitness(raw: float, w: int) -> float:
+    return lib().nwo_normalize_fitness(raw, w)
+
+
+def cell_words_from_shards(shards: list[ShardRecord], rows: int, cols: int, cell: int, capacity: int = 8192):
+    arr = (ShardRecord * len(shards))(*shards)
+    out = np.zeros(capacity, np.uint32)
+    n = lib().nwo_cell_words_from_shards(arr, len(shards), rows, cols, cell, _ptr(out, _u32p), capacity)
+    return out[:n].copy()
+
+
+def select_parent_pair(fitness, has, rows, cols, next_rows, child, radius, draws, weights):
+    p1 = C.c_uint32()
+    p2 = C.c_uint32()
+    ok = lib().nwo_select_parent_pair(_ptr(np.ascontiguousarray(fitness, np.float32), _f32p),
+                                      _ptr(np.ascontiguousarray(has, np.uint8), _u8p), rows, cols, next_rows, child,
+                                      radius, _ptr(np.ascontiguousarray(draws, np.uint32), _u32p),
+                                      _ptr(np.ascontiguousarray(weights, np.float32), _f32p), len(weights) - 1,
+                                      C.byref(p1), C.byref(p2))
+    return (p1.value, p2.value) if ok else None
+
+
+def breed_and_mutate(p1: np.ndarray, p2: np.ndarray, action_count: int, tape: dict, cfg: dict) -> np.ndarray | None:
+    child = np.zeros(genome_halfs(action_count), np.uint16)
+    t = DrawTape(_ptr(tape["raw"], _u32p), _ptr(tape["uniform"], _f32p), _ptr(tape["normal_pair"], _f32p),
+                 len(tape["raw"]), 0, 0, 0.0, 0)
+    c = BreedConfig(cfg["l1"], cfg["l2"], cfg["l3"], cfg["p"], cfg["sigma"], cfg.get("row_scale", 0.0))
+    ok = lib().nwo_breed_and_mutate(_ptr(p1, _u16p), _ptr(p2, _u16p), action_count, _ptr(child, _u16p),
+                                    C.byref(t), C.byref(c))
+    return child if ok else None
+
+
+def bootstrap_normals_per_thread(action_count: int) -> int:
+    return max(lib().nwo_bootstrap_normals_per_thread(action_count, t) for t in range(256))
+
+
+def bootstrap_genome(action_count: int, normals: np.ndarray, per_thread: int) -> np.ndarray:
+    g = np.zeros(genome_halfs(action_count), np.uint16)
+    lib().nwo_bootstrap_genome(_ptr(g, _u16p), action_count, _ptr(np.ascontiguousarray(normals, np.float32), _f32p),
+                               per_thread)
+    return g
+
+
+def summarize(fitness: np.ndarray):
+    best = C.c_float()
+    avg = C.c_float()
+    bi = _sz()
+    f = np.ascontiguousarray(fitness, np.float32)
+    lib().nwo_summarize(_ptr(f, _f32p), len(f), C.byref(best), C.byref(avg), C.byref(bi))
+    return best.value, avg.value, bi.value
+
+
+# ---------------- reference host library (oracle/_ref/libref_host.so) ----------------
+
+@lru_cache(None)
+def ref_host() -> C.CDLL | None:
+    path = HERE / "_ref" / "libref_host.so"
+    if not path.exists():
+        return None
+    L = C.CDLL(str(path))
+    L.refhost_feedback.argtypes = [_u8p, _u8p, _u8p]
+    L.refhost_policy_forward.argtypes = [_u8p, _u8p, _sz, _u8p, _f32p]
+    L.refhost_score_action.restype = C.c_float
+    L.refhost_score_action.argtypes = [_f32p, _u8p, _u8p]
+    L.refhost_genome_stride_bytes.restype = _sz
+    L.refhost_genome_stride_bytes.argtypes = [_sz]
+    L.refhost_evaluate_population.argtypes = [_u8p, _sz, _sz, _sz, _u8p, _u32p, _u32p, _u32p, C.c_int, _f32p, _u64p,
+                                              C.POINTER(C.c_int)]
+    return L
+
+
+def ref_host_policy_forward(genome: np.ndarray, solution: np.ndarray, guesses: np.ndarray) -> np.ndarray | None:
+    guesses = np.ascontiguousarray(np.asarray(guesses, np.uint8).reshape(-1, 5))
+    out = np.zeros(64, np.float32)
+    ok = ref_host().refhost_policy_forward(_ptr(genome.view(np.uint8), _u8p),
+                                           _ptr(np.ascontiguousarray(solution, np.uint8), _u8p), len(guesses),
+                                           _ptr(guesses, _u8p), _ptr(out, _f32p))
+    return out if ok else None
+
+
+def ref_host_evaluate(genomes: np.ndarray, action_count: int, catalog: np.ndarray, cell_offsets: np.ndarray,
+                      cell_words: np.ndarray, cells: np.ndarray, threads: int):
+    """genomes: (n, halfs) uint16; returns (raw fitness, steps, status) per individual."""
+    n = genomes.shape[0]
+    raw = np.zeros(n, np.float32)
+    steps = np.zeros(n, np.uint64)
+    status = np.zeros(n, np.int32)
+    g = np.ascontiguousarray(genomes)
+    ref_host().refhost_evaluate_population(
+        _ptr(g.view(np.uint8).reshape(-1), _u8p), g.shape[1] * 2, n, action_count, _ptr(catalog, _u8p),
+        _ptr(np.ascontiguousarray(cell_offsets, np.uint32), _u32p),
+        _ptr(np.ascontiguousarray(cell_words, np.uint32), _u32p), _ptr(np.ascontiguousarray(cells, np.uint32), _u32p),
+        threads, _ptr(raw, _f32p), _ptr(steps, _u64p), status.ctypes.data_as(C.POINTER(C.c_int)))
+    return raw, steps, status
+
+
+# ---------------- GPU-side libraries (tapes and reference device code) ----------------
+
+@lru_cache(None)
+def tape_lib() -> C.CDLL:
+    L = C.CDLL(str(HERE / "_lib" / "libnwg_tape.so"))
+    L.tape_positions.argtypes = [C.c_uint32, C.c_ulonglong, _sz, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.tape_normal_streams.argtypes = [C.c_uint32, C.c_ulonglong, _sz, _sz, C.c_void_p]
+    L.tape_selection_draws.argtypes = [C.c_uint32, _sz, _sz, C.c_void_p]
+    L.tape_pow_table.argtypes = [C.c_float, _sz, C.c_void_p]
+    return L
+
+
+@lru_cache(None)
+def ref_dev() -> C.CDLL | None:
+    path = HERE / "_ref" / "libref_dev.so"
+    if not path.exists():
+        return None
+    L = C.CDLL(str(path))
+    L.refdev_upload_catalog.argtypes = [_u8p, _sz]
+    L.refdev_evaluate.argtypes = [C.c_void_p, _sz, _sz, _sz, _sz, C.c_void_p, _sz, _sz, C.c_void_p, C.c_void_p,
+                                  C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.refdev_select.argtypes = [C.c_void_p, C.c_void_p, _sz, _sz, _sz, _sz, _sz, C.c_float, C.c_uint32, C.c_void_p,
+                                C.c_void_p, C.c_void_p]
+    L.refdev_breed.argtypes = [C.c_void_p, _sz, C.c_void_p, _sz, C.c_void_p, _sz, _sz, C.c_uint32, _sz, C.c_float,
+                               C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, C.c_void_p]
+    L.refdev_bootstrap.argtypes = [C.c_void_p, _sz, _sz, _sz, C.c_uint32, _sz, C.c_void_p]
+    return L

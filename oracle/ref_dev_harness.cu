@@ -1,0 +1,248 @@
+// Device-side harness around the reference's own device functions.
+//
+// TEST INFRASTRUCTURE ONLY (built into oracle/_ref/libref_dev.so by oracle/build.py,
+// compiled for sm_100a from the reference's headers where they lie; nothing is copied).
+// Each kernel here calls the reference's __device__ functions in the order its own
+// kernels do, so the GPU parity tests can compare the new kernels with the
+// reference's arithmetic and random streams bit for bit on the same B200:
+//   - refdev_evaluate:  slab_runtime.cu:452-549 (warp per episode) with the guesses
+//                       and policy vectors of every decision recorded;
+//   - refdev_select:    slab_runtime.cu:633-675 (BuildSlabAssemblyPlanKernel body);
+//   - refdev_breed:     genotype_slab/device_runtime.cu:448-516 (breed + mutate body);
+//   - refdev_bootstrap: genotype_slab/device_runtime.cu:258-314 (initialisation body).
+// The reference's slab allocator (free-list spin lock) is never called: children and
+// organisms are written to caller-provided slots.
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+#include "genetic_algorithm/device/evaluation_ops.cuh"
+#include "genetic_algorithm/device/genome_ops.cuh"
+#include "genetic_algorithm/device/selection_ops.cuh"
+#include "training_folder/training_data.cu"
+
+namespace {
+
+namespace ga = neuroevolution::genetic_algorithm;
+namespace tf = neuroevolution::training_folder;
+using ga::device_evaluation_ops::DeviceGenomeEvaluationStatusCode;
+using ga::device_evaluation_ops::GenomeEvaluationWarpScratch;
+using ga::device_evaluation_ops::ScoreCompletedEpisode;
+using ga::device_evaluation_ops::TryCountLocalTrainingWords;
+using ga::device_evaluation_ops::TryInitializeEpisodeGrid;
+using neuroevolution::inference::dynamic_policy::DynamicInferenceStatusCode;
+using neuroevolution::inference::dynamic_policy::SelectNextGuessFromDynamicGenomeConcurrently;
+using neuroevolution::model::output_embedding::SelectedAction;
+using neuroevolution::spatial::CellularGridShape;
+
+constexpr int kWarps = 4;
+
+__global__ void EvaluateKernel(const std::uint8_t *slab, std::size_t pitch, std::size_t population,
+                               std::size_t action_count, const tf::TrainingDataShardRuntime *shards,
+                               std::size_t shard_count, CellularGridShape shape, std::size_t max_episodes,
+                               float *scores, int *turns, int *choices, float *policy_trace, int *status) {
+    __shared__ GenomeEvaluationWarpScratch<32> scratch[kWarps];
+    const std::size_t individual = blockIdx.x;
+    const int warp = threadIdx.x / 32;
+    const int lane = threadIdx.x % 32;
+    const std::size_t episode = static_cast<std::size_t>(blockIdx.y) * kWarps + warp;
+    if (individual >= population) {
+        return;
+    }
+    std::size_t local_words = 0;
+    if (TryCountLocalTrainingWords(shards, shard_count, shape, individual, local_words) !=
+        DeviceGenomeEvaluationStatusCode::kOk) {
+        if (lane == 0) {
+            atomicCAS(status, 0, 1);
+        }
+        return;
+    }
+    if (episode >= 3 * local_words || episode >= max_episodes) {
+        return;
+    }
+    const std::uint8_t *genome = slab + individual * pitch;
+    const std::size_t slot = individual * max_episodes + episode;
+    auto &s = scratch[warp];
+    if (lane == 0) {
+        s.status = static_cast<int>(TryInitializeEpisodeGrid(tf::DeviceTrainingWordCatalog(), shards, shard_count,
+                                                             shape, individual, episode, local_words, s.grid));
+    }
+    __syncwarp();
+    if (s.status != 0) {
+        if (lane == 0) {
+            atomicCAS(status, 0, 100 + s.status);
+        }
+        return;
+    }
+    int step = 0;
+    while (!s.grid.IsFinished()) {
+        SelectedAction selected{};
+        const DynamicInferenceStatusCode st = SelectNextGuessFromDynamicGenomeConcurrently<32>(
+            s.grid, tf::DeviceTrainingWordCatalog(), genome, action_count, s.dynamic_policy, selected);
+        if (st != DynamicInferenceStatusCode::kOk) {
+            if (lane == 0) {
+                atomicCAS(status, 0, 200 + static_cast<int>(st));
+            }
+            return;
+        }
+        if (policy_trace != nullptr) {
+            for (int k = lane; k < 64; k += 32) {
+                policy_trace[(slot * 6 + step) * 64 + k] = s.dynamic_policy.model.policy_vector[k];
+            }
+        }
+        if (lane == 0) {
+            choices[slot * 6 + step] = static_cast<int>(selected.action_index);
+            s.status = neuroevolution::wordle::TryAppendGuess(s.grid, selected.word) ? 0 : 2;
+        }
+        __syncwarp();
+        if (s.status != 0) {
+            if (lane == 0) {
+                atomicCAS(status, 0, 300);
+            }
+            return;
+        }
+        ++step;
+    }
+    if (lane == 0) {
+        scores[slot] = ScoreCompletedEpisode(s.grid);
+        turns[slot] = static_cast<int>(s.grid.turn_count);
+    }
+}
+
+__global__ void SelectKernel(const float *fitness, const std::uint8_t *has_fitness, std::size_t population,
+                             std::size_t child_count, std::size_t columns, std::size_t generation_index,
+                             ga::ParentSelectionConfig config, std::uint32_t planning_seed, std::uint32_t *pairs,
+                             int *ok) {
+    const std::size_t child = static_cast<std::size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (child >= child_count) {
+        return;
+    }
+    CellularGridShape current{};
+    CellularGridShape next{};
+    if (!neuroevolution::spatial::TryMakeCellularGridShapeForColumnCount(population, columns, current) ||
+        !neuroevolution::spatial::TryMakeCellularGridShapeForColumnCount(child_count, columns, next)) {
+        ok[child] = 0;
+        return;
+    }
+    auto state = ga::device_genome_ops::MakeDeviceRandomState(
+        planning_seed, static_cast<std::uint32_t>(child + (generation_index * 8191U)));
+    ga::ParentPair pair{};
+    ok[child] = ga::device_selection_ops::TrySelectCellularParentPairDevice(fitness, has_fitness, current, next, child,
+                                                                           state, config, pair)
+                    ? 1
+                    : 0;
+    pairs[2 * child] = static_cast<std::uint32_t>(pair.first_parent_index);
+    pairs[2 * child + 1] = static_cast<std::uint32_t>(pair.second_parent_index);
+}
+
+__global__ void BreedKernel(const std::uint8_t *parents, std::size_t parent_pitch, std::uint8_t *children,
+                            std::size_t child_pitch, const std::uint32_t *pairs, std::size_t child_count,
+                            std::size_t action_count, std::uint32_t generation_seed, std::size_t generation_index,
+                            ga::BreedingConfig breeding, ga::MutationConfig mutation) {
+    const std::size_t child = static_cast<std::size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (child >= child_count) {
+        return;
+    }
+    auto state = ga::device_genome_ops::MakeDeviceRandomState(
+        generation_seed, static_cast<std::uint32_t>(child + (generation_index * 4099U)));
+    ga::device_genome_ops::BreedAndMutateGenome(parents + pairs[2 * child] * parent_pitch,
+                                                parents + pairs[2 * child + 1] * parent_pitch, action_count,
+                                                children + child * child_pitch, state, breeding, mutation);
+}
+
+__global__ void BootstrapKernel(std::uint8_t *slab, std::size_t pitch, std::size_t population,
+                                std::size_t generation_index, std::uint32_t seed, std::size_t action_count) {
+    const std::size_t organism = blockIdx.x;
+    if (organism >= population) {
+        return;
+    }
+    const std::uint64_t stream =
+        ((static_cast<std::uint64_t>(generation_index) * population + organism) * blockDim.x) + threadIdx.x;
+    auto state = ga::device_genome_ops::MakeDeviceRandomState(seed, stream);
+    ga::device_genome_ops::InitializeRandomGenome(slab + organism * pitch, action_count, state, threadIdx.x,
+                                                  blockDim.x);
+}
+
+} // namespace
+
+extern "C" {
+
+int refdev_upload_catalog(const std::uint8_t *letters, std::size_t count) {
+    static tf::TrainingWordCatalog catalog{};
+    catalog = {};
+    if (count > tf::kTrainingWordCatalogCapacity) {
+        return 0;
+    }
+    for (std::size_t w = 0; w < count; ++w) {
+        for (std::size_t p = 0; p < 5; ++p) {
+            catalog.words[w].letter_indices[p] = letters[5 * w + p];
+        }
+    }
+    catalog.word_count = count;
+    return tf::UploadTrainingWordCatalogToDeviceConstantMemory(catalog) ? 1 : 0;
+}
+
+// shards: host array of 48-byte TrainingDataShardRuntime records (training_data.hpp:35-42).
+int refdev_evaluate(const void *slab, std::size_t pitch, std::size_t population, std::size_t columns,
+                    std::size_t action_count, const void *host_shards, std::size_t shard_count,
+                    std::size_t max_episodes, float *scores, int *turns, int *choices, float *policy_trace,
+                    int *status, void *stream) {
+    static_assert(sizeof(tf::TrainingDataShardRuntime) == 48, "shard record layout");
+    tf::TrainingDataShardRuntime *shards = nullptr;
+    if (cudaMalloc(&shards, shard_count * sizeof(*shards)) != cudaSuccess) {
+        return 0;
+    }
+    cudaMemcpy(shards, host_shards, shard_count * sizeof(*shards), cudaMemcpyHostToDevice);
+    CellularGridShape shape{};
+    if (!neuroevolution::spatial::TryMakeCellularGridShapeForColumnCount(population, columns, shape)) {
+        cudaFree(shards);
+        return 0;
+    }
+    dim3 grid(static_cast<unsigned>(population), static_cast<unsigned>((max_episodes + kWarps - 1) / kWarps));
+    EvaluateKernel<<<grid, 32 * kWarps, 0, static_cast<cudaStream_t>(stream)>>>(
+        static_cast<const std::uint8_t *>(slab), pitch, population, action_count, shards, shard_count, shape,
+        max_episodes, scores, turns, choices, policy_trace, status);
+    const bool ok = cudaGetLastError() == cudaSuccess && cudaStreamSynchronize(static_cast<cudaStream_t>(stream)) ==
+                                                             cudaSuccess;
+    cudaFree(shards);
+    return ok ? 1 : 0;
+}
+
+int refdev_select(const float *fitness, const std::uint8_t *has_fitness, std::size_t population,
+                  std::size_t child_count, std::size_t columns, std::size_t generation_index, std::size_t radius,
+                  float rank_exponent, std::uint32_t planning_seed, std::uint32_t *pairs, int *ok, void *stream) {
+    ga::ParentSelectionConfig config{};
+    config.cellular_breeding_radius = radius;
+    config.rank_exponent = rank_exponent;
+    SelectKernel<<<static_cast<unsigned>((child_count + 127) / 128), 128, 0, static_cast<cudaStream_t>(stream)>>>(
+        fitness, has_fitness, population, child_count, columns, generation_index, config, planning_seed, pairs, ok);
+    return cudaGetLastError() == cudaSuccess ? 1 : 0;
+}
+
+int refdev_breed(const void *parents, std::size_t parent_pitch, void *children, std::size_t child_pitch,
+                 const std::uint32_t *pairs, std::size_t child_count, std::size_t action_count,
+                 std::uint32_t generation_seed, std::size_t generation_index, float l1, float l2, float l3,
+                 float mutation_probability, float mutation_sigma, float row_scale_probability, void *stream) {
+    ga::BreedingConfig breeding{};
+    breeding.crossover_temperature_level1 = l1;
+    breeding.crossover_temperature_level2 = l2;
+    breeding.crossover_temperature_level3 = l3;
+    ga::MutationConfig mutation{};
+    mutation.mutation_probability = mutation_probability;
+    mutation.mutation_sigma = mutation_sigma;
+    mutation.output_tail_row_scale_mutation_probability = row_scale_probability;
+    BreedKernel<<<static_cast<unsigned>((child_count + 31) / 32), 32, 0, static_cast<cudaStream_t>(stream)>>>(
+        static_cast<const std::uint8_t *>(parents), parent_pitch, static_cast<std::uint8_t *>(children), child_pitch,
+        pairs, child_count, action_count, generation_seed, generation_index, breeding, mutation);
+    return cudaGetLastError() == cudaSuccess ? 1 : 0;
+}
+
+int refdev_bootstrap(void *slab, std::size_t pitch, std::size_t population, std::size_t generation_index,
+                     std::uint32_t seed, std::size_t action_count, void *stream) {
+    BootstrapKernel<<<static_cast<unsigned>(population), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        static_cast<std::uint8_t *>(slab), pitch, population, generation_index, seed, action_count);
+    return cudaGetLastError() == cudaSuccess ? 1 : 0;
+}
+
+} // extern "C"
