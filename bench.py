@@ -1,0 +1,352 @@
+"""Benchmark: one GA generation (evaluate, select, breed, mutate) per step on the B200.
+
+Workload: population 4,096 on a 64x64 toroidal grid, 4,739 synthetic catalog words all active, 256
+secrets per cell drawn from a 2,315-word secret subset (3 episodes per secret), radius-1 rank selection,
+reference crossover temperatures, mutation p = 0.05, sigma = 0.02. Genomes are the reference's FP16
+layout (bootstrap He-normal weights, N(0, 0.05) tails) and the arithmetic is FP32 (plain form).
+
+Prints one JSON line (rank 0). `--impl reference` times the reference's own CPU path (its host-callable
+model, scoring and Wordle code composed into its episode loop, built in oracle/_ref) on a bounded sample
+of the same workload with every host thread.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+MEASURED = ROOT / "MEASURED_PEAKS.json"
+TRAFFIC = ROOT / "profiles" / "eval_fp32_traffic.json"
+KERNELS_PER_GENERATION = 7  # prepare, evaluate, finalize, summarize, select, plan slots, breed
+
+
+def algorithmic_flops(steps: int, encoded: int, action_count: int) -> float:
+    """2 * (9,472 per encoded turn + (123,136 + 64 A) per game step): encoder 10 gathered columns x 128 +
+    128 x 64; trunk 321x256 + 256x128 + 128x64; scoring 64 per action."""
+    return 2.0 * (9472.0 * encoded + (123136.0 + 64.0 * action_count) * steps)
+
+
+def peaks() -> dict:
+    if MEASURED.exists():
+        m = json.loads(MEASURED.read_text())
+        return dict(hbm_gbs=m["hbm_gbs"], bf16_tflops=m["bf16_tflops"], sm_max_mhz=m.get("sm_max_mhz", 1965.0),
+                    source="measured")
+    return dict(hbm_gbs=6650.0, bf16_tflops=1590.0, sm_max_mhz=1965.0, source="fallback")
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.device_index = device_index
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device_index}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.file,
+                                         stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        self.file.flush()
+        rows = [r.split(",") for r in Path(self.file.name).read_text().splitlines() if r.strip()]
+        os.unlink(self.file.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if len(r) > 5 + i and "Active" in r[5 + i]
+                          and "Not" not in r[5 + i]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup(gpus: int):
+    import torch
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return rank, world, local
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(value: float, world: int) -> float:
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(value: float, world: int) -> float:
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def cpu_reference_rate(catalog, offsets, words, genomes_u16, action_count, sample_individuals, threads):
+    """game-steps/s of the reference's CPU path on `sample_individuals` genomes (oracle/_ref/libref_host.so)."""
+    from oracle import pyoracle as O
+
+    if O.ref_host() is None:
+        return None
+    n = len(genomes_u16)
+    cells = np.arange(n, dtype=np.uint32)
+    t0 = time.perf_counter()
+    raw, steps, status = O.ref_host_evaluate(genomes_u16, action_count, catalog, offsets[:n + 1], words, cells,
+                                             threads)
+    dt = time.perf_counter() - t0
+    assert (status == 0).all()
+    return float(steps.sum()) / dt, dt, int(steps.sum())
+
+
+def run_ours(args) -> None:
+    import torch
+
+    rank, world, local = dist_setup(args.gpus)
+    nwg = importlib.import_module("neuroevolutionary-wordle_b200")
+    wl = nwg.workload.FULL if args.workload == "full" else nwg.workload.SMALL
+    catalog = wl.catalog()
+    offsets, words = wl.cell_lists()
+    nwg.capi.upload_catalog(catalog)
+    stream = torch.cuda.current_stream()
+    rt = nwg.Runtime(wl.action_count, wl.population, wl.columns, stream=stream.cuda_stream)
+    rt.set_cell_words(offsets, words)
+    rt.bootstrap(wl.population, seed=0 + rank)
+    counts = nwg.capi.word_counts(training=wl.action_count, action_space=wl.action_count)
+    cfg = nwg.capi.assembly_config(radius=wl.radius, p=wl.mutation_probability, sigma=wl.mutation_sigma)
+
+    # CPU baseline sample: the reference CPU path on the first genomes of generation 0 (rank 0, N=1 only).
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        sample = min(wl.population, max(2, threads))
+        genomes = np.stack([rt.download_slot(i).view(np.uint16) for i in range(sample)])
+        res = cpu_reference_rate(catalog, offsets, words, genomes, wl.action_count, sample, threads)
+        if res is not None:
+            rate, dt, steps = res
+            cpu = {"value": rate, "unit": "game-steps/s", "cores": threads, "kind": "reference",
+                   "sample": f"generation-0 evaluation of {sample} of {wl.population} individuals "
+                             f"({steps} game steps, {dt:.1f} s) with {threads} threads"}
+
+    gen = 0
+    for _ in range(args.warmup):
+        rt.advance(seed=1000 + gen, counts=counts, config=cfg)
+        gen += 1
+
+    # ---- device-resident timed region ----
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    steps = 0
+    encoded = 0
+    kernel_ms = []
+    barrier(world)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        start.record(stream)
+        for _ in range(args.steps):
+            rt.advance(seed=1000 + gen, counts=counts, config=cfg)
+            st = rt.stats()
+            steps += st.game_steps
+            encoded += st.encoded_turns
+            kernel_ms.append(st.eval_kernel_ms)
+            gen += 1
+        end.record(stream)
+        torch.cuda.synchronize()
+    barrier(world)
+    ms = max_over_ranks(start.elapsed_time(end), world)
+    clock = clocks.summary()
+    total_steps = sum_over_ranks(float(steps), world)
+
+    # ---- end-to-end through the public API with host buffers ----
+    pinned_offsets = torch.from_numpy(offsets).pin_memory().numpy()
+    pinned_words = torch.from_numpy(words).pin_memory().numpy()
+    e2e_start = torch.cuda.Event(enable_timing=True)
+    e2e_end = torch.cuda.Event(enable_timing=True)
+    e2e_steps = 0
+    e2e_iters = max(1, min(args.steps, 3))
+    barrier(world)
+    torch.cuda.synchronize()
+    e2e_start.record(stream)
+    for _ in range(e2e_iters):
+        rt.set_cell_words(pinned_offsets, pinned_words)
+        rt.advance(seed=1000 + gen, counts=counts, config=cfg)
+        e2e_steps += rt.stats().game_steps
+        _ = rt.summary().best_fitness
+        gen += 1
+    e2e_end.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(e2e_start.elapsed_time(e2e_end), world)
+    e2e_total = sum_over_ranks(float(e2e_steps), world)
+
+    if rank != 0:
+        rt.close()
+        return
+    pk = peaks()
+    mean_steps = steps / args.steps
+    mean_encoded = encoded / args.steps
+    kernel_mean_ms = sum(kernel_ms) / len(kernel_ms)
+    flops = algorithmic_flops(int(mean_steps), int(mean_encoded), wl.action_count)
+    achieved_tflops = flops / (kernel_mean_ms * 1e-3) / 1e12
+    fp32_peak = 148 * 128 * 2 * pk["sm_max_mhz"] * 1e6 / 1e12
+    traffic = None
+    if TRAFFIC.exists():
+        traffic = json.loads(TRAFFIC.read_text()).get("bytes_per_launch")
+    value = total_steps / (ms * 1e-3)
+    line = {
+        "metric": "game-steps/s",
+        "value": value,
+        "unit": "game-steps/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "fp32 (fp16-stored genomes)",
+        "data": "synthetic",
+        "impl": "ours",
+        "generations_per_s": args.steps / (ms * 1e-3),
+        "config": {"workload": wl.name, "population": wl.population, "grid": f"{wl.population // wl.columns}x"
+                   f"{wl.columns}", "action_count": wl.action_count, "secrets_per_cell": wl.secrets_per_cell,
+                   "secret_subset": wl.secret_subset, "episodes_per_secret": 3, "selection_radius": wl.radius,
+                   "mutation_probability": wl.mutation_probability, "mutation_sigma": wl.mutation_sigma,
+                   "form": "plain fp32", "parallelism": f"{world} independent populations (one per GPU)",
+                   "l2": "inputs larger than L2 (genome slab "
+                         f"{wl.population * nwg.capi.genome_stride_bytes(wl.action_count) / 1e9:.2f} GB)"},
+        "roofline": {"kernel": "EvalFp32Kernel", "bound": "fp32", "achieved": achieved_tflops,
+                     "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved_tflops / fp32_peak,
+                     "traffic": traffic, "peak_source": f"148 SMs x 128 FFMA/clk x 2 x {pk['sm_max_mhz']:.0f} MHz "
+                                                         f"(sm_max_mhz {pk['source']})",
+                     "frac_of_bf16_tensor_peak": achieved_tflops / pk["bf16_tflops"],
+                     "kernel_ms_per_launch": kernel_mean_ms, "algorithmic_flop_per_launch": flops,
+                     "game_steps_per_launch": mean_steps},
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_total / (e2e_ms * 1e-3), "unit": "game-steps/s",
+                "h2d_bytes_per_step": int(offsets.nbytes + words.nbytes + 120),
+                "d2h_bytes_per_step": 4 + 48 + 24},
+        "gpu_launches": KERNELS_PER_GENERATION * args.steps,
+        "clocks": clock,
+    }
+    print(json.dumps(line), flush=True)
+    rt.close()
+
+
+def run_reference(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import pyoracle as O
+
+    nwg_workload = importlib.import_module("neuroevolutionary-wordle_b200.workload")
+    wl = nwg_workload.FULL if args.workload == "full" else nwg_workload.SMALL
+    if O.ref_host() is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref_host.so was not built"}))
+        return
+    catalog = wl.catalog()
+    offsets, words = wl.cell_lists()
+    threads = os.cpu_count() or 1
+    sample = max(2, threads)
+    rng = np.random.default_rng(0)
+    halfs = 150528 + 38 * wl.action_count
+    stds = [np.sqrt(2.0 / 145)] * (128 * 145) + [0.0] * 128 + [np.sqrt(2.0 / 128)] * (64 * 128) + [0.0] * 64 + \
+        [np.sqrt(2.0 / 321)] * (256 * 321) + [0.0] * 256 + [np.sqrt(2.0 / 256)] * (128 * 256) + [0.0] * 128 + \
+        [np.sqrt(2.0 / 128)] * (64 * 128) + [0.0] * 64 + [0.05] * (38 * wl.action_count)
+    stds = np.array(stds, np.float32)
+    assert len(stds) == halfs
+    genomes = (rng.standard_normal((sample, halfs)).astype(np.float32) * stds).astype(np.float16).view(np.uint16)
+    times = []
+    steps_total = 0
+    for it in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        cells = ((np.arange(sample) + it * sample) % wl.population).astype(np.uint32)
+        raw, steps, status = O.ref_host_evaluate(genomes, wl.action_count, catalog, offsets, words, cells, threads)
+        dt = time.perf_counter() - t0
+        if it >= args.warmup:
+            times.append(dt)
+            steps_total += int(steps.sum())
+    total_s = sum(times)
+    value = steps_total / total_s
+    print(json.dumps({
+        "metric": "game-steps/s", "value": value, "unit": "game-steps/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * total_s / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "fp32 (fp16-stored genomes)", "data": "synthetic",
+        "impl": "reference",
+        "config": {"workload": wl.name, "population": wl.population, "action_count": wl.action_count,
+                   "secrets_per_cell": wl.secrets_per_cell, "form": "reference CPU path",
+                   "sample_per_step": f"evaluation of {sample} individuals"},
+        "cpu_baseline": {"value": value, "unit": "game-steps/s", "cores": threads, "kind": "reference",
+                         "sample": f"{sample} individuals per step, {steps_total} game steps timed"},
+        "e2e": {"value": value, "unit": "game-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["full", "small"], default="full")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

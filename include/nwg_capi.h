@@ -1,0 +1,256 @@
+/*
+ * nwg_capi.h -- C ABI of the B200 fitness-evaluation / generation-step runtime.
+ *
+ * Drop-in boundary for sam-bee/neuroevolutionary-wordle's device GA runtime
+ * (src/genetic_algorithm/device/slab_runtime.hpp, namespace
+ * neuroevolution::genetic_algorithm::slab_device). Every entry point below names the
+ * reference function it replaces. Conventions:
+ *   - plain pointers and sizes, no C++ or torch types;
+ *   - every call returns an nwg status code: 0 is success, 1..16 are the reference's
+ *     DeviceSlabGARuntimeStatusCode values (slab_runtime.hpp:21-39), 17 and 18 are
+ *     additions (a bounded device wait that gave up; a feature this runtime rejects);
+ *   - the last failure is also kept as the runtime's sticky status, readable with
+ *     nwg_read_status, as the reference keeps its device status int;
+ *   - all device work of a runtime is issued on its stream (nwg_set_stream), and a call
+ *     returns after that work has finished, like the reference's synchronous API.
+ * Struct layouts equal the reference's POD structs on LP64 so a C++ shim can pass them
+ * through unchanged.
+ */
+#ifndef NWG_CAPI_H
+#define NWG_CAPI_H
+
+#include <stdbool.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NWG_ABI_VERSION 1
+#define NWG_CATALOG_CAPACITY 4739
+
+enum {
+    NWG_OK = 0,
+    NWG_CUDA_FAILURE = 1,
+    NWG_INVALID_RUNTIME_CONFIG = 2,
+    NWG_INVALID_SLAB = 3,
+    NWG_INVALID_GENERATION = 4,
+    NWG_INVALID_TRAINING_SHARD = 5,
+    NWG_GUESS_APPEND_FAILED = 6,
+    NWG_POLICY_FORWARD_FAILED = 7,
+    NWG_ACTION_SELECTION_FAILED = 8,
+    NWG_POPULATION_NOT_EVALUATED = 9,
+    NWG_INVALID_ASSEMBLY_CONFIG = 10,
+    NWG_PARENT_SELECTION_FAILED = 11,
+    NWG_INVALID_ASSEMBLY_PLAN = 12,
+    NWG_INVALID_PARENT_INDEX = 13,
+    NWG_SLAB_FULL = 14,
+    NWG_OUTPUT_EMBEDDING_INJECTION_FAILED = 15,
+    NWG_SLAB_REPACK_FAILED = 16,
+    NWG_TIMEOUT = 17,
+    NWG_UNSUPPORTED = 18,
+};
+
+typedef struct nwg_runtime nwg_runtime;
+
+/* DeviceSlabGARuntimeConfig (slab_runtime.hpp:41-48). */
+typedef struct {
+    size_t genotype_slab_byte_budget_bytes;
+    size_t generation_byte_budget_bytes;
+    size_t host_spillover_byte_budget_bytes;
+    size_t action_count;
+    size_t population_size_ceiling;
+    size_t grid_column_count;
+} nwg_runtime_config;
+
+/* WordCountSchedule (training_folder/training_data.hpp:24-28). */
+typedef struct {
+    size_t initial_word_count;
+    size_t word_count_step;
+    size_t word_count_step_period_generations;
+} nwg_word_count_schedule;
+
+/* RuntimeWordCounts (genetic_algorithm/device/runtime_common.hpp:10-16). */
+typedef struct {
+    size_t training_word_count;
+    size_t action_space_word_count;
+    nwg_word_count_schedule training_word_schedule;
+    size_t shard_initial_radius;
+    size_t shard_radius_growth_period_generations;
+} nwg_runtime_word_counts;
+
+/* TrainingDataShardReleaseHistory (training_folder/training_data.hpp:49-53). */
+typedef struct {
+    size_t release_generations[NWG_CATALOG_CAPACITY];
+    float release_fitness_p99[NWG_CATALOG_CAPACITY];
+    size_t release_count;
+} nwg_shard_release_history;
+
+/* PopulationFitnessSummary (genetic_algorithm/device/runtime_common.hpp:18-26). */
+typedef struct {
+    float best_fitness;
+    float average_fitness;
+    size_t best_index;
+    uint32_t best_slot_index;
+    size_t generation_index;
+    size_t action_count;
+    size_t population_size;
+} nwg_fitness_summary;
+
+/* ParentSelectionConfig, BreedingConfig, MutationConfig, GenerationAssemblyConfig
+ * (genetic_algorithm/selection.hpp:15-18, breeding.hpp:11-15, mutation.hpp:11-15,
+ * generation_assembly.hpp:9-13). */
+typedef struct {
+    size_t cellular_breeding_radius;
+    float rank_exponent;
+} nwg_parent_selection_config;
+
+typedef struct {
+    float crossover_temperature_level1;
+    float crossover_temperature_level2;
+    float crossover_temperature_level3;
+} nwg_breeding_config;
+
+typedef struct {
+    float mutation_probability;
+    float mutation_sigma;
+    float output_tail_row_scale_mutation_probability;
+} nwg_mutation_config;
+
+typedef struct {
+    nwg_parent_selection_config parent_selection;
+    nwg_breeding_config breeding;
+    nwg_mutation_config mutation;
+} nwg_generation_assembly_config;
+
+/* PendingOutputEmbeddingInjection (genotype_slab/device_runtime.hpp:26-30). */
+typedef struct {
+    bool enabled;
+    size_t first_catalog_word_index;
+    size_t injection_count;
+} nwg_pending_injection;
+
+/* Statistics of the last evaluation, beyond the reference's summary. */
+typedef struct {
+    uint64_t game_steps;        /* policy decisions made (one forward + scoring + argmax + feedback each) */
+    uint64_t episodes;          /* games played */
+    uint64_t encoded_turns;     /* turns run through the shared encoder (each turn once) */
+    double fitness_mean_fp64;   /* FP64 reductions for the adaptive shard-release statistics */
+    double fitness_variance_fp64;
+    double eval_kernel_ms;      /* device time of the last evaluation kernel (CUDA events on the runtime's stream) */
+} nwg_evaluation_stats;
+
+typedef struct {
+    size_t action_count;
+    size_t slot_stride_bytes;   /* reference genome image size (dynamic_layout.hpp:30-36) */
+    size_t slot_pitch_bytes;    /* device placement pitch of a slot (256-byte aligned) */
+    size_t slot_count;
+    size_t max_generation_size;
+    size_t grid_column_count;
+    size_t current_generation_index;
+    size_t current_generation_size;
+} nwg_runtime_info;
+
+/* Callbacks of TryAdvanceGenerationOnDevice (slab_runtime.hpp:81-84); return true to continue. */
+typedef bool (*nwg_post_fitness_fn)(nwg_runtime *runtime, const nwg_runtime_word_counts *counts, void *user);
+typedef bool (*nwg_shard_release_fn)(nwg_runtime *runtime, const nwg_runtime_word_counts *counts,
+                                     nwg_pending_injection *pending, void *user);
+
+/* DeviceSlabGARuntimeStatusCodeString (slab_runtime.hpp:186). */
+const char *nwg_status_string(int status);
+
+int nwg_abi_version(void);
+
+/* UploadTrainingWordCatalogToDeviceConstantMemory (training_folder/training_data.hpp:375).
+ * letters: word_count rows of 5 letter indices (0..25); process-wide, like the reference's catalog. */
+int nwg_upload_catalog(const uint8_t *letters, size_t word_count);
+
+/* TryCreateDeviceSlabGARuntimeBuffers / DestroyDeviceSlabGARuntimeBuffers (slab_runtime.hpp:119-121). */
+int nwg_create(const nwg_runtime_config *config, nwg_runtime **runtime_out);
+void nwg_destroy(nwg_runtime *runtime);
+
+/* Issue this runtime's device work on `cuda_stream` (a cudaStream_t; NULL = legacy default stream). */
+int nwg_set_stream(nwg_runtime *runtime, void *cuda_stream);
+
+int nwg_get_info(const nwg_runtime *runtime, nwg_runtime_info *info);
+
+/* TryBootstrapRandomCurrentGenerationOnDevice (slab_runtime.hpp:123-124). */
+int nwg_bootstrap(nwg_runtime *runtime, size_t generation_size, uint32_t generation_seed, size_t generation_index);
+
+/* Explicit per-cell training-word lists (CSR: cell c's words are words[offsets[c] .. offsets[c+1]),
+ * catalog indices). No reference counterpart: while set, evaluation takes each cell's words from this
+ * list instead of the reference shard set, so per-cell secret sets of any size can be expressed.
+ * Passing cell_count = 0 returns to the shard set. */
+int nwg_set_cell_words(nwg_runtime *runtime, const uint32_t *offsets, const uint32_t *words, size_t cell_count);
+
+/* TryEvaluateCurrentGenerationFitnessOnDevice (slab_runtime.hpp:137-139). history may be NULL. */
+int nwg_evaluate(nwg_runtime *runtime, const nwg_runtime_word_counts *counts,
+                 const nwg_shard_release_history *history);
+
+/* TryReadPopulationFitnessSummaryFromDevice (slab_runtime.hpp:141-142). */
+int nwg_read_summary(const nwg_runtime *runtime, nwg_fitness_summary *summary);
+
+int nwg_read_evaluation_stats(const nwg_runtime *runtime, nwg_evaluation_stats *stats);
+
+/* TryAdvanceGenerationOnDevice (slab_runtime.hpp:144-150): evaluate, select, breed, mutate, swap.
+ * config and pending may be NULL (reference defaults); callbacks may be NULL. */
+int nwg_advance(nwg_runtime *runtime, uint32_t generation_seed, const nwg_runtime_word_counts *counts,
+                const nwg_generation_assembly_config *config, const nwg_pending_injection *pending,
+                nwg_post_fitness_fn post_fitness, void *post_fitness_user, nwg_shard_release_fn shard_release,
+                void *shard_release_user, const nwg_shard_release_history *history);
+
+/* SwapDeviceSlabGenerationBuffers (slab_runtime.hpp:181). */
+int nwg_swap_generations(nwg_runtime *runtime);
+
+/* TryReadDeviceSlabGARuntimeStatus (slab_runtime.hpp:183-184). */
+int nwg_read_status(const nwg_runtime *runtime, int *status);
+
+/* TryDownloadCurrentGenerationFromDevice (slab_runtime.hpp:131-132). Arrays hold `capacity` entries. */
+int nwg_download_current_generation(const nwg_runtime *runtime, uint32_t *slot_indices, float *fitness,
+                                    uint32_t *evaluation_counts, uint8_t *has_fitness, size_t capacity,
+                                    size_t *count_out, size_t *generation_index_out);
+
+/* TryDownloadSlabSlotBytesFromDevice (slab_runtime.hpp:128-129): the slot's genome image,
+ * slot_stride_bytes long, byte-identical to the reference layout. */
+int nwg_download_slot(const nwg_runtime *runtime, uint32_t slot_index, uint8_t *bytes, size_t capacity,
+                      size_t *byte_count_out);
+
+/* TryUploadSlabToDevice / TryUploadCurrentGenerationToDevice (genotype_slab/device_runtime.hpp:89-93):
+ * place a genome image in a slot, and set the current generation's slot list. */
+int nwg_upload_slot(nwg_runtime *runtime, uint32_t slot_index, const uint8_t *bytes, size_t byte_count);
+int nwg_upload_current_generation(nwg_runtime *runtime, const uint32_t *slot_indices, size_t count,
+                                  size_t generation_index);
+
+/* The assembly plan of the last advance: count (first, second) parent indices (SlabParentPair,
+ * genotype_slab/assembly.hpp:12-15). */
+int nwg_download_assembly_plan(const nwg_runtime *runtime, uint32_t *pairs, size_t capacity, size_t *count_out);
+
+/* Test and benchmark hooks (no reference counterpart). */
+int nwg_device_slab(const nwg_runtime *runtime, void **slab_out, size_t *pitch_out);
+
+/* Evaluation with per-episode trace of the first trace_episodes episodes of every individual
+ * (device buffers, each may be NULL): choices[ind][e][6], turns[ind][e], scores[ind][e],
+ * policy[ind][e][6][64]. */
+int nwg_evaluate_traced(nwg_runtime *runtime, const nwg_runtime_word_counts *counts,
+                        const nwg_shard_release_history *history, size_t trace_episodes, void *choices,
+                        void *turns, void *scores, void *policy);
+
+/* Parent selection and child assembly as separate device steps over caller buffers (device pointers),
+ * for differential tests: select writes child_count pairs; breed writes child i to child_slab slot i. */
+int nwg_select_parents_device(const float *fitness, const uint8_t *has_fitness, size_t population,
+                              size_t columns, size_t child_count, size_t generation_index,
+                              const nwg_parent_selection_config *config, uint32_t planning_seed, uint32_t *pairs,
+                              void *cuda_stream);
+int nwg_breed_device(const void *parent_slab, size_t parent_pitch, const uint32_t *parent_slots,
+                     void *child_slab, size_t child_pitch, const uint32_t *pairs, size_t child_count,
+                     size_t action_count, uint32_t generation_seed, size_t generation_index,
+                     const nwg_breeding_config *breeding, const nwg_mutation_config *mutation, void *cuda_stream);
+int nwg_bootstrap_device(void *slab, size_t pitch, size_t population, size_t generation_index, uint32_t seed,
+                         size_t action_count, void *cuda_stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NWG_CAPI_H */

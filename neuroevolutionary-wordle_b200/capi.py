@@ -1,0 +1,322 @@
+"""ctypes bindings of the runtime's C ABI (include/nwg_capi.h).
+
+The product is the CUDA library libnwg.so built in this directory; this module only binds it.
+There is no fallback: loading fails loudly when the library is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from functools import lru_cache
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "libnwg.so"
+CATALOG_CAPACITY = 4739
+_sz = C.c_size_t
+_vp = C.c_void_p
+
+
+class NwgError(RuntimeError):
+    def __init__(self, status: int, where: str):
+        super().__init__(f"{where}: status {status} ({status_string(status)})")
+        self.status = status
+
+
+class RuntimeConfig(C.Structure):
+    _fields_ = [(n, _sz) for n in ("genotype_slab_byte_budget_bytes", "generation_byte_budget_bytes",
+                                   "host_spillover_byte_budget_bytes", "action_count", "population_size_ceiling",
+                                   "grid_column_count")]
+
+
+class WordCountSchedule(C.Structure):
+    _fields_ = [("initial_word_count", _sz), ("word_count_step", _sz), ("word_count_step_period_generations", _sz)]
+
+
+class RuntimeWordCounts(C.Structure):
+    _fields_ = [("training_word_count", _sz), ("action_space_word_count", _sz),
+                ("training_word_schedule", WordCountSchedule), ("shard_initial_radius", _sz),
+                ("shard_radius_growth_period_generations", _sz)]
+
+
+class ShardReleaseHistory(C.Structure):
+    _fields_ = [("release_generations", _sz * CATALOG_CAPACITY), ("release_fitness_p99", C.c_float * CATALOG_CAPACITY),
+                ("release_count", _sz)]
+
+
+class FitnessSummary(C.Structure):
+    _fields_ = [("best_fitness", C.c_float), ("average_fitness", C.c_float), ("best_index", _sz),
+                ("best_slot_index", C.c_uint32), ("generation_index", _sz), ("action_count", _sz),
+                ("population_size", _sz)]
+
+
+class ParentSelectionConfig(C.Structure):
+    _fields_ = [("cellular_breeding_radius", _sz), ("rank_exponent", C.c_float)]
+
+
+class BreedingConfig(C.Structure):
+    _fields_ = [("crossover_temperature_level1", C.c_float), ("crossover_temperature_level2", C.c_float),
+                ("crossover_temperature_level3", C.c_float)]
+
+
+class MutationConfig(C.Structure):
+    _fields_ = [("mutation_probability", C.c_float), ("mutation_sigma", C.c_float),
+                ("output_tail_row_scale_mutation_probability", C.c_float)]
+
+
+class AssemblyConfig(C.Structure):
+    _fields_ = [("parent_selection", ParentSelectionConfig), ("breeding", BreedingConfig),
+                ("mutation", MutationConfig)]
+
+
+class PendingInjection(C.Structure):
+    _fields_ = [("enabled", C.c_bool), ("first_catalog_word_index", _sz), ("injection_count", _sz)]
+
+
+class EvaluationStats(C.Structure):
+    _fields_ = [("game_steps", C.c_uint64), ("episodes", C.c_uint64), ("encoded_turns", C.c_uint64),
+                ("fitness_mean_fp64", C.c_double), ("fitness_variance_fp64", C.c_double),
+                ("eval_kernel_ms", C.c_double)]
+
+
+class RuntimeInfo(C.Structure):
+    _fields_ = [(n, _sz) for n in ("action_count", "slot_stride_bytes", "slot_pitch_bytes", "slot_count",
+                                   "max_generation_size", "grid_column_count", "current_generation_index",
+                                   "current_generation_size")]
+
+
+POST_FITNESS_FN = C.CFUNCTYPE(C.c_bool, _vp, C.POINTER(RuntimeWordCounts), _vp)
+SHARD_RELEASE_FN = C.CFUNCTYPE(C.c_bool, _vp, C.POINTER(RuntimeWordCounts), C.POINTER(PendingInjection), _vp)
+
+EXPORTS = [
+    "nwg_abi_version", "nwg_status_string", "nwg_upload_catalog", "nwg_create", "nwg_destroy", "nwg_set_stream",
+    "nwg_get_info", "nwg_bootstrap", "nwg_set_cell_words", "nwg_evaluate", "nwg_read_summary",
+    "nwg_read_evaluation_stats", "nwg_advance", "nwg_swap_generations", "nwg_read_status",
+    "nwg_download_current_generation", "nwg_download_slot", "nwg_upload_slot", "nwg_upload_current_generation",
+    "nwg_download_assembly_plan", "nwg_device_slab", "nwg_evaluate_traced", "nwg_select_parents_device",
+    "nwg_breed_device", "nwg_bootstrap_device",
+]
+
+
+@lru_cache(None)
+def lib() -> C.CDLL:
+    if not LIB_PATH.exists():
+        raise FileNotFoundError(f"{LIB_PATH} is not built; run neuroevolutionary-wordle_b200/build.py")
+    L = C.CDLL(str(LIB_PATH))
+    L.nwg_status_string.restype = C.c_char_p
+    L.nwg_status_string.argtypes = [C.c_int]
+    L.nwg_upload_catalog.argtypes = [_vp, _sz]
+    L.nwg_create.argtypes = [C.POINTER(RuntimeConfig), C.POINTER(_vp)]
+    L.nwg_destroy.argtypes = [_vp]
+    L.nwg_destroy.restype = None
+    L.nwg_set_stream.argtypes = [_vp, _vp]
+    L.nwg_get_info.argtypes = [_vp, C.POINTER(RuntimeInfo)]
+    L.nwg_bootstrap.argtypes = [_vp, _sz, C.c_uint32, _sz]
+    L.nwg_set_cell_words.argtypes = [_vp, _vp, _vp, _sz]
+    L.nwg_evaluate.argtypes = [_vp, C.POINTER(RuntimeWordCounts), C.POINTER(ShardReleaseHistory)]
+    L.nwg_read_summary.argtypes = [_vp, C.POINTER(FitnessSummary)]
+    L.nwg_read_evaluation_stats.argtypes = [_vp, C.POINTER(EvaluationStats)]
+    L.nwg_advance.argtypes = [_vp, C.c_uint32, C.POINTER(RuntimeWordCounts), C.POINTER(AssemblyConfig),
+                              C.POINTER(PendingInjection), POST_FITNESS_FN, _vp, SHARD_RELEASE_FN, _vp,
+                              C.POINTER(ShardReleaseHistory)]
+    L.nwg_swap_generations.argtypes = [_vp]
+    L.nwg_read_status.argtypes = [_vp, C.POINTER(C.c_int)]
+    L.nwg_download_current_generation.argtypes = [_vp, _vp, _vp, _vp, _vp, _sz, C.POINTER(_sz), C.POINTER(_sz)]
+    L.nwg_download_slot.argtypes = [_vp, C.c_uint32, _vp, _sz, C.POINTER(_sz)]
+    L.nwg_upload_slot.argtypes = [_vp, C.c_uint32, _vp, _sz]
+    L.nwg_upload_current_generation.argtypes = [_vp, _vp, _sz, _sz]
+    L.nwg_download_assembly_plan.argtypes = [_vp, _vp, _sz, C.POINTER(_sz)]
+    L.nwg_device_slab.argtypes = [_vp, C.POINTER(_vp), C.POINTER(_sz)]
+    L.nwg_evaluate_traced.argtypes = [_vp, C.POINTER(RuntimeWordCounts), C.POINTER(ShardReleaseHistory), _sz, _vp,
+                                      _vp, _vp, _vp]
+    L.nwg_select_parents_device.argtypes = [_vp, _vp, _sz, _sz, _sz, _sz, C.POINTER(ParentSelectionConfig),
+                                            C.c_uint32, _vp, _vp]
+    L.nwg_breed_device.argtypes = [_vp, _sz, _vp, _vp, _sz, _vp, _sz, _sz, C.c_uint32, _sz,
+                                   C.POINTER(BreedingConfig), C.POINTER(MutationConfig), _vp]
+    L.nwg_bootstrap_device.argtypes = [_vp, _sz, _sz, _sz, C.c_uint32, _sz, _vp]
+    return L
+
+
+def status_string(status: int) -> str:
+    return lib().nwg_status_string(status).decode()
+
+
+def check(status: int, where: str) -> None:
+    if status != 0:
+        raise NwgError(status, where)
+
+
+def _np_ptr(a: np.ndarray | None):
+    if a is None:
+        return None
+    assert a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data
+
+
+def genome_stride_bytes(action_count: int) -> int:
+    """Reference genome image size (genetic_algorithm/genome/dynamic_layout.hpp:30-36)."""
+    return 0 if action_count == 0 else ((301056 + 76 * action_count + 1) // 2) * 2
+
+
+def upload_catalog(letters: np.ndarray) -> None:
+    letters = np.ascontiguousarray(letters, np.uint8).reshape(-1, 5)
+    check(lib().nwg_upload_catalog(_np_ptr(letters), len(letters)), "nwg_upload_catalog")
+
+
+def word_counts(training: int, action_space: int, initial: int | None = None, step: int = 0, period: int = 1,
+                initial_radius: int = 0, growth_period: int = 2) -> RuntimeWordCounts:
+    wc = RuntimeWordCounts()
+    wc.training_word_count = training
+    wc.action_space_word_count = action_space
+    wc.training_word_schedule.initial_word_count = training if initial is None else initial
+    wc.training_word_schedule.word_count_step = step
+    wc.training_word_schedule.word_count_step_period_generations = period
+    wc.shard_initial_radius = initial_radius
+    wc.shard_radius_growth_period_generations = growth_period
+    return wc
+
+
+def assembly_config(radius=2, rank_exponent=0.5, l1=0.02, l2=0.01, l3=0.005, p=1e-4, sigma=0.02,
+                    row_scale=0.0) -> AssemblyConfig:
+    cfg = AssemblyConfig()
+    cfg.parent_selection.cellular_breeding_radius = radius
+    cfg.parent_selection.rank_exponent = rank_exponent
+    cfg.breeding.crossover_temperature_level1 = l1
+    cfg.breeding.crossover_temperature_level2 = l2
+    cfg.breeding.crossover_temperature_level3 = l3
+    cfg.mutation.mutation_probability = p
+    cfg.mutation.mutation_sigma = sigma
+    cfg.mutation.output_tail_row_scale_mutation_probability = row_scale
+    return cfg
+
+
+class Runtime:
+    """One device GA runtime (DeviceSlabGARuntimeBuffers of the reference)."""
+
+    def __init__(self, action_count: int, population: int, columns: int, slab_generations: float = 2.0,
+                 stream: int | None = None):
+        stride = genome_stride_bytes(action_count)
+        cfg = RuntimeConfig()
+        cfg.generation_byte_budget_bytes = population * stride
+        cfg.genotype_slab_byte_budget_bytes = int(slab_generations * population) * stride
+        cfg.host_spillover_byte_budget_bytes = 0
+        cfg.action_count = action_count
+        cfg.population_size_ceiling = population
+        cfg.grid_column_count = columns
+        handle = _vp()
+        check(lib().nwg_create(C.byref(cfg), C.byref(handle)), "nwg_create")
+        self.handle = handle
+        self.action_count = action_count
+        self.population = population
+        self.columns = columns
+        self._keep = []
+        if stream is not None:
+            self.set_stream(stream)
+
+    def close(self):
+        if self.handle:
+            lib().nwg_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream: int) -> None:
+        check(lib().nwg_set_stream(self.handle, stream), "nwg_set_stream")
+
+    def info(self) -> RuntimeInfo:
+        info = RuntimeInfo()
+        check(lib().nwg_get_info(self.handle, C.byref(info)), "nwg_get_info")
+        return info
+
+    def bootstrap(self, size: int, seed: int, generation_index: int = 0) -> None:
+        check(lib().nwg_bootstrap(self.handle, size, seed, generation_index), "nwg_bootstrap")
+
+    def set_cell_words(self, offsets: np.ndarray | None, words: np.ndarray | None) -> None:
+        if offsets is None:
+            check(lib().nwg_set_cell_words(self.handle, None, None, 0), "nwg_set_cell_words")
+            return
+        offsets = np.ascontiguousarray(offsets, np.uint32)
+        words = np.ascontiguousarray(words, np.uint32)
+        check(lib().nwg_set_cell_words(self.handle, _np_ptr(offsets), _np_ptr(words), len(offsets) - 1),
+              "nwg_set_cell_words")
+
+    def evaluate(self, counts: RuntimeWordCounts, history: ShardReleaseHistory | None = None) -> None:
+        check(lib().nwg_evaluate(self.handle, C.byref(counts), C.byref(history) if history else None),
+              "nwg_evaluate")
+
+    def evaluate_traced(self, counts, trace_episodes, choices=0, turns=0, scores=0, policy=0, history=None) -> None:
+        check(lib().nwg_evaluate_traced(self.handle, C.byref(counts), C.byref(history) if history else None,
+                                        trace_episodes, choices or None, turns or None, scores or None,
+                                        policy or None), "nwg_evaluate_traced")
+
+    def summary(self) -> FitnessSummary:
+        s = FitnessSummary()
+        check(lib().nwg_read_summary(self.handle, C.byref(s)), "nwg_read_summary")
+        return s
+
+    def stats(self) -> EvaluationStats:
+        s = EvaluationStats()
+        check(lib().nwg_read_evaluation_stats(self.handle, C.byref(s)), "nwg_read_evaluation_stats")
+        return s
+
+    def advance(self, seed: int, counts: RuntimeWordCounts, config: AssemblyConfig | None = None,
+                pending: PendingInjection | None = None, post_fitness=None, shard_release=None,
+                history: ShardReleaseHistory | None = None) -> None:
+        pf = POST_FITNESS_FN(post_fitness) if post_fitness else POST_FITNESS_FN()
+        sr = SHARD_RELEASE_FN(shard_release) if shard_release else SHARD_RELEASE_FN()
+        check(lib().nwg_advance(self.handle, seed, C.byref(counts), C.byref(config) if config else None,
+                                C.byref(pending) if pending else None, pf, None, sr, None,
+                                C.byref(history) if history else None), "nwg_advance")
+
+    def status(self) -> int:
+        v = C.c_int()
+        check(lib().nwg_read_status(self.handle, C.byref(v)), "nwg_read_status")
+        return v.value
+
+    def current_generation(self):
+        n = self.population
+        slots = np.zeros(n, np.uint32)
+        fitness = np.zeros(n, np.float32)
+        evals = np.zeros(n, np.uint32)
+        has = np.zeros(n, np.uint8)
+        count = _sz()
+        gen = _sz()
+        check(lib().nwg_download_current_generation(self.handle, _np_ptr(slots), _np_ptr(fitness), _np_ptr(evals),
+                                                    _np_ptr(has), n, C.byref(count), C.byref(gen)),
+              "nwg_download_current_generation")
+        k = count.value
+        return dict(slots=slots[:k], fitness=fitness[:k], evaluation_counts=evals[:k], has_fitness=has[:k],
+                    generation_index=gen.value)
+
+    def download_slot(self, slot: int) -> np.ndarray:
+        out = np.zeros(genome_stride_bytes(self.action_count), np.uint8)
+        n = _sz()
+        check(lib().nwg_download_slot(self.handle, slot, _np_ptr(out), out.nbytes, C.byref(n)), "nwg_download_slot")
+        return out
+
+    def upload_slot(self, slot: int, image: np.ndarray) -> None:
+        image = np.ascontiguousarray(image).view(np.uint8)
+        check(lib().nwg_upload_slot(self.handle, slot, _np_ptr(image), image.nbytes), "nwg_upload_slot")
+
+    def upload_current_generation(self, slots: np.ndarray, generation_index: int = 0) -> None:
+        slots = np.ascontiguousarray(slots, np.uint32)
+        check(lib().nwg_upload_current_generation(self.handle, _np_ptr(slots), len(slots), generation_index),
+              "nwg_upload_current_generation")
+
+    def assembly_plan(self) -> np.ndarray:
+        out = np.zeros(2 * self.population, np.uint32)
+        n = _sz()
+        check(lib().nwg_download_assembly_plan(self.handle, _np_ptr(out), len(out), C.byref(n)),
+              "nwg_download_assembly_plan")
+        return out[:2 * n.value].reshape(-1, 2)
+
+    def device_slab(self):
+        ptr = _vp()
+        pitch = _sz()
+        check(lib().nwg_device_slab(self.handle, C.byref(ptr), C.byref(pitch)), "nwg_device_slab")
+        return ptr.value, pitch.value

@@ -1,0 +1,359 @@
+// Child assembly: hierarchical crossover plus Philox-driven mutation, one warp per child.
+//
+// Replaces AssembleChildBatchKernel (genotype_slab/device_runtime.cu:448-516), whose single thread per
+// child walked BreedAndMutateGenome (genetic_algorithm/device/genome_ops.cuh:386-407) byte by byte.
+// Here a warp assembles a child:
+//   1. the crossover decisions are drawn from the child's stream (seed, uint32(child + g * 4099))
+//      in the reference's order (genome_ops.cuh:264-299, :344-376);
+//   2. the donor layers and tail rows are copied with coalesced 128-bit loads and stores, then the
+//      single-neuron / single-row / splice overrides are applied;
+//   3. the per-value mutation stream (genome_ops.cuh:153-167, :237-257) is walked 128 draw positions
+//      at a time: each lane computes four consecutive uniforms, a ballot finds the hits, the hit list
+//      is resolved in order (a fresh normal pair consumes two more draw positions and leaves its
+//      second value cached for the next hit, as the generator's normal does), and the lanes then apply
+//      the hits' normals in parallel.
+// Every uniform, 32-bit draw and normal is produced by the toolkit generator itself (curand_init at the
+// draw's position, then curand_uniform / curand / curand_normal), so the child image is bit-identical
+// to the reference's serial walk.
+#include <cuda_fp16.h>
+#include <curand_kernel.h>
+
+#include "nwg_internal.cuh"
+
+namespace nwg {
+namespace {
+
+constexpr int kBreedWarps = 8;
+constexpr int kEventCapacity = 128;
+
+struct LayerSpan {
+    int weights;
+    int biases;
+    int fan_in;
+    int outputs;
+};
+
+__constant__ LayerSpan kLayers[5] = {
+    {kEncW1, kEncB1, kTurnFeatures, kEncoderHidden},
+    {kEncW2, kEncB2, kEncoderHidden, kEncoderOut},
+    {kTrW1, kTrB1, kModelInput, kHidden0},
+    {kTrW2, kTrB2, kHidden0, kHidden1},
+    {kTrW3, kTrB3, kHidden1, kPolicy},
+};
+
+struct Stream {
+    unsigned long long seed;
+    unsigned long long subsequence;
+    unsigned long long position;     // next 32-bit output to be consumed
+    unsigned long long cached_pair;  // position of the normal pair whose second value is cached
+    bool cached;
+};
+
+__device__ __forceinline__ curandStatePhilox4_32_10_t StateAt(const Stream &s, unsigned long long position) {
+    curandStatePhilox4_32_10_t state;
+    curand_init(s.seed, s.subsequence, position, &state);
+    return state;
+}
+
+// Sequential control draws (genome_ops.cuh:35-52); every lane computes the same values.
+__device__ bool DrawBernoulli(Stream &s, float p) {
+    if (p <= 0.0f) {
+        return false;
+    }
+    if (p >= 1.0f) {
+        return true;
+    }
+    curandStatePhilox4_32_10_t state = StateAt(s, s.position);
+    s.position += 1;
+    return curand_uniform(&state) < p;
+}
+
+__device__ std::uint32_t DrawIndex(Stream &s, std::uint32_t n) {
+    if (n <= 1) {
+        return 0;
+    }
+    curandStatePhilox4_32_10_t state = StateAt(s, s.position);
+    s.position += 1;
+    return curand(&state) % n;
+}
+
+struct EventList {
+    std::uint32_t value[kEventCapacity];
+    unsigned long long pair[kEventCapacity];
+    std::uint8_t second[kEventCapacity];
+};
+
+__device__ __forceinline__ int NextHit(unsigned long long lo, unsigned long long hi, int r) {
+    if (r < 64) {
+        const unsigned long long x = lo & (~0ull << r);
+        if (x) {
+            return __ffsll(static_cast<long long>(x)) - 1;
+        }
+        return hi ? 64 + __ffsll(static_cast<long long>(hi)) - 1 : 128;
+    }
+    if (r >= 128) {
+        return 128;
+    }
+    const unsigned long long x = hi & (~0ull << (r - 64));
+    return x ? 64 + __ffsll(static_cast<long long>(x)) - 1 : 128;
+}
+
+__device__ __forceinline__ void ApplyNormal(__half *values, std::uint32_t v, const Stream &s, unsigned long long pair,
+                                            bool second, float sigma) {
+    curandStatePhilox4_32_10_t state = StateAt(s, pair);
+    float n = curand_normal(&state);
+    if (second) {
+        n = curand_normal(&state);
+    }
+    values[v] = __float2half(__fmaf_rn(sigma, n, __half2float(values[v])));
+}
+
+// Per-value Bernoulli(p) mutation with sigma * N(0, 1) on hits, over values[0, count).
+// with_normals = false draws the Bernoulli uniforms but no normals (genome_ops.cuh:241-243 with sigma <= 0).
+__device__ void MutateRun(__half *values, std::uint32_t count, Stream &s, float p, float sigma, bool with_normals,
+                          EventList &ev, int lane) {
+    if (count == 0 || p <= 0.0f) {
+        return;
+    }
+    if (p >= 1.0f) {
+        // every value is a hit and no uniform is drawn
+        if (!with_normals) {
+            return;
+        }
+        const bool c0 = s.cached;
+        const unsigned long long base = s.position;
+        for (std::uint32_t k0 = 0; k0 < count; k0 += 32) {
+            const std::uint32_t k = k0 + lane;
+            if (k < count) {
+                if (c0 && k == 0) {
+                    ApplyNormal(values, k, s, s.cached_pair, true, sigma);
+                } else {
+                    const std::uint32_t j = c0 ? k - 1 : k;
+                    ApplyNormal(values, k, s, base + 2ull * (j / 2), (j & 1u) != 0, sigma);
+                }
+            }
+        }
+        const std::uint32_t fresh = c0 ? count - 1 : count;
+        const unsigned long long pairs = (fresh + 1) / 2;
+        s.position = base + 2ull * pairs;
+        s.cached = (fresh & 1u) != 0;
+        s.cached_pair = s.position - 2;
+        __syncwarp();
+        return;
+    }
+    std::uint32_t v = 0;
+    while (v < count) {
+        const unsigned long long window = s.position & ~3ull;
+        int r = static_cast<int>(s.position - window);
+        curandStatePhilox4_32_10_t state = StateAt(s, window + 4ull * lane);
+        const float u0 = curand_uniform(&state);
+        const float u1 = curand_uniform(&state);
+        const float u2 = curand_uniform(&state);
+        const float u3 = curand_uniform(&state);
+        const std::uint32_t nibble = (u0 < p ? 1u : 0u) | (u1 < p ? 2u : 0u) | (u2 < p ? 4u : 0u) |
+                                     (u3 < p ? 8u : 0u);
+        const std::uint32_t shifted = nibble << (4 * (lane & 7));
+        const std::uint32_t m0 = __reduce_or_sync(0xffffffffu, (lane >> 3) == 0 ? shifted : 0u);
+        const std::uint32_t m1 = __reduce_or_sync(0xffffffffu, (lane >> 3) == 1 ? shifted : 0u);
+        const std::uint32_t m2 = __reduce_or_sync(0xffffffffu, (lane >> 3) == 2 ? shifted : 0u);
+        const std::uint32_t m3 = __reduce_or_sync(0xffffffffu, (lane >> 3) == 3 ? shifted : 0u);
+        const unsigned long long lo = static_cast<unsigned long long>(m0) | (static_cast<unsigned long long>(m1) << 32);
+        const unsigned long long hi = static_cast<unsigned long long>(m2) | (static_cast<unsigned long long>(m3) << 32);
+        int n_events = 0;
+        while (v < count && r < 128) {
+            const int h = NextHit(lo, hi, r);
+            const std::uint32_t misses = static_cast<std::uint32_t>(h - r);
+            if (misses >= count - v) {
+                r += static_cast<int>(count - v);
+                v = count;
+                break;
+            }
+            v += misses;
+            r = h;
+            if (r >= 128) {
+                break;
+            }
+            // value v is hit at draw position window + r
+            if (with_normals) {
+                if (lane == 0) {
+                    ev.value[n_events] = v;
+                    ev.pair[n_events] = s.cached ? s.cached_pair : window + r + 1;
+                    ev.second[n_events] = s.cached ? 1 : 0;
+                }
+                ++n_events;
+                if (s.cached) {
+                    s.cached = false;
+                    r += 1;
+                } else {
+                    s.cached = true;
+                    s.cached_pair = window + r + 1;
+                    r += 3;
+                }
+            } else {
+                r += 1;
+            }
+            ++v;
+        }
+        s.position = window + r;
+        __syncwarp();
+        for (int e = lane; e < n_events; e += 32) {
+            ApplyNormal(values, ev.value[e], s, ev.pair[e], ev.second[e] != 0, sigma);
+        }
+        __syncwarp();
+    }
+}
+
+__device__ void CopyRegion(std::uint8_t *__restrict__ dst, const std::uint8_t *__restrict__ src, std::size_t bytes,
+                           int lane) {
+    const std::size_t n16 = bytes / 16;
+    uint4 *d = reinterpret_cast<uint4 *>(dst);
+    const uint4 *s = reinterpret_cast<const uint4 *>(src);
+    std::size_t i = lane;
+    for (; i + 96 < n16; i += 128) {
+        const uint4 a = s[i];
+        const uint4 b = s[i + 32];
+        const uint4 c = s[i + 64];
+        const uint4 e = s[i + 96];
+        d[i] = a;
+        d[i + 32] = b;
+        d[i + 64] = c;
+        d[i + 96] = e;
+    }
+    for (; i < n16; i += 32) {
+        d[i] = s[i];
+    }
+    const std::size_t halfs = bytes / 2;
+    std::uint16_t *d16 = reinterpret_cast<std::uint16_t *>(dst);
+    const std::uint16_t *s16 = reinterpret_cast<const std::uint16_t *>(src);
+    for (std::size_t k = n16 * 8 + lane; k < halfs; k += 32) {
+        d16[k] = s16[k];
+    }
+}
+
+__global__ void __launch_bounds__(kBreedWarps * 32) BreedKernel(const BreedParams p) {
+    __shared__ EventList events[kBreedWarps];
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const std::uint32_t child = blockIdx.x * kBreedWarps + warp;
+    if (child >= p.child_count) {
+        return;
+    }
+    EventList &ev = events[warp];
+    const std::uint32_t first_index = p.pairs[2 * child];
+    const std::uint32_t second_index = p.pairs[2 * child + 1];
+    const std::uint8_t *parent1 = p.parent_slab + static_cast<std::size_t>(p.parent_slots[first_index]) * p.parent_pitch;
+    const std::uint8_t *parent2 =
+        p.parent_slab + static_cast<std::size_t>(p.parent_slots[second_index]) * p.parent_pitch;
+    const std::uint32_t child_slot = p.child_slots != nullptr ? p.child_slots[child] : child;
+    std::uint8_t *out = p.child_slab + static_cast<std::size_t>(child_slot) * p.child_pitch;
+
+    Stream s;
+    s.seed = p.generation_seed;
+    s.subsequence = static_cast<std::uint32_t>(child + p.generation_index * 4099u);
+    s.position = 0;
+    s.cached = false;
+    s.cached_pair = 0;
+
+    // ---- policy recombination decisions (genome_ops.cuh:264-299, :210-221, :259-262) ----
+    bool from_first[5];
+    int neuron[5];
+    for (int group = 0; group < 2; ++group) {
+        const bool base_first = !DrawBernoulli(s, p.crossover_l1);
+        const int begin = group == 0 ? 0 : 2;
+        const int end = group == 0 ? 2 : 5;
+        for (int l = begin; l < end; ++l) {
+            from_first[l] = DrawBernoulli(s, p.crossover_l2) ? !base_first : base_first;
+            neuron[l] = DrawBernoulli(s, p.crossover_l3) ? static_cast<int>(DrawIndex(s, kLayers[l].outputs)) : -1;
+        }
+    }
+    for (int l = 0; l < 5; ++l) {
+        const LayerSpan layer = kLayers[l];
+        const std::size_t begin = static_cast<std::size_t>(layer.weights) * 2;
+        const std::size_t end = static_cast<std::size_t>(layer.biases + layer.outputs) * 2;
+        CopyRegion(out + begin, (from_first[l] ? parent1 : parent2) + begin, end - begin, lane);
+    }
+    __syncwarp();
+    for (int l = 0; l < 5; ++l) {
+        if (neuron[l] < 0) {
+            continue;
+        }
+        const LayerSpan layer = kLayers[l];
+        const __half *other = reinterpret_cast<const __half *>(from_first[l] ? parent2 : parent1);
+        __half *dst = reinterpret_cast<__half *>(out);
+        const int row = layer.weights + neuron[l] * layer.fan_in;
+        for (int k = lane; k < layer.fan_in; k += 32) {
+            dst[row + k] = other[row + k];
+        }
+        if (lane == 0) {
+            dst[layer.biases + neuron[l]] = other[layer.biases + neuron[l]];
+        }
+    }
+    __syncwarp();
+
+    // ---- policy mutation (genome_ops.cuh:153-167, :301-309): skipped entirely when p <= 0 or sigma <= 0 ----
+    __half *values = reinterpret_cast<__half *>(out);
+    if (p.mutation_probability > 0.0f && p.mutation_sigma > 0.0f) {
+        MutateRun(values, kPolicyHalfs, s, p.mutation_probability, p.mutation_sigma, true, ev, lane);
+    }
+
+    // ---- tail rows (genome_ops.cuh:344-376) ----
+    const std::uint32_t a_count = p.action_count;
+    const bool rows_first = !DrawBernoulli(s, p.crossover_l1);
+    CopyRegion(out + kTailOffsetBytes, (rows_first ? parent1 : parent2) + kTailOffsetBytes, a_count * kTailRowBytes,
+               lane);
+    __syncwarp();
+    const __half *t1 = reinterpret_cast<const __half *>(parent1 + kTailOffsetBytes);
+    const __half *t2 = reinterpret_cast<const __half *>(parent2 + kTailOffsetBytes);
+    __half *tc = reinterpret_cast<__half *>(out + kTailOffsetBytes);
+    bool has_swap = false;
+    std::uint32_t swap_index = 0;
+    if (a_count > 0 && DrawBernoulli(s, p.crossover_l2)) {
+        has_swap = true;
+        swap_index = DrawIndex(s, a_count);
+        const __half *src = rows_first ? t2 : t1;
+        for (int k = lane; k < kTailDim; k += 32) {
+            tc[swap_index * kTailDim + k] = src[swap_index * kTailDim + k];
+        }
+    }
+    __syncwarp();
+    if (a_count > 0 && DrawBernoulli(s, p.crossover_l3)) {
+        const std::uint32_t splice = DrawIndex(s, a_count);
+        const bool row_first = (has_swap && splice == swap_index) ? !rows_first : rows_first;
+        const std::uint32_t point = 1 + DrawIndex(s, kTailDim - 1);  // genome_ops.cuh:335-342
+        for (int k = lane; k < kTailDim; k += 32) {
+            const bool take_first = (static_cast<std::uint32_t>(k) < point) ? row_first : !row_first;
+            tc[splice * kTailDim + k] = take_first ? t1[splice * kTailDim + k] : t2[splice * kTailDim + k];
+        }
+    }
+    __syncwarp();
+
+    // ---- tail mutation (genome_ops.cuh:237-257, :378-384) ----
+    const bool with_normals = p.mutation_sigma > 0.0f;
+    if (p.row_scale_probability <= 0.0f) {
+        MutateRun(tc, a_count * kTailDim, s, p.mutation_probability, p.mutation_sigma, with_normals, ev, lane);
+    } else {
+        for (std::uint32_t row = 0; row < a_count; ++row) {
+            MutateRun(tc + row * kTailDim, kTailDim, s, p.mutation_probability, p.mutation_sigma, with_normals, ev,
+                      lane);
+            if (DrawBernoulli(s, p.row_scale_probability)) {
+                const float scale = DrawBernoulli(s, 0.5f) ? 1.02f : 0.98f;  // output_tail_ops.hpp:7-12
+                for (int k = lane; k < kTailDim; k += 32) {
+                    tc[row * kTailDim + k] = __float2half(__half2float(tc[row * kTailDim + k]) * scale);
+                }
+            }
+            __syncwarp();
+        }
+    }
+}
+
+}  // namespace
+
+cudaError_t LaunchBreed(const BreedParams &params, cudaStream_t stream) {
+    if (params.child_count == 0) {
+        return cudaSuccess;
+    }
+    BreedKernel<<<(params.child_count + kBreedWarps - 1) / kBreedWarps, kBreedWarps * 32, 0, stream>>>(params);
+    return cudaGetLastError();
+}
+
+}  // namespace nwg

@@ -1,0 +1,1004 @@
+// Host runtime behind the C ABI (include/nwg_capi.h).
+//
+// Mirrors the reference's device GA runtime (genetic_algorithm/device/slab_runtime.cu) at its public
+// entry points, with B200-first internals:
+//   - the slab is a planned slot array (no device free list, no spin lock, no host spill): the
+//     current generation's slots are fixed, and before assembly one kernel marks the parents the plan
+//     references and hands the remaining slots to the children in ascending order;
+//   - the whole generation (evaluate -> finalize -> summary -> select -> plan slots -> breed) is issued
+//     on the runtime's stream with no intermediate host synchronisation; the call synchronises once at
+//     the end and reads the sticky device status, which keeps the reference's "bool + status" contract.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <limits>
+#include <mutex>
+#include <new>
+#include <vector>
+
+#include "../../include/nwg_capi.h"
+#include "nwg_internal.cuh"
+
+using namespace nwg;
+
+namespace {
+
+constexpr std::size_t kMaxSizeT = std::numeric_limits<std::size_t>::max();
+
+struct Catalog {
+    std::uint32_t *codes = nullptr;  // device
+    float *fixed_t = nullptr;        // device [26][pad]
+    std::size_t count = 0;
+    std::size_t pad = 0;
+    int device = -1;
+};
+
+Catalog g_catalog;
+std::mutex g_catalog_mutex;
+
+}  // namespace
+
+struct nwg_runtime {
+    cudaStream_t stream = nullptr;
+    std::size_t action_count = 0;
+    std::size_t stride = 0;
+    std::size_t pitch = 0;
+    std::size_t slot_count = 0;
+    std::size_t max_generation_size = 0;
+    std::size_t grid_column_count = 0;
+    std::size_t generation_byte_budget = 0;
+    std::size_t slab_byte_budget = 0;
+    std::size_t host_spill_budget = 0;
+    std::size_t epicenter_rows = 0;
+
+    std::uint8_t *slab = nullptr;
+    std::uint32_t *cur_slots = nullptr, *next_slots = nullptr;
+    float *cur_fitness = nullptr, *next_fitness = nullptr;
+    std::uint32_t *cur_eval = nullptr, *next_eval = nullptr;
+    std::uint8_t *cur_has = nullptr, *next_has = nullptr;
+    std::uint32_t *pairs = nullptr;
+    std::uint8_t *slot_used = nullptr;
+    std::size_t cur_gen_index = 0, cur_gen_size = 0, next_gen_index = 0, next_gen_size = 0, planned_children = 0;
+
+    int *status = nullptr;
+    SummaryDevice *summary = nullptr;
+    ShardRecord *shards = nullptr;
+    std::size_t shard_count = 0;
+    std::uint32_t *cell_offsets = nullptr, *cell_words = nullptr;
+    std::size_t cell_count = 0, cell_word_capacity = 0;
+    std::uint32_t *local_words = nullptr, *chunk_start = nullptr, *score_sum = nullptr;
+    unsigned long long *steps = nullptr;
+    float *scratch = nullptr;
+    int scratch_ctas = 0;
+
+    // pinned host staging
+    ShardRecord *host_shards = nullptr;
+    int *host_status = nullptr;
+    SummaryDevice *host_summary = nullptr;
+    unsigned long long *host_steps = nullptr;  // [3]: decisions, encoded turns, episodes
+    cudaEvent_t eval_begin = nullptr;
+    cudaEvent_t eval_end = nullptr;
+    std::uint64_t last_episodes = 0;
+    std::size_t last_eval_population = 0;
+    std::size_t last_action_count = 0;
+    std::size_t last_eval_generation = 0;
+};
+
+namespace {
+
+#define NWG_TRY(expr)                                \
+    do {                                             \
+        if ((expr) != cudaSuccess) {                 \
+            return kCudaFailure;                     \
+        }                                            \
+    } while (0)
+
+// ---- byte budgets (genetic_algorithm/genome/dynamic_layout.hpp:38-54, spatial/grid.hpp:61-67) ----
+std::size_t SlotsForBudget(std::size_t budget, std::size_t action_count, std::size_t ceiling = 0) {
+    const std::size_t stride = GenomeStrideBytes(action_count);
+    if (stride == 0 || budget < stride) {
+        return 0;
+    }
+    const std::size_t n = budget / stride;
+    return (ceiling == 0 || n < ceiling) ? n : ceiling;
+}
+
+std::size_t FloorRows(std::size_t n, std::size_t cols) { return cols == 0 ? 0 : (n / cols) * cols; }
+
+// slab_runtime.hpp:50-60
+bool ValidConfig(const nwg_runtime_config &c) {
+    return c.genotype_slab_byte_budget_bytes >= c.generation_byte_budget_bytes && c.action_count > 0 &&
+           c.grid_column_count > 0 && (c.population_size_ceiling == 0 || c.population_size_ceiling % c.grid_column_count == 0) &&
+           SlotsForBudget(c.genotype_slab_byte_budget_bytes, c.action_count) > 0 &&
+           SlotsForBudget(c.generation_byte_budget_bytes, c.action_count, c.population_size_ceiling) / c.grid_column_count > 0;
+}
+
+// ---- training-data shard set (training_folder/training_data.hpp:73-117, :150-206, :251-316) ----
+bool ValidSchedule(const nwg_word_count_schedule &s) {
+    return s.initial_word_count > 0 && s.word_count_step_period_generations > 0;
+}
+
+std::size_t ShardCountForIntroduced(const nwg_word_count_schedule &s, std::size_t introduced) {
+    if (!ValidSchedule(s) || introduced == 0) {
+        return 0;
+    }
+    const std::size_t foundation = std::min(s.initial_word_count, introduced);
+    if (introduced == foundation) {
+        return 1;
+    }
+    if (s.word_count_step == 0) {
+        return 0;
+    }
+    return 1 + (introduced - foundation + s.word_count_step - 1) / s.word_count_step;
+}
+
+bool ValidHistoryFor(const nwg_word_count_schedule &s, std::size_t introduced, const nwg_shard_release_history &h) {
+    const std::size_t required = ShardCountForIntroduced(s, introduced);
+    if (required == 0 || h.release_count == 0 || h.release_count > NWG_CATALOG_CAPACITY) {
+        return false;
+    }
+    for (std::size_t i = 1; i < h.release_count; ++i) {
+        if (h.release_generations[i] <= h.release_generations[i - 1]) {
+            return false;
+        }
+    }
+    return h.release_count >= required;
+}
+
+std::size_t RadiusAtGeneration(std::size_t intro, std::size_t current, std::size_t initial, std::size_t period) {
+    if (period == 0 || current < intro) {
+        return 0;
+    }
+    const std::size_t steps = (current - intro) / period;
+    if (steps > kMaxSizeT - initial) {
+        return kMaxSizeT;
+    }
+    return initial + steps;
+}
+
+bool BuildShardSet(const nwg_runtime_word_counts &wc, std::size_t generation_index, std::size_t rows,
+                   std::size_t cols, std::size_t epicenter_rows, const nwg_shard_release_history *history,
+                   std::vector<ShardRecord> &out) {
+    out.clear();
+    const std::size_t introduced = wc.training_word_count;
+    const nwg_word_count_schedule &s = wc.training_word_schedule;
+    if (!ValidSchedule(s) || introduced == 0 || introduced > NWG_CATALOG_CAPACITY || rows == 0 || cols == 0 ||
+        epicenter_rows == 0 || wc.shard_radius_growth_period_generations == 0) {
+        return false;
+    }
+    if (history != nullptr && !ValidHistoryFor(s, introduced, *history)) {
+        return false;
+    }
+    const std::size_t foundation = std::min(s.initial_word_count, introduced);
+    out.push_back(ShardRecord{0, foundation, 0, 0, 0, 1});
+    if (s.word_count_step == 0 || foundation == introduced) {
+        return true;
+    }
+    std::size_t next = foundation;
+    std::size_t local = 0;
+    const std::size_t epicenter_cells = epicenter_rows * cols;
+    while (next < introduced) {
+        const std::size_t count = std::min(introduced - next, s.word_count_step);
+        const std::size_t history_index = out.size();
+        const std::size_t intro = history == nullptr ? (local + 1) * s.word_count_step_period_generations
+                                                     : history->release_generations[history_index];
+        // DeterministicTrainingShardCenterCoordinate: golden-ratio stride over the epicentre grid
+        const std::size_t cell =
+            static_cast<std::size_t>((static_cast<std::uint64_t>(local + 1) * 11400714819323198485ull) % epicenter_cells);
+        const std::size_t row = cell / cols;
+        const std::size_t col = cell % cols;
+        out.push_back(ShardRecord{next, count, std::min(row, rows - 1), col,
+                                  RadiusAtGeneration(intro, generation_index, wc.shard_initial_radius,
+                                                     wc.shard_radius_growth_period_generations),
+                                  0});
+        next += count;
+        ++local;
+    }
+    return true;
+}
+
+int Sync(nwg_runtime *rt) {
+    if (cudaMemcpyAsync(rt->host_status, rt->status, sizeof(int), cudaMemcpyDeviceToHost, rt->stream) != cudaSuccess ||
+        cudaStreamSynchronize(rt->stream) != cudaSuccess) {
+        return kCudaFailure;
+    }
+    return *rt->host_status;
+}
+
+int SetHostStatus(nwg_runtime *rt, int code) {
+    *rt->host_status = code;
+    cudaMemcpyAsync(rt->status, rt->host_status, sizeof(int), cudaMemcpyHostToDevice, rt->stream);
+    cudaStreamSynchronize(rt->stream);
+    return code;
+}
+
+__global__ void PlanChildSlotsKernel(const std::uint32_t *pairs, std::uint32_t child_count,
+                                     const std::uint32_t *parent_slots, std::uint32_t parent_count,
+                                     std::uint8_t *used, std::uint32_t slot_count, std::uint32_t *child_slots,
+                                     int *status) {
+    __shared__ std::uint32_t partial[1024];
+    __shared__ std::uint32_t base;
+    const std::uint32_t t = threadIdx.x;
+    for (std::uint32_t s = t; s < slot_count; s += blockDim.x) {
+        used[s] = 0;
+    }
+    __syncthreads();
+    for (std::uint32_t c = t; c < child_count; c += blockDim.x) {
+        const std::uint32_t a = pairs[2 * c];
+        const std::uint32_t b = pairs[2 * c + 1];
+        if (a >= parent_count || b >= parent_count || parent_slots[a] >= slot_count || parent_slots[b] >= slot_count) {
+            SetStatus(status, kInvalidParentIndex);
+            continue;
+        }
+        used[parent_slots[a]] = 1;
+        used[parent_slots[b]] = 1;
+    }
+    if (t == 0) {
+        base = 0;
+    }
+    __syncthreads();
+    for (std::uint32_t start = 0; start < slot_count; start += blockDim.x) {
+        const std::uint32_t s = start + t;
+        const std::uint32_t is_free = (s < slot_count && used[s] == 0) ? 1u : 0u;
+        partial[t] = is_free;
+        __syncthreads();
+        for (std::uint32_t off = 1; off < blockDim.x; off <<= 1) {
+            const std::uint32_t v = t >= off ? partial[t - off] : 0;
+            __syncthreads();
+            partial[t] += v;
+            __syncthreads();
+        }
+        const std::uint32_t index = base + partial[t] - is_free;
+        if (is_free && index < child_count) {
+            child_slots[index] = s;
+        }
+        __syncthreads();
+        if (t == blockDim.x - 1) {
+            base += partial[t];
+        }
+        __syncthreads();
+    }
+    if (t == 0 && base < child_count) {
+        SetStatus(status, kSlabFull);
+    }
+}
+
+void FreeRuntime(nwg_runtime *rt) {
+    if (rt == nullptr) {
+        return;
+    }
+    void *device_ptrs[] = {rt->slab,       rt->cur_slots,    rt->next_slots,  rt->cur_fitness, rt->next_fitness,
+                           rt->cur_eval,   rt->next_eval,    rt->cur_has,     rt->next_has,    rt->pairs,
+                           rt->slot_used,  rt->status,       rt->summary,     rt->shards,      rt->cell_offsets,
+                           rt->cell_words, rt->local_words,  rt->chunk_start, rt->score_sum,   rt->steps,
+                           rt->scratch};
+    for (void *p : device_ptrs) {
+        if (p != nullptr) {
+            cudaFree(p);
+        }
+    }
+    void *host_ptrs[] = {rt->host_shards, rt->host_status, rt->host_summary, rt->host_steps};
+    for (void *p : host_ptrs) {
+        if (p != nullptr) {
+            cudaFreeHost(p);
+        }
+    }
+    if (rt->eval_begin != nullptr) {
+        cudaEventDestroy(rt->eval_begin);
+    }
+    if (rt->eval_end != nullptr) {
+        cudaEventDestroy(rt->eval_end);
+    }
+    delete rt;
+}
+
+bool ValidWordCounts(const nwg_runtime_word_counts &wc, std::size_t catalog_count) {
+    // evaluation_ops.cuh:77-85
+    return wc.training_word_count <= catalog_count && wc.action_space_word_count <= catalog_count &&
+           wc.training_word_count <= wc.action_space_word_count && ValidSchedule(wc.training_word_schedule) &&
+           wc.shard_radius_growth_period_generations > 0;
+}
+
+int EvaluateImpl(nwg_runtime *rt, const nwg_runtime_word_counts *counts, const nwg_shard_release_history *history,
+                 std::size_t trace_episodes, void *choices, void *turns, void *scores, void *policy) {
+    if (rt == nullptr || counts == nullptr) {
+        return kInvalidRuntimeConfig;
+    }
+    if (rt->max_generation_size == 0 || rt->cur_gen_size == 0 || rt->cur_gen_size > rt->max_generation_size ||
+        rt->cur_gen_size % rt->grid_column_count != 0) {
+        return kInvalidGeneration;
+    }
+    NWG_TRY(cudaMemsetAsync(rt->status, 0, sizeof(int), rt->stream));
+    const std::size_t rows = rt->cur_gen_size / rt->grid_column_count;
+    const std::size_t cols = rt->grid_column_count;
+    const std::size_t selectable = std::min(rt->action_count, counts->action_space_word_count);
+    if (g_catalog.codes == nullptr || !ValidWordCounts(*counts, g_catalog.count) || selectable == 0) {
+        return SetHostStatus(rt, kInvalidTrainingShard);
+    }
+    WordSource src{};
+    src.rows = static_cast<std::uint32_t>(rows);
+    src.cols = static_cast<std::uint32_t>(cols);
+    if (rt->cell_count > 0) {
+        if (rt->cell_count != rt->cur_gen_size) {
+            return SetHostStatus(rt, kInvalidTrainingShard);
+        }
+        src.mode = 0;
+        src.cell_offsets = rt->cell_offsets;
+        src.cell_words = rt->cell_words;
+    } else {
+        std::vector<ShardRecord> set;
+        if (!BuildShardSet(*counts, rt->cur_gen_index, rows, cols, rt->epicenter_rows, history, set) ||
+            set.size() > NWG_CATALOG_CAPACITY) {
+            return SetHostStatus(rt, kInvalidTrainingShard);
+        }
+        std::memcpy(rt->host_shards, set.data(), set.size() * sizeof(ShardRecord));
+        NWG_TRY(cudaMemcpyAsync(rt->shards, rt->host_shards, set.size() * sizeof(ShardRecord), cudaMemcpyHostToDevice,
+                                rt->stream));
+        rt->shard_count = set.size();
+        src.mode = 1;
+        src.shards = rt->shards;
+        src.shard_count = static_cast<std::uint32_t>(set.size());
+    }
+    const std::uint32_t population = static_cast<std::uint32_t>(rt->cur_gen_size);
+    NWG_TRY(cudaMemsetAsync(rt->cur_fitness, 0, rt->max_generation_size * sizeof(float), rt->stream));
+    NWG_TRY(cudaMemsetAsync(rt->cur_eval, 0, rt->max_generation_size * sizeof(std::uint32_t), rt->stream));
+    NWG_TRY(cudaMemsetAsync(rt->cur_has, 0, rt->max_generation_size, rt->stream));
+    NWG_TRY(cudaMemsetAsync(rt->steps, 0, 3 * sizeof(unsigned long long), rt->stream));
+    NWG_TRY(LaunchEvalPrepare(src, population, static_cast<std::uint32_t>(g_catalog.count), rt->local_words,
+                              rt->chunk_start, rt->score_sum, rt->status, rt->stream));
+    EvalParams p{};
+    p.slab = rt->slab;
+    p.pitch = rt->pitch;
+    p.slot_of_individual = rt->cur_slots;
+    p.population = population;
+    p.action_count = static_cast<std::uint32_t>(selectable);
+    p.catalog_count = static_cast<std::uint32_t>(g_catalog.count);
+    p.codes = g_catalog.codes;
+    p.fixed_t = g_catalog.fixed_t;
+    p.action_pad = static_cast<std::uint32_t>(g_catalog.pad);
+    p.source = src;
+    p.chunk_start = rt->chunk_start;
+    p.local_words = rt->local_words;
+    p.scratch = rt->scratch;
+    p.score_sum = rt->score_sum;
+    p.steps = rt->steps;
+    p.status = rt->status;
+    p.trace_episodes = static_cast<std::uint32_t>(trace_episodes);
+    p.trace_choices = static_cast<std::int32_t *>(choices);
+    p.trace_turns = static_cast<std::int32_t *>(turns);
+    p.trace_scores = static_cast<float *>(scores);
+    p.trace_policy = static_cast<float *>(policy);
+    NWG_TRY(cudaEventRecord(rt->eval_begin, rt->stream));
+    NWG_TRY(LaunchEvalFp32(p, rt->scratch_ctas, rt->stream));
+    NWG_TRY(cudaEventRecord(rt->eval_end, rt->stream));
+    NWG_TRY(LaunchFinalizeFitness(rt->score_sum, rt->local_words, population, rt->cur_fitness, rt->cur_eval,
+                                  rt->cur_has, rt->status, rt->stream));
+    NWG_TRY(LaunchSummarize(rt->cur_fitness, rt->cur_has, rt->cur_slots, population, rt->summary, rt->status,
+                            rt->stream));
+    NWG_TRY(cudaMemcpyAsync(rt->host_summary, rt->summary, sizeof(SummaryDevice), cudaMemcpyDeviceToHost, rt->stream));
+    NWG_TRY(cudaMemcpyAsync(rt->host_steps, rt->steps, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                            rt->stream));
+    rt->last_eval_population = population;
+    rt->last_action_count = rt->action_count;
+    rt->last_eval_generation = rt->cur_gen_index;
+    return kOk;
+}
+
+}  // namespace
+
+extern "C" {
+
+int nwg_abi_version(void) { return NWG_ABI_VERSION; }
+
+const char *nwg_status_string(int status) {
+    switch (status) {
+    case NWG_OK: return "ok";
+    case NWG_CUDA_FAILURE: return "cuda failure";
+    case NWG_INVALID_RUNTIME_CONFIG: return "invalid slab ga runtime config";
+    case NWG_INVALID_SLAB: return "invalid slab state";
+    case NWG_INVALID_GENERATION: return "invalid generation state";
+    case NWG_INVALID_TRAINING_SHARD: return "invalid training-data shard";
+    case NWG_GUESS_APPEND_FAILED: return "could not append a model-selected guess to the Wordle grid";
+    case NWG_POLICY_FORWARD_FAILED: return "policy model forward pass failed";
+    case NWG_ACTION_SELECTION_FAILED: return "output-embedding action selection failed";
+    case NWG_POPULATION_NOT_EVALUATED:
+        return "population fitness summary requested before the population was fully evaluated";
+    case NWG_INVALID_ASSEMBLY_CONFIG: return "invalid next-generation assembly config";
+    case NWG_PARENT_SELECTION_FAILED: return "device parent selection failed";
+    case NWG_INVALID_ASSEMBLY_PLAN: return "invalid slab assembly plan";
+    case NWG_INVALID_PARENT_INDEX: return "invalid parent index in slab assembly plan";
+    case NWG_SLAB_FULL: return "slab is genuinely full";
+    case NWG_OUTPUT_EMBEDDING_INJECTION_FAILED: return "device output-embedding injection failed";
+    case NWG_SLAB_REPACK_FAILED: return "slab compaction/repacking failed";
+    case NWG_TIMEOUT: return "a bounded device wait gave up";
+    case NWG_UNSUPPORTED: return "request not supported by this runtime";
+    default: return "unknown slab ga runtime status";
+    }
+}
+
+int nwg_upload_catalog(const uint8_t *letters, size_t word_count) {
+    if (letters == nullptr || word_count == 0 || word_count > NWG_CATALOG_CAPACITY) {
+        return kInvalidTrainingShard;
+    }
+    for (std::size_t i = 0; i < word_count * kWordLength; ++i) {
+        if (letters[i] >= kAlphabet) {
+            return kInvalidTrainingShard;
+        }
+    }
+    std::lock_guard<std::mutex> lock(g_catalog_mutex);
+    const std::size_t pad = ((word_count + 127) / 128) * 128;
+    std::vector<std::uint32_t> codes(pad, 0);
+    std::vector<float> fixed(static_cast<std::size_t>(kFixedDim) * pad, 0.0f);
+    for (std::size_t w = 0; w < word_count; ++w) {
+        codes[w] = PackWord(letters + kWordLength * w);
+        int counts[kAlphabet] = {0};
+        for (int p = 0; p < kWordLength; ++p) {
+            ++counts[letters[kWordLength * w + p]];
+        }
+        // output_embedding.hpp:59-73: letter count, or -1 when the letter is absent
+        for (int l = 0; l < kFixedDim; ++l) {
+            fixed[static_cast<std::size_t>(l) * pad + w] = counts[l] == 0 ? -1.0f : static_cast<float>(counts[l]);
+        }
+    }
+    if (g_catalog.codes != nullptr) {
+        cudaFree(g_catalog.codes);
+        cudaFree(g_catalog.fixed_t);
+        g_catalog = Catalog{};
+    }
+    if (cudaMalloc(&g_catalog.codes, pad * sizeof(std::uint32_t)) != cudaSuccess ||
+        cudaMalloc(&g_catalog.fixed_t, fixed.size() * sizeof(float)) != cudaSuccess ||
+        cudaMemcpy(g_catalog.codes, codes.data(), pad * sizeof(std::uint32_t), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(g_catalog.fixed_t, fixed.data(), fixed.size() * sizeof(float), cudaMemcpyHostToDevice) !=
+            cudaSuccess) {
+        return kCudaFailure;
+    }
+    g_catalog.count = word_count;
+    g_catalog.pad = pad;
+    cudaGetDevice(&g_catalog.device);
+    return kOk;
+}
+
+int nwg_create(const nwg_runtime_config *config, nwg_runtime **runtime_out) {
+    if (runtime_out == nullptr) {
+        return kInvalidRuntimeConfig;
+    }
+    *runtime_out = nullptr;
+    if (config == nullptr || !ValidConfig(*config)) {
+        return kInvalidRuntimeConfig;
+    }
+    const std::size_t slot_count = SlotsForBudget(config->genotype_slab_byte_budget_bytes, config->action_count);
+    const std::size_t max_gen = FloorRows(
+        SlotsForBudget(config->generation_byte_budget_bytes, config->action_count, config->population_size_ceiling),
+        config->grid_column_count);
+    if (slot_count < max_gen || max_gen == 0 || slot_count >= 0xFFFFFFFFull) {
+        return kInvalidRuntimeConfig;
+    }
+    nwg_runtime *rt = new (std::nothrow) nwg_runtime();
+    if (rt == nullptr) {
+        return kInvalidRuntimeConfig;
+    }
+    rt->action_count = config->action_count;
+    rt->stride = GenomeStrideBytes(config->action_count);
+    rt->pitch = SlotPitchBytes(config->action_count);
+    rt->slot_count = slot_count;
+    rt->max_generation_size = max_gen;
+    rt->grid_column_count = config->grid_column_count;
+    rt->generation_byte_budget = max_gen * rt->stride;
+    rt->slab_byte_budget = config->genotype_slab_byte_budget_bytes;
+    rt->host_spill_budget = config->host_spillover_byte_budget_bytes;
+    rt->epicenter_rows = max_gen / config->grid_column_count;
+    rt->scratch_ctas = EvalCtaCount(0xFFFFFFFFu);
+    bool ok = true;
+    auto alloc = [&](auto **ptr, std::size_t bytes) {
+        ok = ok && cudaMalloc(reinterpret_cast<void **>(ptr), bytes) == cudaSuccess;
+        if (ok) {
+            ok = cudaMemset(*ptr, 0, bytes) == cudaSuccess;
+        }
+    };
+    alloc(&rt->slab, slot_count * rt->pitch);
+    alloc(&rt->cur_slots, max_gen * sizeof(std::uint32_t));
+    alloc(&rt->next_slots, max_gen * sizeof(std::uint32_t));
+    alloc(&rt->cur_fitness, max_gen * sizeof(float));
+    alloc(&rt->next_fitness, max_gen * sizeof(float));
+    alloc(&rt->cur_eval, max_gen * sizeof(std::uint32_t));
+    alloc(&rt->next_eval, max_gen * sizeof(std::uint32_t));
+    alloc(&rt->cur_has, max_gen);
+    alloc(&rt->next_has, max_gen);
+    alloc(&rt->pairs, max_gen * 2 * sizeof(std::uint32_t));
+    alloc(&rt->slot_used, slot_count);
+    alloc(&rt->status, sizeof(int));
+    alloc(&rt->summary, sizeof(SummaryDevice));
+    alloc(&rt->shards, NWG_CATALOG_CAPACITY * sizeof(ShardRecord));
+    alloc(&rt->local_words, max_gen * sizeof(std::uint32_t));
+    alloc(&rt->chunk_start, (max_gen + 1) * sizeof(std::uint32_t));
+    alloc(&rt->score_sum, max_gen * sizeof(std::uint32_t));
+    alloc(&rt->steps, 3 * sizeof(unsigned long long));
+    alloc(&rt->scratch, static_cast<std::size_t>(rt->scratch_ctas) * EvalScratchFloatsPerCta() * sizeof(float));
+    ok = ok && cudaMallocHost(&rt->host_shards, NWG_CATALOG_CAPACITY * sizeof(ShardRecord)) == cudaSuccess;
+    ok = ok && cudaMallocHost(&rt->host_status, sizeof(int)) == cudaSuccess;
+    ok = ok && cudaMallocHost(&rt->host_summary, sizeof(SummaryDevice)) == cudaSuccess;
+    ok = ok && cudaMallocHost(&rt->host_steps, 3 * sizeof(unsigned long long)) == cudaSuccess;
+    ok = ok && cudaEventCreate(&rt->eval_begin) == cudaSuccess && cudaEventCreate(&rt->eval_end) == cudaSuccess;
+    if (!ok) {
+        FreeRuntime(rt);
+        return kCudaFailure;
+    }
+    std::memset(rt->host_summary, 0, sizeof(SummaryDevice));
+    std::memset(rt->host_steps, 0, 3 * sizeof(unsigned long long));
+    *runtime_out = rt;
+    return kOk;
+}
+
+void nwg_destroy(nwg_runtime *runtime) {
+    if (runtime != nullptr) {
+        cudaStreamSynchronize(runtime->stream);
+    }
+    FreeRuntime(runtime);
+}
+
+int nwg_set_stream(nwg_runtime *runtime, void *cuda_stream) {
+    if (runtime == nullptr) {
+        return kInvalidRuntimeConfig;
+    }
+    runtime->stream = static_cast<cudaStream_t>(cuda_stream);
+    return kOk;
+}
+
+int nwg_get_info(const nwg_runtime *rt, nwg_runtime_info *info) {
+    if (rt == nullptr || info == nullptr) {
+        return kInvalidRuntimeConfig;
+    }
+    info->action_count = rt->action_count;
+    info->slot_stride_bytes = rt->stride;
+    info->slot_pitch_bytes = rt->pitch;
+    info->slot_count = rt->slot_count;
+    info->max_generation_size = rt->max_generation_size;
+    info->grid_column_count = rt->grid_column_count;
+    info->current_generation_index = rt->cur_gen_index;
+    info->current_generation_size = rt->cur_gen_size;
+    return kOk;
+}
+
+int nwg_bootstrap(nwg_runtime *rt, size_t generation_size, uint32_t generation_seed, size_t generation_index) {
+    if (rt == nullptr) {
+        return kInvalidRuntimeConfig;
+    }
+    if (generation_size == 0 || generation_size > rt->max_generation_size ||
+        generation_size % rt->grid_column_count != 0) {
+        return kInvalidGeneration;
+    }
+    std::vector<std::uint32_t> slots(generation_size);
+    for (std::size_t i = 0; i < generation_size; ++i) {
+        slots[i] = static_cast<std::uint32_t>(i);
+    }
+    NWG_TRY(cudaMemcpyAsync(rt->cur_slots, slots.data(), generation_size * sizeof(std::uint32_t),
+                            cudaMemcpyHostToDevice, rt->stream));
+    NWG_TRY(cudaMemsetAsync(rt->cur_fitness, 0, rt->max_generation_size * sizeof(float), rt->stream));
+    NWG_TRY(cudaMemsetAsync(rt->cur_eval, 0, rt->max_generation_size * sizeof(std::uint32_t), rt->stream));
+    NWG_TRY(cudaMemsetAsync(rt->cur_has, 0, rt->max_generation_size, rt->stream));
+    NWG_TRY(cudaMemsetAsync(rt->status, 0, sizeof(int), rt->stream));
+    NWG_TRY(cudaMemsetAsync(rt->summary, 0, sizeof(SummaryDevice), rt->stream));
+    NWG_TRY(LaunchBootstrap(rt->slab, rt->pitch, rt->cur_slots, static_cast<std::uint32_t>(generation_size),
+                            generation_index, generation_seed, static_cast<std::uint32_t>(rt->action_count),
+                            rt->stream));
+    const int st = Sync(rt);
+    if (st != kOk) {
+        rt->cur_gen_size = 0;
+        return st;
+    }
+    rt->cur_gen_index = generation_index;
+    rt->cur_gen_size = generation_size;
+    rt->next_gen_index = 0;
+    rt->next_gen_size = 0;
+    rt->planned_children = 0;
+    return kOk;
+}
+
+int nwg_set_cell_words(nwg_runtime *rt, const uint32_t *offsets, const uint32_t *words, size_t cell_count) {
+    if (rt == nullptr) {
+        return kInvalidRuntimeConfig;
+    }
+    if (cell_count == 0) {
+        rt->cell_count = 0;
+        return kOk;
+    }
+    if (offsets == nullptr || words == nullptr || cell_count > rt->max_generation_size || offsets[0] != 0) {
+        return kInvalidTrainingShard;
+    }
+    for (std::size_t c = 0; c < cell_count; ++c) {
+        if (offsets[c + 1] < offsets[c] || offsets[c + 1] == offsets[c]) {
+            return kInvalidTrainingShard;
+        }
+    }
+    const std::size_t total = offsets[cell_count];
+    if (rt->cell_offsets == nullptr || rt->cell_word_capacity < total) {
+        if (rt->cell_words != nullptr) {
+            cudaFree(rt->cell_words);
+            rt->cell_words = nullptr;
+        }
+        if (rt->cell_offsets == nullptr) {
+            NWG_TRY(cudaMalloc(&rt->cell_offsets, (rt->max_generation_size + 1) * sizeof(std::uint32_t)));
+        }
+        NWG_TRY(cudaMalloc(&rt->cell_words, total * sizeof(std::uint32_t)));
+        rt->cell_word_capacity = total;
+    }
+    NWG_TRY(cudaMemcpyAsync(rt->cell_offsets, offsets, (cell_count + 1) * sizeof(std::uint32_t),
+                            cudaMemcpyHostToDevice, rt->stream));
+    NWG_TRY(cudaMemcpyAsync(rt->cell_words, words, total * sizeof(std::uint32_t), cudaMemcpyHostToDevice, rt->stream));
+    NWG_TRY(cudaStreamSynchronize(rt->stream));
+    rt->cell_count = cell_count;
+    return kOk;
+}
+
+int nwg_evaluate(nwg_runtime *rt, const nwg_runtime_word_counts *counts, const nwg_shard_release_history *history) {
+    const int st = EvaluateImpl(rt, counts, history, 0, nullptr, nullptr, nullptr, nullptr);
+    if (st != kOk) {
+        return st;
+    }
+    return Sync(rt);
+}
+
+int nwg_evaluate_traced(nwg_runtime *rt, const nwg_runtime_word_counts *counts,
+                        const nwg_shard_release_history *history, size_t trace_episodes, void *choices, void *turns,
+                        void *scores, void *policy) {
+    const int st = EvaluateImpl(rt, counts, history, trace_episodes, choices, turns, scores, policy);
+    if (st != kOk) {
+        return st;
+    }
+    return Sync(rt);
+}
+
+int nwg_read_summary(const nwg_runtime *rt, nwg_fitness_summary *summary) {
+    if (rt == nullptr || summary == nullptr) {
+        return kInvalidRuntimeConfig;
+    }
+    summary->best_fitness = rt->host_summary->best_fitness;
+    summary->average_fitness = rt->host_summary->average_fitness;
+    summary->best_index = rt->host_summary->best_index;
+    summary->best_slot_index = rt->host_summary->best_slot_index;
+    summary->generation_index = rt->last_eval_generation;
+    summary->action_count = rt->last_action_count;
+    summary->population_size = rt->last_eval_population;
+    return kOk;
+}
+
+int nwg_read_evaluation_stats(const nwg_runtime *rt, nwg_evaluation_stats *stats) {
+    if (rt == nullptr || stats == nullptr) {
+        return kInvalidRuntimeConfig;
+    }
+    stats->game_steps = rt->host_steps[0];
+    stats->encoded_turns = rt->host_steps[1];
+    stats->episodes = rt->host_steps[2];
+    stats->fitness_mean_fp64 = rt->host_summary->mean_fp64;
+    stats->fitness_variance_fp64 = rt->host_summary->variance_fp64;
+    float ms = 0.0f;
+    stats->eval_kernel_ms = cudaEventElapsedTime(&ms, rt->eval_begin, rt->eval_end) == cudaSuccess ? ms : -1.0;
+    return kOk;
+}
+
+int nwg_advance(nwg_runtime *rt, uint32_t generation_seed, const nwg_runtime_word_counts *counts,
+                const nwg_generation_assembly_config *config, const nwg_pending_injection *pending,
+                nwg_post_fitness_fn post_fitness, void *post_fitness_user, nwg_shard_release_fn shard_release,
+                void *shard_release_user, const nwg_shard_release_history *history) {
+    if (rt == nullptr || counts == nullptr) {
+        return kInvalidRuntimeConfig;
+    }
+    nwg_generation_assembly_config cfg{};
+    cfg.parent_selection.cellular_breeding_radius = 2;  // selection.hpp:13-18, spatial/grid.hpp:11
+    cfg.parent_selection.rank_exponent = 0.5f;
+    cfg.breeding = {0.02f, 0.01f, 0.005f};              // breeding.hpp:6-14
+    cfg.mutation = {0.0001f, 0.02f, 0.0f};              // mutation.hpp:7-15
+    if (config != nullptr) {
+        cfg = *config;
+    }
+    nwg_pending_injection injection{};
+    if (pending != nullptr) {
+        injection = *pending;
+    }
+    // generation_assembly.hpp:15-19
+    const auto in01 = [](float v) { return v >= 0.0f && v <= 1.0f; };
+    const bool valid = cfg.parent_selection.cellular_breeding_radius > 0 && cfg.parent_selection.rank_exponent >= 0.0f &&
+                       cfg.parent_selection.rank_exponent <= 4.0f && in01(cfg.breeding.crossover_temperature_level1) &&
+                       in01(cfg.breeding.crossover_temperature_level2) &&
+                       in01(cfg.breeding.crossover_temperature_level3) && in01(cfg.mutation.mutation_probability) &&
+                       cfg.mutation.mutation_sigma >= 0.0f &&
+                       in01(cfg.mutation.output_tail_row_scale_mutation_probability);
+    if (!valid) {
+        return SetHostStatus(rt, kInvalidAssemblyConfig);
+    }
+    int st = EvaluateImpl(rt, counts, history, 0, nullptr, nullptr, nullptr, nullptr);
+    if (st != kOk) {
+        return st;
+    }
+    if (shard_release != nullptr || post_fitness != nullptr) {
+        st = Sync(rt);
+        if (st != kOk) {
+            return st;
+        }
+    }
+    if (shard_release != nullptr && !shard_release(rt, counts, &injection, shard_release_user)) {
+        return SetHostStatus(rt, kInvalidAssemblyConfig);
+    }
+    if (injection.enabled) {
+        // action-space growth (output-embedding injection with widening repack) is not built yet
+        return SetHostStatus(rt, kUnsupported);
+    }
+    // slab_runtime.cu:919-939: next population from the generation byte budget at the next width
+    std::size_t next_size = FloorRows(SlotsForBudget(rt->generation_byte_budget, rt->action_count,
+                                                     rt->max_generation_size),
+                                      rt->grid_column_count);
+    next_size = std::min(next_size, rt->cur_gen_size);
+    if (next_size == 0) {
+        return SetHostStatus(rt, kInvalidAssemblyConfig);
+    }
+    SelectParams sp{};
+    sp.fitness = rt->cur_fitness;
+    sp.has_fitness = rt->cur_has;
+    sp.rows = static_cast<std::uint32_t>(rt->cur_gen_size / rt->grid_column_count);
+    sp.cols = static_cast<std::uint32_t>(rt->grid_column_count);
+    sp.child_count = static_cast<std::uint32_t>(next_size);
+    sp.generation_index = rt->cur_gen_index;
+    sp.radius = cfg.parent_selection.cellular_breeding_radius;
+    sp.rank_exponent = cfg.parent_selection.rank_exponent;
+    sp.planning_seed = generation_seed ^ 0xA341316Cu;  // slab_runtime.cu:1443
+    sp.pairs = rt->pairs;
+    sp.status = rt->status;
+    NWG_TRY(LaunchSelect(sp, rt->stream));
+    rt->planned_children = next_size;
+    if (post_fitness != nullptr) {
+        st = Sync(rt);
+        if (st != kOk) {
+            return st;
+        }
+        if (!post_fitness(rt, counts, post_fitness_user)) {
+            return SetHostStatus(rt, kInvalidAssemblyConfig);
+        }
+    }
+    PlanChildSlotsKernel<<<1, 1024, 0, rt->stream>>>(rt->pairs, static_cast<std::uint32_t>(next_size), rt->cur_slots,
+                                                     static_cast<std::uint32_t>(rt->cur_gen_size), rt->slot_used,
+                                                     static_cast<std::uint32_t>(rt->slot_count), rt->next_slots,
+                                                     rt->status);
+    NWG_TRY(cudaGetLastError());
+    BreedParams bp{};
+    bp.parent_slab = rt->slab;
+    bp.parent_pitch = rt->pitch;
+    bp.parent_slots = rt->cur_slots;
+    bp.child_slab = rt->slab;
+    bp.child_pitch = rt->pitch;
+    bp.child_slots = rt->next_slots;
+    bp.pairs = rt->pairs;
+    bp.child_count = static_cast<std::uint32_t>(next_size);
+    bp.action_count = static_cast<std::uint32_t>(rt->action_count);
+    bp.generation_seed = generation_seed;
+    bp.generation_index = rt->cur_gen_index;
+    bp.crossover_l1 = cfg.breeding.crossover_temperature_level1;
+    bp.crossover_l2 = cfg.breeding.crossover_temperature_level2;
+    bp.crossover_l3 = cfg.breeding.crossover_temperature_level3;
+    bp.mutation_probability = cfg.mutation.mutation_probability;
+    bp.mutation_sigma = cfg.mutation.mutation_sigma;
+    bp.row_scale_probability = cfg.mutation.output_tail_row_scale_mutation_probability;
+    bp.status = rt->status;
+    NWG_TRY(LaunchBreed(bp, rt->stream));
+    NWG_TRY(cudaMemsetAsync(rt->next_fitness, 0, rt->max_generation_size * sizeof(float), rt->stream));
+    NWG_TRY(cudaMemsetAsync(rt->next_eval, 0, rt->max_generation_size * sizeof(std::uint32_t), rt->stream));
+    NWG_TRY(cudaMemsetAsync(rt->next_has, 0, rt->max_generation_size, rt->stream));
+    st = Sync(rt);
+    if (st != kOk) {
+        return st;
+    }
+    rt->next_gen_index = rt->cur_gen_index + 1;
+    rt->next_gen_size = next_size;
+    return nwg_swap_generations(rt);
+}
+
+int nwg_swap_generations(nwg_runtime *rt) {
+    if (rt == nullptr) {
+        return kInvalidRuntimeConfig;
+    }
+    std::swap(rt->cur_slots, rt->next_slots);
+    std::swap(rt->cur_fitness, rt->next_fitness);
+    std::swap(rt->cur_eval, rt->next_eval);
+    std::swap(rt->cur_has, rt->next_has);
+    std::swap(rt->cur_gen_index, rt->next_gen_index);
+    std::swap(rt->cur_gen_size, rt->next_gen_size);
+    return kOk;
+}
+
+int nwg_read_status(const nwg_runtime *rt, int *status) {
+    if (rt == nullptr || status == nullptr) {
+        return kInvalidRuntimeConfig;
+    }
+    int value = 0;
+    if (cudaMemcpy(&value, rt->status, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) {
+        return kCudaFailure;
+    }
+    *status = value;
+    return kOk;
+}
+
+int nwg_download_current_generation(const nwg_runtime *rt, uint32_t *slot_indices, float *fitness,
+                                    uint32_t *evaluation_counts, uint8_t *has_fitness, size_t capacity,
+                                    size_t *count_out, size_t *generation_index_out) {
+    if (rt == nullptr || rt->cur_gen_size == 0 || capacity < rt->cur_gen_size) {
+        return kInvalidGeneration;
+    }
+    cudaStreamSynchronize(rt->stream);
+    const std::size_t n = rt->cur_gen_size;
+    if ((slot_indices && cudaMemcpy(slot_indices, rt->cur_slots, n * 4, cudaMemcpyDeviceToHost) != cudaSuccess) ||
+        (fitness && cudaMemcpy(fitness, rt->cur_fitness, n * 4, cudaMemcpyDeviceToHost) != cudaSuccess) ||
+        (evaluation_counts && cudaMemcpy(evaluation_counts, rt->cur_eval, n * 4, cudaMemcpyDeviceToHost) != cudaSuccess) ||
+        (has_fitness && cudaMemcpy(has_fitness, rt->cur_has, n, cudaMemcpyDeviceToHost) != cudaSuccess)) {
+        return kCudaFailure;
+    }
+    if (count_out) {
+        *count_out = n;
+    }
+    if (generation_index_out) {
+        *generation_index_out = rt->cur_gen_index;
+    }
+    return kOk;
+}
+
+int nwg_download_slot(const nwg_runtime *rt, uint32_t slot_index, uint8_t *bytes, size_t capacity,
+                      size_t *byte_count_out) {
+    if (rt == nullptr || bytes == nullptr || slot_index >= rt->slot_count || capacity < rt->stride) {
+        return kInvalidSlab;
+    }
+    cudaStreamSynchronize(rt->stream);
+    if (cudaMemcpy(bytes, rt->slab + static_cast<std::size_t>(slot_index) * rt->pitch, rt->stride,
+                   cudaMemcpyDeviceToHost) != cudaSuccess) {
+        return kCudaFailure;
+    }
+    if (byte_count_out) {
+        *byte_count_out = rt->stride;
+    }
+    return kOk;
+}
+
+int nwg_upload_slot(nwg_runtime *rt, uint32_t slot_index, const uint8_t *bytes, size_t byte_count) {
+    if (rt == nullptr || bytes == nullptr || slot_index >= rt->slot_count || byte_count != rt->stride) {
+        return kInvalidSlab;
+    }
+    cudaStreamSynchronize(rt->stream);
+    if (cudaMemcpy(rt->slab + static_cast<std::size_t>(slot_index) * rt->pitch, bytes, byte_count,
+                   cudaMemcpyHostToDevice) != cudaSuccess) {
+        return kCudaFailure;
+    }
+    return kOk;
+}
+
+int nwg_upload_current_generation(nwg_runtime *rt, const uint32_t *slot_indices, size_t count,
+                                  size_t generation_index) {
+    if (rt == nullptr || slot_indices == nullptr || count == 0 || count > rt->max_generation_size ||
+        count % rt->grid_column_count != 0) {
+        return kInvalidGeneration;
+    }
+    for (std::size_t i = 0; i < count; ++i) {
+        if (slot_indices[i] >= rt->slot_count) {
+            return kInvalidGeneration;
+        }
+    }
+    cudaStreamSynchronize(rt->stream);
+    if (cudaMemcpy(rt->cur_slots, slot_indices, count * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemset(rt->cur_fitness, 0, rt->max_generation_size * 4) != cudaSuccess ||
+        cudaMemset(rt->cur_eval, 0, rt->max_generation_size * 4) != cudaSuccess ||
+        cudaMemset(rt->cur_has, 0, rt->max_generation_size) != cudaSuccess) {
+        return kCudaFailure;
+    }
+    rt->cur_gen_size = count;
+    rt->cur_gen_index = generation_index;
+    return kOk;
+}
+
+int nwg_download_assembly_plan(const nwg_runtime *rt, uint32_t *pairs, size_t capacity, size_t *count_out) {
+    if (rt == nullptr || pairs == nullptr || capacity < rt->planned_children) {
+        return kInvalidAssemblyPlan;
+    }
+    cudaStreamSynchronize(rt->stream);
+    if (cudaMemcpy(pairs, rt->pairs, rt->planned_children * 2 * sizeof(std::uint32_t), cudaMemcpyDeviceToHost) !=
+        cudaSuccess) {
+        return kCudaFailure;
+    }
+    if (count_out) {
+        *count_out = rt->planned_children;
+    }
+    return kOk;
+}
+
+int nwg_device_slab(const nwg_runtime *rt, void **slab_out, size_t *pitch_out) {
+    if (rt == nullptr || slab_out == nullptr || pitch_out == nullptr) {
+        return kInvalidRuntimeConfig;
+    }
+    *slab_out = rt->slab;
+    *pitch_out = rt->pitch;
+    return kOk;
+}
+
+int nwg_select_parents_device(const float *fitness, const uint8_t *has_fitness, size_t population, size_t columns,
+                              size_t child_count, size_t generation_index, const nwg_parent_selection_config *config,
+                              uint32_t planning_seed, uint32_t *pairs, void *cuda_stream) {
+    if (fitness == nullptr || has_fitness == nullptr || pairs == nullptr || config == nullptr || columns == 0 ||
+        population % columns != 0 || child_count % columns != 0 || child_count > population ||
+        config->cellular_breeding_radius == 0) {
+        return kInvalidAssemblyConfig;
+    }
+    int *status = nullptr;
+    if (cudaMalloc(&status, sizeof(int)) != cudaSuccess) {
+        return kCudaFailure;
+    }
+    cudaStream_t stream = static_cast<cudaStream_t>(cuda_stream);
+    cudaMemsetAsync(status, 0, sizeof(int), stream);
+    SelectParams sp{};
+    sp.fitness = fitness;
+    sp.has_fitness = has_fitness;
+    sp.rows = static_cast<std::uint32_t>(population / columns);
+    sp.cols = static_cast<std::uint32_t>(columns);
+    sp.child_count = static_cast<std::uint32_t>(child_count);
+    sp.generation_index = generation_index;
+    sp.radius = config->cellular_breeding_radius;
+    sp.rank_exponent = config->rank_exponent;
+    sp.planning_seed = planning_seed;
+    sp.pairs = pairs;
+    sp.status = status;
+    int host_status = kCudaFailure;
+    if (LaunchSelect(sp, stream) == cudaSuccess &&
+        cudaMemcpyAsync(&host_status, status, sizeof(int), cudaMemcpyDeviceToHost, stream) == cudaSuccess) {
+        cudaStreamSynchronize(stream);
+    }
+    cudaFree(status);
+    return host_status;
+}
+
+int nwg_breed_device(const void *parent_slab, size_t parent_pitch, const uint32_t *parent_slots, void *child_slab,
+                     size_t child_pitch, const uint32_t *pairs, size_t child_count, size_t action_count,
+                     uint32_t generation_seed, size_t generation_index, const nwg_breeding_config *breeding,
+                     const nwg_mutation_config *mutation, void *cuda_stream) {
+    if (parent_slab == nullptr || child_slab == nullptr || parent_slots == nullptr || pairs == nullptr ||
+        breeding == nullptr || mutation == nullptr || parent_pitch % 16 != 0 || child_pitch % 16 != 0 ||
+        parent_pitch < GenomeStrideBytes(action_count) || child_pitch < GenomeStrideBytes(action_count)) {
+        return kInvalidAssemblyConfig;
+    }
+    BreedParams bp{};
+    bp.parent_slab = static_cast<const std::uint8_t *>(parent_slab);
+    bp.parent_pitch = parent_pitch;
+    bp.parent_slots = parent_slots;
+    bp.child_slab = static_cast<std::uint8_t *>(child_slab);
+    bp.child_pitch = child_pitch;
+    bp.child_slots = nullptr;
+    bp.pairs = pairs;
+    bp.child_count = static_cast<std::uint32_t>(child_count);
+    bp.action_count = static_cast<std::uint32_t>(action_count);
+    bp.generation_seed = generation_seed;
+    bp.generation_index = generation_index;
+    bp.crossover_l1 = breeding->crossover_temperature_level1;
+    bp.crossover_l2 = breeding->crossover_temperature_level2;
+    bp.crossover_l3 = breeding->crossover_temperature_level3;
+    bp.mutation_probability = mutation->mutation_probability;
+    bp.mutation_sigma = mutation->mutation_sigma;
+    bp.row_scale_probability = mutation->output_tail_row_scale_mutation_probability;
+    bp.status = nullptr;
+    cudaStream_t stream = static_cast<cudaStream_t>(cuda_stream);
+    if (LaunchBreed(bp, stream) != cudaSuccess || cudaStreamSynchronize(stream) != cudaSuccess) {
+        return kCudaFailure;
+    }
+    return kOk;
+}
+
+int nwg_bootstrap_device(void *slab, size_t pitch, size_t population, size_t generation_index, uint32_t seed,
+                         size_t action_count, void *cuda_stream) {
+    if (slab == nullptr || pitch < GenomeStrideBytes(action_count) || pitch % 2 != 0) {
+        return kInvalidRuntimeConfig;
+    }
+    cudaStream_t stream = static_cast<cudaStream_t>(cuda_stream);
+    if (LaunchBootstrap(static_cast<std::uint8_t *>(slab), pitch, nullptr, static_cast<std::uint32_t>(population),
+                        generation_index, seed, static_cast<std::uint32_t>(action_count), stream) != cudaSuccess ||
+        cudaStreamSynchronize(stream) != cudaSuccess) {
+        return kCudaFailure;
+    }
+    return kOk;
+}
+
+}  // extern "C"

@@ -1,0 +1,143 @@
+// Internal kernel interfaces of the runtime (not part of the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+#include "nwg_layout.cuh"
+
+namespace nwg {
+
+// Status codes: the reference's DeviceSlabGARuntimeStatusCode values
+// (genetic_algorithm/device/slab_runtime.hpp:21-39) followed by this runtime's additions.
+enum Status : int {
+    kOk = 0,
+    kCudaFailure = 1,
+    kInvalidRuntimeConfig = 2,
+    kInvalidSlab = 3,
+    kInvalidGeneration = 4,
+    kInvalidTrainingShard = 5,
+    kGuessAppendFailed = 6,
+    kPolicyForwardFailed = 7,
+    kActionSelectionFailed = 8,
+    kPopulationNotEvaluated = 9,
+    kInvalidAssemblyConfig = 10,
+    kParentSelectionFailed = 11,
+    kInvalidAssemblyPlan = 12,
+    kInvalidParentIndex = 13,
+    kSlabFull = 14,
+    kOutputEmbeddingInjectionFailed = 15,
+    kSlabRepackFailed = 16,
+    kTimeout = 17,
+    kUnsupported = 18,
+};
+
+__device__ inline void SetStatus(int *status, int code) { atomicCAS(status, 0, code); }
+
+// Where each cell's local training words come from: the reference shard set
+// (training_data.hpp:251-316) or an explicit per-cell list (CSR).
+struct WordSource {
+    int mode;  // 0: CSR lists, 1: shard records
+    const std::uint32_t *cell_offsets;
+    const std::uint32_t *cell_words;
+    const ShardRecord *shards;
+    std::uint32_t shard_count;
+    std::uint32_t rows;
+    std::uint32_t cols;
+};
+
+// ---- fitness evaluation (plain FP32 form) ----
+constexpr int kEvalThreads = 256;
+constexpr int kChunkGames = 128;
+
+struct EvalParams {
+    const std::uint8_t *slab;
+    std::size_t pitch;
+    const std::uint32_t *slot_of_individual;
+    std::uint32_t population;
+    std::uint32_t action_count;       // selectable actions
+    std::uint32_t catalog_count;
+    const std::uint32_t *codes;       // packed catalog words
+    const float *fixed_t;             // [26][action_pad] fixed word features
+    std::uint32_t action_pad;
+    WordSource source;
+    const std::uint32_t *chunk_start; // [population + 1]; chunk_start[population] = total chunks
+    const std::uint32_t *local_words; // [population]
+    float *scratch;                   // per CTA: kChunkGames x 256 layer-1 accumulators
+    std::uint32_t *score_sum;         // [population]
+    unsigned long long *steps;        // [0] policy decisions, [1] turns encoded, [2] episodes
+    int *status;
+    // optional trace (null when unused)
+    std::int32_t *trace_choices;      // [population * trace_episodes * 6]
+    std::int32_t *trace_turns;        // [population * trace_episodes]
+    float *trace_scores;              // [population * trace_episodes]
+    float *trace_policy;              // [population * trace_episodes * 6 * 64]
+    std::uint32_t trace_episodes;
+};
+
+std::size_t EvalScratchFloatsPerCta();
+int EvalCtaCount(std::uint32_t total_chunks);
+cudaError_t LaunchEvalPrepare(const WordSource &source, std::uint32_t population, std::uint32_t catalog_count,
+                              std::uint32_t *local_words, std::uint32_t *chunk_start, std::uint32_t *score_sum,
+                              int *status, cudaStream_t stream);
+cudaError_t LaunchEvalFp32(const EvalParams &params, int cta_count, cudaStream_t stream);
+cudaError_t LaunchFinalizeFitness(const std::uint32_t *score_sum, const std::uint32_t *local_words,
+                                  std::uint32_t population, float *fitness, std::uint32_t *evaluation_counts,
+                                  std::uint8_t *has_fitness, int *status, cudaStream_t stream);
+
+struct SummaryDevice {
+    float best_fitness;
+    float average_fitness;
+    std::uint64_t best_index;
+    std::uint32_t best_slot_index;
+    std::uint32_t pad;
+    double mean_fp64;
+    double variance_fp64;
+};
+
+cudaError_t LaunchSummarize(const float *fitness, const std::uint8_t *has_fitness, const std::uint32_t *slots,
+                            std::uint32_t population, SummaryDevice *out, int *status, cudaStream_t stream);
+
+// ---- selection ----
+struct SelectParams {
+    const float *fitness;
+    const std::uint8_t *has_fitness;
+    std::uint32_t rows;
+    std::uint32_t cols;
+    std::uint32_t child_count;
+    std::uint64_t generation_index;
+    std::uint64_t radius;
+    float rank_exponent;
+    std::uint32_t planning_seed;
+    std::uint32_t *pairs;  // [child_count * 2]
+    int *status;
+};
+cudaError_t LaunchSelect(const SelectParams &params, cudaStream_t stream);
+
+// ---- breeding ----
+struct BreedParams {
+    const std::uint8_t *parent_slab;
+    std::size_t parent_pitch;
+    const std::uint32_t *parent_slots;  // slot of each current individual
+    std::uint8_t *child_slab;
+    std::size_t child_pitch;
+    const std::uint32_t *child_slots;   // slot of each child (null: child i at slot i)
+    const std::uint32_t *pairs;
+    std::uint32_t child_count;
+    std::uint32_t action_count;
+    std::uint32_t generation_seed;
+    std::uint64_t generation_index;
+    float crossover_l1, crossover_l2, crossover_l3;
+    float mutation_probability, mutation_sigma, row_scale_probability;
+    int *status;
+};
+cudaError_t LaunchBreed(const BreedParams &params, cudaStream_t stream);
+
+// ---- bootstrap ----
+cudaError_t LaunchBootstrap(std::uint8_t *slab, std::size_t pitch, const std::uint32_t *slots,
+                            std::uint32_t population, std::uint64_t generation_index, std::uint32_t seed,
+                            std::uint32_t action_count, cudaStream_t stream);
+
+}  // namespace nwg
