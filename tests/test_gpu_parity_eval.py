@@ -27,7 +27,7 @@ def _run_reference(slab_ptr, pitch, population, columns, action_count, shards, e
     status = t.zeros(1, dtype=t.int32, device="cuda")
     arr = (O.ShardRecord * len(shards))(*shards)
     ok = O.ref_dev().refdev_evaluate(slab_ptr, pitch, population, columns, action_count, O.C.cast(arr, O.C.c_void_p),
-                                     len(shards), episodes, choices.data_ptr(), turns.data_ptr(), scores.data_ptr(),
+                                     len(shards), episodes, scores.data_ptr(), turns.data_ptr(), choices.data_ptr(),
                                      policy.data_ptr(), status.data_ptr(), G.stream_handle())
     assert ok == 1
     t.cuda.synchronize()
