@@ -156,7 +156,7 @@ def run_ours(args) -> None:
 
     rank, world, local = dist_setup(args.gpus)
     nwg = importlib.import_module("neuroevolutionary-wordle_b200")
-    wl = nwg.workload.FULL if args.workload == "full" else nwg.workload.SMALL
+    wl = {"full": nwg.workload.FULL, "medium": nwg.workload.MEDIUM, "small": nwg.workload.SMALL}[args.workload]
     catalog = wl.catalog()
     offsets, words = wl.cell_lists()
     nwg.capi.upload_catalog(catalog)
@@ -291,7 +291,7 @@ def run_reference(args) -> None:
     from oracle import pyoracle as O
 
     nwg_workload = importlib.import_module("neuroevolutionary-wordle_b200.workload")
-    wl = nwg_workload.FULL if args.workload == "full" else nwg_workload.SMALL
+    wl = {"full": nwg_workload.FULL, "medium": nwg_workload.MEDIUM, "small": nwg_workload.SMALL}[args.workload]
     if O.ref_host() is None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref_host.so was not built"}))
         return
@@ -339,7 +339,7 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["full", "small"], default="full")
+    ap.add_argument("--workload", choices=["full", "medium", "small"], default="full")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":

@@ -44,7 +44,7 @@ def test_advance_builds_local_plan_and_new_generation():
     rt.advance(seed=42, counts=counts, config=cfg)
     plan = rt.assembly_plan()
     rows, cols = 4, 4
-    for child, (a, b) in enumerate(plan):
+    for child, (a, b) in enumerate(plan.astype(np.int64)):
         assert a != b
         for parent in (a, b):
             dr = min(abs(child // cols - parent // cols), rows - abs(child // cols - parent // cols))
