@@ -86,3 +86,5 @@ class Workload:
 SMALL = Workload("p64_a512_s64", 64, 8, 512, 256, 64)
 # P=4096 on 64x64, 4,739 words, 256 secrets per cell from a 2,315-word subset.
 FULL = Workload("p4096_a4739_s256", 4096, 64, 4739, 2315, 256)
+# The same per-individual work on 256 individuals (16x16): a profiling case whose slab (170 MB) still exceeds L2.
+MEDIUM = Workload("p256_a4739_s256", 256, 16, 4739, 2315, 256)
