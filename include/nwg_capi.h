@@ -249,6 +249,25 @@ int nwg_breed_device(const void *parent_slab, size_t parent_pitch, const uint32_
 int nwg_bootstrap_device(void *slab, size_t pitch, size_t population, size_t generation_index, uint32_t seed,
                          size_t action_count, void *cuda_stream);
 
+/* Fitness evaluation that allocates no device memory. No counterpart in the reference.
+ * For callers that cannot call cudaMalloc: work being captured into a CUDA graph (an allocation would
+ * break the capture), embedders whose device memory belongs to another allocator or pool, and processes
+ * that keep a fixed device-memory footprint after start-up. Every pointer is a device pointer the caller
+ * owns: the slab (individual i's genome image at slab + slot_indices[i] * slot_pitch), the catalog as
+ * rows of 5 letter indices, the per-cell word lists in CSR form (catalog indices), and the outputs
+ * fitness[population] and, when not NULL, counters[3] (game steps, encoded turns, episodes). The
+ * selectable actions are catalog words [0, action_count). Everything else lives in one fixed array of
+ * 4,789,760 bytes inside the library, which every GPU that loads the library holds until the process
+ * exits; it limits population to 4,096 and the catalog to 4,739 words (NWG_UNSUPPORTED beyond). All
+ * calls share that array and it keeps the last call's contents, so calls that overlap on the GPU (other
+ * streams or host threads) race and must be serialised by the caller. The first call on each device
+ * resolves the array's device address; make that first call before any stream capture. The call
+ * synchronises its stream and returns the evaluation status. */
+int nwg_evaluate_noalloc(const void *slab, size_t slot_pitch, const uint32_t *slot_indices, size_t population,
+                         size_t grid_column_count, size_t action_count, const uint8_t *catalog_letters,
+                         size_t catalog_count, const uint32_t *cell_offsets, const uint32_t *cell_words,
+                         float *fitness, uint64_t *counters, void *cuda_stream);
+
 #ifdef __cplusplus
 }
 #endif
