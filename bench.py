@@ -30,6 +30,9 @@ sys.path.insert(0, str(ROOT))
 MEASURED = ROOT / "MEASURED_PEAKS.json"
 TRAFFIC = ROOT / "profiles" / "eval_fp32_traffic.json"
 KERNELS_PER_GENERATION = 7  # prepare, evaluate, finalize, summarize, select, plan slots, breed
+FORMS = {"fp32": 0, "tc-bf16": 1, "tc-fp16": 2}
+FORM_NAMES = {"fp32": "plain fp32", "tc-bf16": "tensor-core bf16 scoring, exact fp32 re-scoring",
+              "tc-fp16": "tensor-core fp16 scoring, exact fp32 re-scoring"}
 
 
 def algorithmic_flops(steps: int, encoded: int, action_count: int) -> float:
@@ -163,6 +166,7 @@ def run_ours(args) -> None:
     stream = torch.cuda.current_stream()
     rt = nwg.Runtime(wl.action_count, wl.population, wl.columns, stream=stream.cuda_stream)
     rt.set_cell_words(offsets, words)
+    rt.set_form(FORMS[args.form])
     rt.bootstrap(wl.population, seed=0 + rank)
     counts = nwg.capi.word_counts(training=wl.action_count, action_space=wl.action_count)
     cfg = nwg.capi.assembly_config(radius=wl.radius, p=wl.mutation_probability, sigma=wl.mutation_sigma)
@@ -191,6 +195,8 @@ def run_ours(args) -> None:
     steps = 0
     encoded = 0
     kernel_ms = []
+    rescored = 0
+    full = 0
     barrier(world)
     torch.cuda.synchronize()
     with ClockSampler(local) as clocks:
@@ -201,6 +207,8 @@ def run_ours(args) -> None:
             steps += st.game_steps
             encoded += st.encoded_turns
             kernel_ms.append(st.eval_kernel_ms)
+            rescored += st.rescored_chunks
+            full += st.full_rescores
             gen += 1
         end.record(stream)
         torch.cuda.synchronize()
@@ -263,7 +271,7 @@ def run_ours(args) -> None:
                    f"{wl.columns}", "action_count": wl.action_count, "secrets_per_cell": wl.secrets_per_cell,
                    "secret_subset": wl.secret_subset, "episodes_per_secret": 3, "selection_radius": wl.radius,
                    "mutation_probability": wl.mutation_probability, "mutation_sigma": wl.mutation_sigma,
-                   "form": "plain fp32", "parallelism": f"{world} independent populations (one per GPU)",
+                   "form": FORM_NAMES[args.form], "parallelism": f"{world} independent populations (one per GPU)",
                    "l2": "inputs larger than L2 (genome slab "
                          f"{wl.population * nwg.capi.genome_stride_bytes(wl.action_count) / 1e9:.2f} GB)"},
         "roofline": {"kernel": "EvalFp32Kernel", "bound": "fp32", "achieved": achieved_tflops,
@@ -277,7 +285,8 @@ def run_ours(args) -> None:
         "e2e": {"value": e2e_total / (e2e_ms * 1e-3), "unit": "game-steps/s",
                 "h2d_bytes_per_step": int(offsets.nbytes + words.nbytes + 120),
                 "d2h_bytes_per_step": 4 + 48 + 24},
-        "gpu_launches": KERNELS_PER_GENERATION * args.steps,
+        "gpu_launches": (KERNELS_PER_GENERATION + (1 if args.form != "fp32" else 0)) * args.steps,
+        "rescoring": {"chunks_per_step": rescored / max(steps, 1), "full_rescore_fraction": full / max(steps, 1)},
         "clocks": clock,
     }
     print(json.dumps(line), flush=True)
@@ -341,6 +350,7 @@ def main() -> None:
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["full", "medium", "small"], default="full")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--form", choices=sorted(FORMS), default="fp32")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -139,7 +139,16 @@ typedef struct {
     double fitness_mean_fp64;   /* FP64 reductions for the adaptive shard-release statistics */
     double fitness_variance_fp64;
     double eval_kernel_ms;      /* device time of the last evaluation kernel (CUDA events on the runtime's stream) */
+    uint64_t rescored_chunks;   /* tensor-core form: 32-action chunks re-scored exactly in FP32 */
+    uint64_t full_rescores;     /* tensor-core form: game steps re-scored over every action */
 } nwg_evaluation_stats;
+
+/* Evaluation forms (nwg_set_evaluation_form). */
+enum {
+    NWG_FORM_FP32 = 0,          /* plain form: every score an FP32 fused-multiply-add chain (default) */
+    NWG_FORM_TC_BF16 = 1,       /* scores on tcgen05 with BF16 operands, near-top chunks re-scored in FP32 */
+    NWG_FORM_TC_FP16 = 2,       /* as above with FP16 operands (tighter bound, fewer re-scored chunks) */
+};
 
 typedef struct {
     size_t action_count;
@@ -174,6 +183,12 @@ void nwg_destroy(nwg_runtime *runtime);
 int nwg_set_stream(nwg_runtime *runtime, void *cuda_stream);
 
 int nwg_get_info(const nwg_runtime *runtime, nwg_runtime_info *info);
+
+/* Selects how nwg_evaluate / nwg_advance score actions (NWG_FORM_*). No reference counterpart. Both tensor-core
+ * forms keep the FP32 trunk, score on tcgen05 and re-score in FP32 every 32-action chunk within a proven error
+ * bound of the best, so their guesses equal the plain form's; they keep a 16-bit embedding table per
+ * individual on the device (about 128 bytes per action). */
+int nwg_set_evaluation_form(nwg_runtime *runtime, int form);
 
 /* TryBootstrapRandomCurrentGenerationOnDevice (slab_runtime.hpp:123-124). */
 int nwg_bootstrap(nwg_runtime *runtime, size_t generation_size, uint32_t generation_seed, size_t generation_index);

@@ -77,7 +77,10 @@ class PendingInjection(C.Structure):
 class EvaluationStats(C.Structure):
     _fields_ = [("game_steps", C.c_uint64), ("episodes", C.c_uint64), ("encoded_turns", C.c_uint64),
                 ("fitness_mean_fp64", C.c_double), ("fitness_variance_fp64", C.c_double),
-                ("eval_kernel_ms", C.c_double)]
+                ("eval_kernel_ms", C.c_double), ("rescored_chunks", C.c_uint64), ("full_rescores", C.c_uint64)]
+
+
+FORM_FP32, FORM_TC_BF16, FORM_TC_FP16 = 0, 1, 2
 
 
 class RuntimeInfo(C.Structure):
@@ -91,7 +94,7 @@ SHARD_RELEASE_FN = C.CFUNCTYPE(C.c_bool, _vp, C.POINTER(RuntimeWordCounts), C.PO
 
 EXPORTS = [
     "nwg_abi_version", "nwg_status_string", "nwg_upload_catalog", "nwg_create", "nwg_destroy", "nwg_set_stream",
-    "nwg_get_info", "nwg_bootstrap", "nwg_set_cell_words", "nwg_evaluate", "nwg_read_summary",
+    "nwg_get_info", "nwg_set_evaluation_form", "nwg_bootstrap", "nwg_set_cell_words", "nwg_evaluate", "nwg_read_summary",
     "nwg_read_evaluation_stats", "nwg_advance", "nwg_swap_generations", "nwg_read_status",
     "nwg_download_current_generation", "nwg_download_slot", "nwg_upload_slot", "nwg_upload_current_generation",
     "nwg_download_assembly_plan", "nwg_device_slab", "nwg_evaluate_traced", "nwg_select_parents_device",
@@ -113,6 +116,7 @@ def lib() -> C.CDLL:
     L.nwg_set_stream.argtypes = [_vp, _vp]
     L.nwg_get_info.argtypes = [_vp, C.POINTER(RuntimeInfo)]
     L.nwg_bootstrap.argtypes = [_vp, _sz, C.c_uint32, _sz]
+    L.nwg_set_evaluation_form.argtypes = [_vp, C.c_int]
     L.nwg_set_cell_words.argtypes = [_vp, _vp, _vp, _sz]
     L.nwg_evaluate.argtypes = [_vp, C.POINTER(RuntimeWordCounts), C.POINTER(ShardReleaseHistory)]
     L.nwg_read_summary.argtypes = [_vp, C.POINTER(FitnessSummary)]
@@ -232,6 +236,9 @@ class Runtime:
         info = RuntimeInfo()
         check(lib().nwg_get_info(self.handle, C.byref(info)), "nwg_get_info")
         return info
+
+    def set_form(self, form: int) -> None:
+        check(lib().nwg_set_evaluation_form(self.handle, form), "nwg_set_evaluation_form")
 
     def bootstrap(self, size: int, seed: int, generation_index: int = 0) -> None:
         check(lib().nwg_bootstrap(self.handle, size, seed, generation_index), "nwg_bootstrap")

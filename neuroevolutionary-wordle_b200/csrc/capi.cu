@@ -73,12 +73,15 @@ struct nwg_runtime {
     unsigned long long *steps = nullptr;
     float *scratch = nullptr;
     int scratch_ctas = 0;
+    int form = NWG_FORM_FP32;
+    std::uint8_t *tc_tables = nullptr;
+    std::size_t tc_tables_bytes = 0;
 
     // pinned host staging
     ShardRecord *host_shards = nullptr;
     int *host_status = nullptr;
     SummaryDevice *host_summary = nullptr;
-    unsigned long long *host_steps = nullptr;  // [3]: decisions, encoded turns, episodes
+    unsigned long long *host_steps = nullptr;  // [5]: decisions, encoded turns, episodes, re-scored chunks, full
     cudaEvent_t eval_begin = nullptr;
     cudaEvent_t eval_end = nullptr;
     std::uint64_t last_episodes = 0;
@@ -274,7 +277,7 @@ void FreeRuntime(nwg_runtime *rt) {
                            rt->cur_eval,   rt->next_eval,    rt->cur_has,     rt->next_has,    rt->pairs,
                            rt->slot_used,  rt->status,       rt->summary,     rt->shards,      rt->cell_offsets,
                            rt->cell_words, rt->local_words,  rt->chunk_start, rt->score_sum,   rt->steps,
-                           rt->scratch};
+                           rt->scratch,    rt->tc_tables};
     for (void *p : device_ptrs) {
         if (p != nullptr) {
             cudaFree(p);
@@ -346,7 +349,7 @@ int EvaluateImpl(nwg_runtime *rt, const nwg_runtime_word_counts *counts, const n
     NWG_TRY(cudaMemsetAsync(rt->cur_fitness, 0, rt->max_generation_size * sizeof(float), rt->stream));
     NWG_TRY(cudaMemsetAsync(rt->cur_eval, 0, rt->max_generation_size * sizeof(std::uint32_t), rt->stream));
     NWG_TRY(cudaMemsetAsync(rt->cur_has, 0, rt->max_generation_size, rt->stream));
-    NWG_TRY(cudaMemsetAsync(rt->steps, 0, 3 * sizeof(unsigned long long), rt->stream));
+    NWG_TRY(cudaMemsetAsync(rt->steps, 0, 5 * sizeof(unsigned long long), rt->stream));
     NWG_TRY(LaunchEvalPrepare(src, population, static_cast<std::uint32_t>(g_catalog.count), rt->local_words,
                               rt->chunk_start, rt->score_sum, rt->status, rt->stream));
     EvalParams p{};
@@ -371,15 +374,29 @@ int EvaluateImpl(nwg_runtime *rt, const nwg_runtime_word_counts *counts, const n
     p.trace_turns = static_cast<std::int32_t *>(turns);
     p.trace_scores = static_cast<float *>(scores);
     p.trace_policy = static_cast<float *>(policy);
-    NWG_TRY(cudaEventRecord(rt->eval_begin, rt->stream));
-    NWG_TRY(LaunchEvalFp32(p, rt->scratch_ctas, rt->stream));
-    NWG_TRY(cudaEventRecord(rt->eval_end, rt->stream));
+    if (rt->form == NWG_FORM_FP32) {
+        NWG_TRY(cudaEventRecord(rt->eval_begin, rt->stream));
+        NWG_TRY(LaunchEvalFp32(p, rt->scratch_ctas, rt->stream));
+        NWG_TRY(cudaEventRecord(rt->eval_end, rt->stream));
+    } else {
+        const bool fp16 = rt->form == NWG_FORM_TC_FP16;
+        // |16-bit product - FP32 product| <= (2u + u^2)|p||e| with u = 2^-8 (BF16: p and e rounded) or 2^-11 (FP16:
+        // p rounded, e exact), plus 64-term FP32 accumulation on both sides; with a safety margin.
+        const float kappa = fp16 ? 6.5e-4f : 1.0e-2f;
+        NWG_TRY(LaunchBuildTcTables(rt->slab, rt->pitch, rt->cur_slots, population, g_catalog.fixed_t,
+                                    static_cast<std::uint32_t>(g_catalog.pad), static_cast<std::uint32_t>(selectable),
+                                    rt->tc_tables, fp16, rt->stream));
+        NWG_TRY(cudaEventRecord(rt->eval_begin, rt->stream));
+        NWG_TRY(LaunchEvalTc(p, rt->tc_tables, TcTablePitch(static_cast<std::uint32_t>(selectable)), kappa, fp16,
+                             rt->steps + 3, rt->scratch_ctas, rt->stream));
+        NWG_TRY(cudaEventRecord(rt->eval_end, rt->stream));
+    }
     NWG_TRY(LaunchFinalizeFitness(rt->score_sum, rt->local_words, population, rt->cur_fitness, rt->cur_eval,
                                   rt->cur_has, rt->status, rt->stream));
     NWG_TRY(LaunchSummarize(rt->cur_fitness, rt->cur_has, rt->cur_slots, population, rt->summary, rt->status,
                             rt->stream));
     NWG_TRY(cudaMemcpyAsync(rt->host_summary, rt->summary, sizeof(SummaryDevice), cudaMemcpyDeviceToHost, rt->stream));
-    NWG_TRY(cudaMemcpyAsync(rt->host_steps, rt->steps, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+    NWG_TRY(cudaMemcpyAsync(rt->host_steps, rt->steps, 5 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                             rt->stream));
     rt->last_eval_population = population;
     rt->last_action_count = rt->action_count;
@@ -515,19 +532,19 @@ int nwg_create(const nwg_runtime_config *config, nwg_runtime **runtime_out) {
     alloc(&rt->local_words, max_gen * sizeof(std::uint32_t));
     alloc(&rt->chunk_start, (max_gen + 1) * sizeof(std::uint32_t));
     alloc(&rt->score_sum, max_gen * sizeof(std::uint32_t));
-    alloc(&rt->steps, 3 * sizeof(unsigned long long));
+    alloc(&rt->steps, 5 * sizeof(unsigned long long));
     alloc(&rt->scratch, static_cast<std::size_t>(rt->scratch_ctas) * EvalScratchFloatsPerCta() * sizeof(float));
     ok = ok && cudaMallocHost(&rt->host_shards, NWG_CATALOG_CAPACITY * sizeof(ShardRecord)) == cudaSuccess;
     ok = ok && cudaMallocHost(&rt->host_status, sizeof(int)) == cudaSuccess;
     ok = ok && cudaMallocHost(&rt->host_summary, sizeof(SummaryDevice)) == cudaSuccess;
-    ok = ok && cudaMallocHost(&rt->host_steps, 3 * sizeof(unsigned long long)) == cudaSuccess;
+    ok = ok && cudaMallocHost(&rt->host_steps, 5 * sizeof(unsigned long long)) == cudaSuccess;
     ok = ok && cudaEventCreate(&rt->eval_begin) == cudaSuccess && cudaEventCreate(&rt->eval_end) == cudaSuccess;
     if (!ok) {
         FreeRuntime(rt);
         return kCudaFailure;
     }
     std::memset(rt->host_summary, 0, sizeof(SummaryDevice));
-    std::memset(rt->host_steps, 0, 3 * sizeof(unsigned long long));
+    std::memset(rt->host_steps, 0, 5 * sizeof(unsigned long long));
     *runtime_out = rt;
     return kOk;
 }
@@ -559,6 +576,22 @@ int nwg_get_info(const nwg_runtime *rt, nwg_runtime_info *info) {
     info->grid_column_count = rt->grid_column_count;
     info->current_generation_index = rt->cur_gen_index;
     info->current_generation_size = rt->cur_gen_size;
+    return kOk;
+}
+
+int nwg_set_evaluation_form(nwg_runtime *rt, int form) {
+    if (rt == nullptr || form < NWG_FORM_FP32 || form > NWG_FORM_TC_FP16) {
+        return kInvalidRuntimeConfig;
+    }
+    if (form != NWG_FORM_FP32 && rt->tc_tables == nullptr) {
+        const std::size_t bytes = rt->max_generation_size * TcTablePitch(static_cast<std::uint32_t>(rt->action_count));
+        if (cudaMalloc(&rt->tc_tables, bytes) != cudaSuccess) {
+            rt->tc_tables = nullptr;
+            return kCudaFailure;
+        }
+        rt->tc_tables_bytes = bytes;
+    }
+    rt->form = form;
     return kOk;
 }
 
@@ -672,6 +705,8 @@ int nwg_read_evaluation_stats(const nwg_runtime *rt, nwg_evaluation_stats *stats
     stats->game_steps = rt->host_steps[0];
     stats->encoded_turns = rt->host_steps[1];
     stats->episodes = rt->host_steps[2];
+    stats->rescored_chunks = rt->host_steps[3];
+    stats->full_rescores = rt->host_steps[4];
     stats->fitness_mean_fp64 = rt->host_summary->mean_fp64;
     stats->fitness_variance_fp64 = rt->host_summary->variance_fp64;
     float ms = 0.0f;

@@ -1,0 +1,584 @@
+// Fitness evaluation, tensor-core scoring form: action scores on tcgen05, decisions re-scored exactly.
+//
+// Same chunk structure, encoder and FP32 trunk as the plain form (eval_common.cuh); only the scoring
+// phase differs. Per game step and chunk of up to 128 games:
+//   1. the FP32 policy vectors are rounded to 16-bit (BF16, or FP16) into a K-major operand tile;
+//   2. the individual's embedding table, kept as a 16-bit copy in the tensor-core layout
+//      (BuildTcTablesKernel), streams through shared memory 128 actions at a time by bulk copies;
+//   3. one thread issues tcgen05.mma (M = 128 games, N = 128 actions, K = 64) into one of two TMEM
+//      accumulators while all eight warps read the other one back (tcgen05.ld) and keep, per game, the
+//      four largest 32-action chunk maxima;
+//   4. every chunk whose maximum lies within 2 * eps of the best (plus every chunk holding a word the
+//      game already guessed) is re-scored in FP32 with the plain form's own fused-multiply-add chain,
+//      and the game's guess is the exact FP32 argmax (ties to the lower index, guessed words masked).
+//      eps bounds |tensor-core score - FP32 score|: eps = kappa * sum_k |p_k| * max_a |e_ak|, with kappa
+//      covering the 16-bit rounding of p (and of e for BF16) and both FP32 accumulations. When the four
+//      tracked chunks cannot prove that no other chunk reaches the window, the game is re-scored over
+//      every action. The guesses are therefore identical to the plain form's.
+// Every mbarrier wait is bounded; a wait that gives up records NWG_TIMEOUT and the kernel winds down.
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include "eval_common.cuh"
+#include "umma.cuh"
+
+namespace nwg {
+namespace {
+
+using namespace evalx;
+
+constexpr int kTileN = 128;                  // actions per MMA tile
+constexpr int kTopK = 4;                     // chunk maxima kept per thread (per game half)
+constexpr std::uint32_t kTmemColumns = 256;  // two 128-column FP32 accumulators
+constexpr std::uint32_t kWaitLimit = 1u << 26;
+constexpr int kTileBytes = kTileN * kPolicy * 2;  // 16 KB of 16-bit embeddings per tile
+constexpr int kMaxTasks = 2048;
+
+// Shared-memory arena (floats) during the scoring phase.
+constexpr int kOffA = kTile;                          // 16-bit policy operand tile, 16 KB
+constexpr int kOffB = kOffA + 4096;                   // two 16 KB embedding tiles
+constexpr int kOffCand = kOffB + 8192;                // [128 games][2 halves][4] values, then ids
+constexpr int kOffTask = kOffCand + 2 * kChunkGames * 2 * kTopK;  // task list: (game << 16) | chunk
+constexpr int kOffKeys = kOffTask + kMaxTasks;        // per game: packed (exact score, action) maximum
+constexpr int kOffWindow = kOffKeys + 2 * kChunkGames;  // per game: best tensor-core score minus eps
+constexpr int kOffFull = kOffWindow + kChunkGames;    // games re-scored over every action
+constexpr int kOffEnd = kOffFull + kChunkGames;
+static_assert(kOffEnd <= kArenaFloats, "scoring buffers must fit in the arena");
+static_assert((kOffKeys * 4) % 8 == 0, "64-bit keys need 8-byte alignment");
+
+struct TcState {
+    std::uint64_t mbar_load[2];
+    std::uint64_t mbar_mma[2];
+    int task_count;
+    int full_count;
+    std::uint32_t tmem_base;
+    int failed;
+};
+
+struct TcParams {
+    EvalParams base;
+    const std::uint8_t *tables;  // per individual: 256-byte header (emax[64]) + A_pad x 64 16-bit values
+    std::size_t table_pitch;
+    float kappa;
+    int fp16_operands;
+    unsigned long long *tc_counters;  // [0] re-scored chunks, [1] games re-scored over every action
+};
+
+__device__ __forceinline__ std::uint32_t OrderedBits(float f) {
+    const std::uint32_t u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+
+__device__ __forceinline__ float FromOrderedBits(std::uint32_t u) {
+    return __uint_as_float((u & 0x80000000u) ? (u & 0x7FFFFFFFu) : ~u);
+}
+
+__device__ __forceinline__ unsigned long long PackKey(float score, std::uint32_t action) {
+    return (static_cast<unsigned long long>(OrderedBits(score)) << 32) | (0xFFFFFFFFu - action);
+}
+
+__device__ __forceinline__ void BulkLoad(void *dst, const void *src, std::uint32_t bytes, std::uint64_t *mbar) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(umma::SmemAddress(mbar)), "r"(bytes)
+                 : "memory");
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            umma::SmemAddress(dst)),
+        "l"(src), "r"(bytes), "r"(umma::SmemAddress(mbar))
+        : "memory");
+}
+
+// Insert x (chunk id xi) into the descending list v[0..3].
+__device__ __forceinline__ void InsertTop4(float (&v)[kTopK], int (&id)[kTopK], float x, int xi) {
+#pragma unroll
+    for (int j = 0; j < kTopK; ++j) {
+        const bool c = x > v[j];
+        const float tv = c ? v[j] : x;
+        const int ti = c ? id[j] : xi;
+        v[j] = c ? x : v[j];
+        id[j] = c ? xi : id[j];
+        x = tv;
+        xi = ti;
+    }
+}
+
+// Exact FP32 score of action a for game g (the plain form's chain: output_embedding.hpp:98-119).
+__device__ __forceinline__ float ExactScore(const EvalParams &p, const float *pv, int g, const __half *tail,
+                                            std::uint32_t a) {
+    float s = 0.0f;
+#pragma unroll 2
+    for (int k = 0; k < kFixedDim; ++k) {
+        s = __fmaf_rn(pv[k * kLd + g], p.fixed_t[static_cast<std::size_t>(k) * p.action_pad + a], s);
+    }
+    const __half *row = tail + static_cast<std::size_t>(a) * kTailDim;
+#pragma unroll 2
+    for (int k = 0; k < kTailDim; ++k) {
+        s = __fmaf_rn(pv[(kFixedDim + k) * kLd + g], __half2float(row[k]), s);
+    }
+    return s;
+}
+
+// Warp-cooperative exact re-scoring of chunk `chunk` (32 actions) for game g; folds the masked argmax
+// into st.best_key[g].
+__device__ __forceinline__ void RescoreChunk(const EvalParams &p, const ChunkState &cs, unsigned long long *best_key,
+                                             const float *pv, const __half *tail, int g, int chunk, int turns) {
+    const int lane = threadIdx.x & 31;
+    const std::uint32_t a = static_cast<std::uint32_t>(chunk) * 32u + lane;
+    unsigned long long key = 0;
+    if (a < p.action_count) {
+        const std::uint32_t code = p.codes[a];
+        bool masked = false;
+        for (int u = 0; u < turns; ++u) {
+            masked |= cs.guess[u][g] == code;
+        }
+        if (!masked) {
+            key = PackKey(ExactScore(p, pv, g, tail, a), a);
+        }
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        const unsigned long long other = __shfl_xor_sync(0xffffffffu, key, off);
+        key = other > key ? other : key;
+    }
+    if (lane == 0 && key != 0) {
+        atomicMax(&best_key[g], key);
+    }
+}
+
+template <bool kFp16>
+__device__ void ScoreTensorCores(const TcParams &q, ChunkState &cs, TcState &ts, const __half *gh, float *arena,
+                                 int t, std::uint32_t (&load_uses)[2], std::uint32_t (&mma_uses)[2]) {
+    const EvalParams &p = q.base;
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5;
+    const int lane = tid & 31;
+    const float *pv = arena;
+    unsigned char *a_tile = reinterpret_cast<unsigned char *>(arena + kOffA);
+    unsigned char *b_tile = reinterpret_cast<unsigned char *>(arena + kOffB);
+    float *cand_v = arena + kOffCand;
+    int *cand_id = reinterpret_cast<int *>(arena + kOffCand + kChunkGames * 2 * kTopK);
+    std::uint32_t *task_list = reinterpret_cast<std::uint32_t *>(arena + kOffTask);
+    unsigned long long *best_key = reinterpret_cast<unsigned long long *>(arena + kOffKeys);
+    float *window_low = arena + kOffWindow;
+    int *full_rows = reinterpret_cast<int *>(arena + kOffFull);
+    const std::uint32_t ind = static_cast<std::uint32_t>(cs.individual);
+    const std::uint8_t *table = q.tables + static_cast<std::size_t>(ind) * q.table_pitch;
+    const float *emax = reinterpret_cast<const float *>(table);
+    const std::uint8_t *embed = table + 256;
+    const int n_tiles = static_cast<int>((p.action_count + kTileN - 1) / kTileN);
+
+    // 16-bit policy operand, K-major tile [128 games][64]
+    for (int idx = tid; idx < kChunkGames * kPolicy; idx += kEvalThreads) {
+        const int g = idx & 127;
+        const int k = idx >> 7;
+        const float v = pv[k * kLd + g];
+        std::uint16_t bits;
+        if constexpr (kFp16) {
+            bits = __half_as_ushort(__float2half_rn(v));
+        } else {
+            bits = __bfloat16_as_ushort(__float2bfloat16_rn(v));
+        }
+        *reinterpret_cast<std::uint16_t *>(a_tile + umma::TileOffset(g, k, kPolicy)) = bits;
+    }
+    if (tid < kChunkGames) {
+        best_key[tid] = 0;
+    }
+    if (tid == 0) {
+        ts.task_count = 0;
+        ts.full_count = 0;
+    }
+    umma::FenceProxyAsyncShared();
+    __syncthreads();
+
+    const std::uint32_t idesc = kFp16 ? (umma::InstrDescBf16(128, kTileN) & ~((7u << 7) | (7u << 10)))
+                                      : umma::InstrDescBf16(128, kTileN);
+    const std::uint64_t a_desc0 = umma::SmemDescriptor(umma::SmemAddress(a_tile), 128, 1024);
+    const std::uint32_t b_addr0 = umma::SmemAddress(b_tile);
+    auto issue_mma = [&](int tile) {
+        const int buf = tile & 1;
+        const std::uint32_t d = ts.tmem_base + static_cast<std::uint32_t>(buf * kTileN);
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            const std::uint64_t ad = a_desc0 + static_cast<std::uint64_t>((s * 256) >> 4);
+            const std::uint64_t bd = umma::SmemDescriptor(b_addr0 + buf * kTileBytes + s * 256, 128, 1024);
+            umma::Mma(d, ad, bd, idesc, s > 0);
+        }
+        umma::Commit(&ts.mbar_mma[buf]);
+    };
+    if (tid == 0) {
+        for (int tile = 0; tile < 2 && tile < n_tiles; ++tile) {
+            BulkLoad(b_tile + tile * kTileBytes, embed + static_cast<std::size_t>(tile) * kTileBytes, kTileBytes,
+                     &ts.mbar_load[tile]);
+        }
+        if (!umma::MbarWait(&ts.mbar_load[0], load_uses[0] & 1u, kWaitLimit)) {
+            ts.failed = 1;
+        }
+        load_uses[0] += 1;
+        umma::FenceAfterSync();
+        issue_mma(0);
+    }
+
+    const int quadrant = warp & 3;
+    const int half = warp >> 2;
+    const int row = quadrant * 32 + lane;
+    float tv[kTopK];
+    int ti[kTopK];
+#pragma unroll
+    for (int j = 0; j < kTopK; ++j) {
+        tv[j] = -INFINITY;
+        ti[j] = -1;
+    }
+    for (int tile = 0; tile < n_tiles; ++tile) {
+        const int buf = tile & 1;
+        if (tid == 0 && tile + 1 < n_tiles) {
+            const int nb = (tile + 1) & 1;
+            if (!umma::MbarWait(&ts.mbar_load[nb], load_uses[nb] & 1u, kWaitLimit)) {
+                ts.failed = 1;
+            }
+            load_uses[nb] += 1;
+            umma::FenceAfterSync();
+            issue_mma(tile + 1);
+        }
+        if (!umma::MbarWait(&ts.mbar_mma[buf], mma_uses[buf] & 1u, kWaitLimit)) {
+            ts.failed = 1;
+        }
+        mma_uses[buf] += 1;
+        umma::FenceAfterSync();
+        if (tid == 0 && tile + 2 < n_tiles) {
+            BulkLoad(b_tile + buf * kTileBytes, embed + static_cast<std::size_t>(tile + 2) * kTileBytes, kTileBytes,
+                     &ts.mbar_load[buf]);
+        }
+        const bool last = tile + 1 == n_tiles;
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            const int col0 = half * 64 + c * 32;
+            float v[32];
+            umma::Load32(ts.tmem_base + static_cast<std::uint32_t>(buf * kTileN + col0) +
+                             (static_cast<std::uint32_t>(quadrant * 32) << 16),
+                         v);
+            if (last) {
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                    if (static_cast<std::uint32_t>(tile * kTileN + col0 + j) >= p.action_count) {
+                        v[j] = -INFINITY;
+                    }
+                }
+            }
+#pragma unroll
+            for (int w = 16; w > 0; w >>= 1) {
+#pragma unroll
+                for (int j = 0; j < w; ++j) {
+                    v[j] = fmaxf(v[j], v[j + w]);
+                }
+            }
+            InsertTop4(tv, ti, v[0], tile * 4 + half * 2 + c);
+        }
+        umma::FenceBeforeSync();
+        __syncthreads();
+    }
+#pragma unroll
+    for (int j = 0; j < kTopK; ++j) {
+        cand_v[(row * 2 + half) * kTopK + j] = tv[j];
+        cand_id[(row * 2 + half) * kTopK + j] = ti[j];
+    }
+    __syncthreads();
+
+    // ---- candidate chunks per game ----
+    const int turns_now = t;
+    if (tid < kChunkGames && !cs.done[tid]) {
+        const int g = tid;
+        int masked_chunk[kMaxTurns];
+        for (int u = 0; u < kMaxTurns; ++u) {
+            masked_chunk[u] = (u < turns_now && cs.word_index[u][g] >= 0) ? cs.word_index[u][g] / 32 : -1;
+        }
+        auto is_masked_chunk = [&](int chunk) {
+            bool m = false;
+            for (int u = 0; u < kMaxTurns; ++u) {
+                m |= masked_chunk[u] == chunk;
+            }
+            return m;
+        };
+        float s_sum = 0.0f;
+        bool finite = true;
+        for (int k = 0; k < kPolicy; ++k) {
+            const float pk = pv[k * kLd + g];
+            finite &= fabsf(pk) < (kFp16 ? 60000.0f : 3.0e38f);
+            s_sum = __fmaf_rn(fabsf(pk), emax[k], s_sum);
+        }
+        const float eps = q.kappa * s_sum * 1.0001f;
+        bool full = !finite || !(eps < INFINITY);
+        float top = -INFINITY;
+        for (int h = 0; h < 2; ++h) {
+            bool found = false;
+            for (int j = 0; j < kTopK && !found; ++j) {
+                const int id = cand_id[(g * 2 + h) * kTopK + j];
+                if (id >= 0 && !is_masked_chunk(id)) {
+                    top = fmaxf(top, cand_v[(g * 2 + h) * kTopK + j]);
+                    found = true;
+                }
+            }
+            if (!found && cand_id[(g * 2 + h) * kTopK + kTopK - 1] >= 0) {
+                full = true;  // every tracked chunk of this half holds a guessed word
+            }
+        }
+        const float window = top - 2.0f * eps;
+        if (!(top > -INFINITY)) {
+            full = true;
+        }
+        for (int h = 0; h < 2 && !full; ++h) {
+            const int last_id = cand_id[(g * 2 + h) * kTopK + kTopK - 1];
+            if (last_id >= 0 && cand_v[(g * 2 + h) * kTopK + kTopK - 1] >= window) {
+                full = true;  // more chunks of this half may reach the window
+            }
+        }
+        window_low[g] = top - eps;
+        if (full) {
+            const int slot = atomicAdd(&ts.full_count, 1);
+            full_rows[slot] = g;
+        } else {
+            for (int h = 0; h < 2; ++h) {
+                for (int j = 0; j < kTopK; ++j) {
+                    const int id = cand_id[(g * 2 + h) * kTopK + j];
+                    if (id >= 0 && cand_v[(g * 2 + h) * kTopK + j] >= window && !is_masked_chunk(id)) {
+                        const int slot = atomicAdd(&ts.task_count, 1);
+                        if (slot < kMaxTasks) {
+                            task_list[slot] = (static_cast<std::uint32_t>(g) << 16) | static_cast<std::uint32_t>(id);
+                        }
+                    }
+                }
+            }
+            for (int u = 0; u < kMaxTurns; ++u) {
+                bool first = masked_chunk[u] >= 0;
+                for (int v2 = 0; v2 < u; ++v2) {
+                    first &= masked_chunk[v2] != masked_chunk[u];
+                }
+                if (first) {
+                    const int slot = atomicAdd(&ts.task_count, 1);
+                    if (slot < kMaxTasks) {
+                        task_list[slot] = (static_cast<std::uint32_t>(g) << 16) |
+                                          static_cast<std::uint32_t>(masked_chunk[u]);
+                    }
+                }
+            }
+        }
+    }
+    __syncthreads();
+
+    // ---- exact re-scoring of the candidate chunks (a warp per chunk) ----
+    const __half *tail = reinterpret_cast<const __half *>(reinterpret_cast<const std::uint8_t *>(gh) + kTailOffsetBytes);
+    const int tasks = ts.task_count < kMaxTasks ? ts.task_count : kMaxTasks;
+    const int first_full = ts.full_count;
+    for (int k = warp; k < tasks; k += kEvalThreads / 32) {
+        const std::uint32_t task = task_list[k];
+        RescoreChunk(p, cs, best_key, pv, tail, static_cast<int>(task >> 16), static_cast<int>(task & 0xFFFFu),
+                     turns_now);
+    }
+    __syncthreads();
+    // a game whose exact best stays below top - eps, or whose task list overflowed, is re-scored in full
+    if (tid < kChunkGames && !cs.done[tid]) {
+        const int g = tid;
+        const unsigned long long key = best_key[g];
+        bool in_full = false;
+        for (int i = 0; i < first_full; ++i) {
+            in_full |= full_rows[i] == g;
+        }
+        if (!in_full && (ts.task_count > kMaxTasks || key == 0 ||
+                         FromOrderedBits(static_cast<std::uint32_t>(key >> 32)) < window_low[g])) {
+            const int slot = atomicAdd(&ts.full_count, 1);
+            full_rows[slot] = g;
+        }
+    }
+    __syncthreads();
+    const int full_count = ts.full_count;
+    const int chunks_per_row = static_cast<int>((p.action_count + 31) / 32);
+    for (int i = 0; i < full_count; ++i) {
+        const int g = full_rows[i];
+        for (int chunk = warp; chunk < chunks_per_row; chunk += kEvalThreads / 32) {
+            RescoreChunk(p, cs, best_key, pv, tail, g, chunk, turns_now);
+        }
+    }
+    __syncthreads();
+    if (tid < kChunkGames) {
+        const unsigned long long key = best_key[tid];
+        cs.best[tid] = key == 0 ? -1 : static_cast<int>(0xFFFFFFFFu - static_cast<std::uint32_t>(key & 0xFFFFFFFFull));
+    }
+    if (tid == 0 && q.tc_counters != nullptr) {
+        atomicAdd(q.tc_counters, static_cast<unsigned long long>(tasks));
+        atomicAdd(q.tc_counters + 1, static_cast<unsigned long long>(full_count));
+    }
+    __syncthreads();
+}
+
+template <bool kFp16>
+__global__ void __launch_bounds__(kEvalThreads, 2) EvalTcKernel(const TcParams q) {
+    extern __shared__ __align__(1024) float arena[];
+    __shared__ ChunkState cs;
+    __shared__ TcState ts;
+    const EvalParams &p = q.base;
+    const int tid = threadIdx.x;
+    float *scratch = p.scratch + static_cast<std::size_t>(blockIdx.x) * kScratchFloats;
+    unsigned long long decisions = 0;
+    unsigned long long encoded = 0;
+    unsigned long long episodes = 0;
+    std::uint32_t load_uses[2] = {0, 0};
+    std::uint32_t mma_uses[2] = {0, 0};
+    const std::uint32_t total_chunks = p.chunk_start[p.population];
+
+    if (tid < 32) {
+        umma::Alloc(&ts.tmem_base, kTmemColumns);
+    }
+    if (tid == 0) {
+        for (int b = 0; b < 2; ++b) {
+            umma::MbarInit(&ts.mbar_load[b], 1);
+            umma::MbarInit(&ts.mbar_mma[b], 1);
+        }
+        ts.failed = 0;
+    }
+    umma::FenceBeforeSync();
+    __syncthreads();
+    umma::FenceAfterSync();
+
+    for (std::uint32_t chunk = blockIdx.x; chunk < total_chunks; chunk += gridDim.x) {
+        if (!BeginChunk(p, cs, chunk) || ts.failed) {
+            break;
+        }
+        const std::uint32_t ind = static_cast<std::uint32_t>(cs.individual);
+        const __half *gh = reinterpret_cast<const __half *>(p.slab + static_cast<std::size_t>(cs.slot) * p.pitch);
+        SetupGames(p, cs, gh, scratch);
+        if (cs.cls == 1 && CountActive(cs) > 0) {
+            EncodeRound(cs, gh, arena, scratch, 0);
+            EncodeRound(cs, gh, arena, scratch, 1);
+            encoded += tid == 0 ? 2ull * cs.active : 0ull;
+        }
+        for (int step = 0; step < kMaxTurns; ++step) {
+            if (CountActive(cs) == 0 || ts.failed) {
+                break;
+            }
+            const int t = cs.cls == 0 ? step : step + 2;
+            if (step > 0) {
+                EncodeRound(cs, gh, arena, scratch, t - 1);
+                encoded += tid == 0 ? static_cast<unsigned long long>(cs.active) : 0ull;
+            }
+            TrunkForward(p, cs, gh, arena, scratch, t, step, ind);
+            ScoreTensorCores<kFp16>(q, cs, ts, gh, arena, t, load_uses, mma_uses);
+            if (ts.failed) {
+                break;
+            }
+            AppendGuesses(p, cs, step, decisions);
+        }
+        FinishChunk(p, cs, ind, episodes);
+    }
+    FlushCounters(p, decisions, encoded, episodes);
+    if (tid == 0 && ts.failed) {
+        SetStatus(p.status, kTimeout);
+        // let any tensor-core work still in flight finish before the columns are released (bounded)
+        (void)umma::MbarWait(&ts.mbar_mma[0], mma_uses[0] & 1u, 1u << 20);
+        (void)umma::MbarWait(&ts.mbar_mma[1], mma_uses[1] & 1u, 1u << 20);
+    }
+    umma::FenceBeforeSync();
+    __syncthreads();
+    if (tid < 32) {
+        umma::Dealloc(ts.tmem_base, kTmemColumns);
+    }
+}
+
+// Per individual: emax[k] = max over the selectable actions of |e_ak| (header), and the embeddings as
+// 16-bit values in the K-major core-matrix layout, 1 KB per 8 actions, zero past the last action.
+template <bool kFp16>
+__global__ void BuildTcTablesKernel(const std::uint8_t *slab, std::size_t pitch, const std::uint32_t *slots,
+                                    const float *fixed_t, std::uint32_t action_pad, std::uint32_t action_count,
+                                    std::uint32_t tiles, std::uint8_t *tables, std::size_t table_pitch) {
+    const std::uint32_t ind = blockIdx.y;
+    const std::uint32_t tile = blockIdx.x;
+    const __half *tail =
+        reinterpret_cast<const __half *>(slab + static_cast<std::size_t>(slots[ind]) * pitch + kTailOffsetBytes);
+    std::uint8_t *table = tables + static_cast<std::size_t>(ind) * table_pitch;
+    unsigned int *emax_bits = reinterpret_cast<unsigned int *>(table);
+    std::uint8_t *out = table + 256 + static_cast<std::size_t>(tile) * kTileBytes;
+    __shared__ unsigned int block_max[kPolicy];
+    if (threadIdx.x < kPolicy) {
+        block_max[threadIdx.x] = 0;
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < kTileN * kPolicy; idx += blockDim.x) {
+        const int a_local = idx >> 6;
+        const int k = idx & 63;
+        const std::uint32_t a = tile * kTileN + a_local;
+        float v = 0.0f;
+        if (a < action_count) {
+            v = k < kFixedDim ? fixed_t[static_cast<std::size_t>(k) * action_pad + a]
+                              : __half2float(tail[static_cast<std::size_t>(a) * kTailDim + (k - kFixedDim)]);
+            atomicMax(&block_max[k], __float_as_uint(fabsf(v)));
+        }
+        std::uint16_t bits;
+        if constexpr (kFp16) {
+            bits = __half_as_ushort(__float2half_rn(v));
+        } else {
+            bits = __bfloat16_as_ushort(__float2bfloat16_rn(v));
+        }
+        *reinterpret_cast<std::uint16_t *>(out + umma::TileOffset(a_local, k, kPolicy)) = bits;
+    }
+    __syncthreads();
+    if (threadIdx.x < kPolicy && block_max[threadIdx.x] != 0) {
+        atomicMax(&emax_bits[threadIdx.x], block_max[threadIdx.x]);
+    }
+}
+
+}  // namespace
+
+std::size_t TcTablePitch(std::uint32_t action_count) {
+    const std::size_t tiles = (action_count + kTileN - 1) / kTileN;
+    return 256 + tiles * static_cast<std::size_t>(kTileBytes);
+}
+
+cudaError_t LaunchBuildTcTables(const std::uint8_t *slab, std::size_t pitch, const std::uint32_t *slots,
+                                std::uint32_t population, const float *fixed_t, std::uint32_t action_pad,
+                                std::uint32_t action_count, std::uint8_t *tables, bool fp16, cudaStream_t stream) {
+    const std::size_t table_pitch = TcTablePitch(action_count);
+    const std::uint32_t tiles = (action_count + kTileN - 1) / kTileN;
+    cudaError_t e = cudaMemset2DAsync(tables, table_pitch, 0, 256, population, stream);
+    if (e != cudaSuccess) {
+        return e;
+    }
+    dim3 grid(tiles, population);
+    if (fp16) {
+        BuildTcTablesKernel<true><<<grid, 256, 0, stream>>>(slab, pitch, slots, fixed_t, action_pad, action_count,
+                                                           tiles, tables, table_pitch);
+    } else {
+        BuildTcTablesKernel<false><<<grid, 256, 0, stream>>>(slab, pitch, slots, fixed_t, action_pad, action_count,
+                                                            tiles, tables, table_pitch);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t LaunchEvalTc(const EvalParams &params, const std::uint8_t *tables, std::size_t table_pitch, float kappa,
+                         bool fp16, unsigned long long *tc_counters, int cta_count, cudaStream_t stream) {
+    static bool configured[2] = {false, false};
+    const int arena_bytes = kArenaFloats * static_cast<int>(sizeof(float));
+    if (!configured[fp16 ? 1 : 0]) {
+        cudaError_t e = fp16 ? cudaFuncSetAttribute(EvalTcKernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                    arena_bytes)
+                             : cudaFuncSetAttribute(EvalTcKernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                    arena_bytes);
+        if (e != cudaSuccess) {
+            return e;
+        }
+        configured[fp16 ? 1 : 0] = true;
+    }
+    if (cta_count <= 0) {
+        return cudaSuccess;
+    }
+    TcParams q{};
+    q.base = params;
+    q.tables = tables;
+    q.table_pitch = table_pitch;
+    q.kappa = kappa;
+    q.fp16_operands = fp16 ? 1 : 0;
+    q.tc_counters = tc_counters;
+    if (fp16) {
+        EvalTcKernel<true><<<cta_count, kEvalThreads, arena_bytes, stream>>>(q);
+    } else {
+        EvalTcKernel<false><<<cta_count, kEvalThreads, arena_bytes, stream>>>(q);
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace nwg

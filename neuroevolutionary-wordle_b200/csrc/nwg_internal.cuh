@@ -87,6 +87,14 @@ cudaError_t LaunchFinalizeFitness(const std::uint32_t *score_sum, const std::uin
                                   std::uint32_t population, float *fitness, std::uint32_t *evaluation_counts,
                                   std::uint8_t *has_fitness, int *status, cudaStream_t stream);
 
+// ---- fitness evaluation, tensor-core scoring form ----
+std::size_t TcTablePitch(std::uint32_t action_count);
+cudaError_t LaunchBuildTcTables(const std::uint8_t *slab, std::size_t pitch, const std::uint32_t *slots,
+                                std::uint32_t population, const float *fixed_t, std::uint32_t action_pad,
+                                std::uint32_t action_count, std::uint8_t *tables, bool fp16, cudaStream_t stream);
+cudaError_t LaunchEvalTc(const EvalParams &params, const std::uint8_t *tables, std::size_t table_pitch, float kappa,
+                         bool fp16, unsigned long long *tc_counters, int cta_count, cudaStream_t stream);
+
 struct SummaryDevice {
     float best_fitness;
     float average_fitness;
