@@ -8,9 +8,9 @@
 //   3. one thread issues tcgen05.mma (M = 128 games, N = 128 actions, K = 64) into one of two TMEM
 //      accumulators while all eight warps read the other one back (tcgen05.ld) and keep, per game, the
 //      four largest 32-action chunk maxima;
-//   4. every chunk whose maximum lies within 2 * eps of the best (plus every chunk holding a word the
-//      game already guessed) is re-scored in FP32 with the plain form's own fused-multiply-add chain,
-//      and the game's guess is the exact FP32 argmax (ties to the lower index, guessed words masked).
+//   4. every chunk whose maximum lies within 2 * eps of the best chunk free of guessed words is re-scored
+//      in FP32 with the plain form's own fused-multiply-add chain, and the game's guess is the exact FP32
+//      argmax (ties to the lower index, guessed words masked).
 //      eps bounds |tensor-core score - FP32 score|: eps = kappa * sum_k |p_k| * max_a |e_ak|, with kappa
 //      covering the 16-bit rounding of p (and of e for BF16) and both FP32 accumulations. When the four
 //      tracked chunks cannot prove that no other chunk reaches the window, the game is re-scored over
@@ -102,17 +102,25 @@ __device__ __forceinline__ void InsertTop4(float (&v)[kTopK], int (&id)[kTopK], 
 }
 
 // Exact FP32 score of action a for game g (the plain form's chain: output_embedding.hpp:98-119).
+// All 64 embedding values are loaded before the chain starts, so a call costs one memory latency.
 __device__ __forceinline__ float ExactScore(const EvalParams &p, const float *pv, int g, const __half *tail,
                                             std::uint32_t a) {
-    float s = 0.0f;
-#pragma unroll 2
+    float e[kPolicy];
+#pragma unroll
     for (int k = 0; k < kFixedDim; ++k) {
-        s = __fmaf_rn(pv[k * kLd + g], p.fixed_t[static_cast<std::size_t>(k) * p.action_pad + a], s);
+        e[k] = p.fixed_t[static_cast<std::size_t>(k) * p.action_pad + a];
     }
-    const __half *row = tail + static_cast<std::size_t>(a) * kTailDim;
-#pragma unroll 2
-    for (int k = 0; k < kTailDim; ++k) {
-        s = __fmaf_rn(pv[(kFixedDim + k) * kLd + g], __half2float(row[k]), s);
+    const __half2 *row = reinterpret_cast<const __half2 *>(tail + static_cast<std::size_t>(a) * kTailDim);
+#pragma unroll
+    for (int j = 0; j < kTailDim / 2; ++j) {
+        const float2 f = __half22float2(row[j]);
+        e[kFixedDim + 2 * j] = f.x;
+        e[kFixedDim + 2 * j + 1] = f.y;
+    }
+    float s = 0.0f;
+#pragma unroll
+    for (int k = 0; k < kPolicy; ++k) {
+        s = __fmaf_rn(pv[k * kLd + g], e[k], s);
     }
     return s;
 }
@@ -345,16 +353,17 @@ __device__ void ScoreTensorCores(const TcParams &q, ChunkState &cs, TcState &ts,
                     }
                 }
             }
-            for (int u = 0; u < kMaxTurns; ++u) {
-                bool first = masked_chunk[u] >= 0;
-                for (int v2 = 0; v2 < u; ++v2) {
-                    first &= masked_chunk[v2] != masked_chunk[u];
-                }
-                if (first) {
-                    const int slot = atomicAdd(&ts.task_count, 1);
-                    if (slot < kMaxTasks) {
-                        task_list[slot] = (static_cast<std::uint32_t>(g) << 16) |
-                                          static_cast<std::uint32_t>(masked_chunk[u]);
+            // A chunk holding a guessed word matters only when its maximum reaches the window: tracked chunks
+            // are compared directly; an untracked chunk lies below the tracked list's last entry, which
+            // (no overflow) is below the window.
+            for (int h = 0; h < 2; ++h) {
+                for (int j = 0; j < kTopK; ++j) {
+                    const int id = cand_id[(g * 2 + h) * kTopK + j];
+                    if (id >= 0 && cand_v[(g * 2 + h) * kTopK + j] >= window && is_masked_chunk(id)) {
+                        const int slot = atomicAdd(&ts.task_count, 1);
+                        if (slot < kMaxTasks) {
+                            task_list[slot] = (static_cast<std::uint32_t>(g) << 16) | static_cast<std::uint32_t>(id);
+                        }
                     }
                 }
             }
