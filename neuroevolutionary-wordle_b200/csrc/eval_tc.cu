@@ -34,10 +34,14 @@ constexpr std::uint32_t kWaitLimit = 1u << 26;
 constexpr int kTileBytes = kTileN * kPolicy * 2;  // 16 KB of 16-bit embeddings per tile
 constexpr int kMaxTasks = 2048;
 
-// Shared-memory arena (floats) during the scoring phase.
+// Shared-memory arena (floats) during the scoring phase: the FP32 policy vectors (arena[0 .. kTile)), the
+// 16-bit policy operand and three 16 KB embedding tiles; once the tile loop ends, the candidate lists, task
+// list and per-game keys reuse the embedding tiles' space.
+constexpr int kStages = 3;
 constexpr int kOffA = kTile;                          // 16-bit policy operand tile, 16 KB
-constexpr int kOffB = kOffA + 4096;                   // two 16 KB embedding tiles
-constexpr int kOffCand = kOffB + 8192;                // [128 games][2 halves][4] values, then ids
+constexpr int kOffB = kOffA + 4096;                   // kStages 16 KB embedding tiles
+static_assert(kOffB + kStages * 4096 <= kArenaFloats, "embedding tiles must fit in the arena");
+constexpr int kOffCand = kOffB;                       // [128 games][2 halves][4] values, then ids
 constexpr int kOffTask = kOffCand + 2 * kChunkGames * 2 * kTopK;  // task list: (game << 16) | chunk
 constexpr int kOffKeys = kOffTask + kMaxTasks;        // per game: packed (exact score, action) maximum
 constexpr int kOffWindow = kOffKeys + 2 * kChunkGames;  // per game: best tensor-core score minus eps
@@ -47,7 +51,7 @@ static_assert(kOffEnd <= kArenaFloats, "scoring buffers must fit in the arena");
 static_assert((kOffKeys * 4) % 8 == 0, "64-bit keys need 8-byte alignment");
 
 struct TcState {
-    std::uint64_t mbar_load[2];
+    std::uint64_t mbar_load[kStages];
     std::uint64_t mbar_mma[2];
     int task_count;
     int full_count;
@@ -153,7 +157,7 @@ __device__ __forceinline__ void RescoreChunk(const EvalParams &p, const ChunkSta
 
 template <bool kFp16>
 __device__ void ScoreTensorCores(const TcParams &q, ChunkState &cs, TcState &ts, const __half *gh, float *arena,
-                                 int t, std::uint32_t (&load_uses)[2], std::uint32_t (&mma_uses)[2]) {
+                                 int t, std::uint32_t (&load_uses)[kStages], std::uint32_t (&mma_uses)[2]) {
     const EvalParams &p = q.base;
     const int tid = threadIdx.x;
     const int warp = tid >> 5;
@@ -186,9 +190,6 @@ __device__ void ScoreTensorCores(const TcParams &q, ChunkState &cs, TcState &ts,
         }
         *reinterpret_cast<std::uint16_t *>(a_tile + umma::TileOffset(g, k, kPolicy)) = bits;
     }
-    if (tid < kChunkGames) {
-        best_key[tid] = 0;
-    }
     if (tid == 0) {
         ts.task_count = 0;
         ts.full_count = 0;
@@ -200,26 +201,32 @@ __device__ void ScoreTensorCores(const TcParams &q, ChunkState &cs, TcState &ts,
                                       : umma::InstrDescBf16(128, kTileN);
     const std::uint64_t a_desc0 = umma::SmemDescriptor(umma::SmemAddress(a_tile), 128, 1024);
     const std::uint32_t b_addr0 = umma::SmemAddress(b_tile);
+    // accumulator buffer: tile & 1; embedding stage: tile % kStages
     auto issue_mma = [&](int tile) {
-        const int buf = tile & 1;
-        const std::uint32_t d = ts.tmem_base + static_cast<std::uint32_t>(buf * kTileN);
+        const int acc = tile & 1;
+        const int stage = tile % kStages;
+        const std::uint32_t d = ts.tmem_base + static_cast<std::uint32_t>(acc * kTileN);
 #pragma unroll
         for (int s = 0; s < 4; ++s) {
             const std::uint64_t ad = a_desc0 + static_cast<std::uint64_t>((s * 256) >> 4);
-            const std::uint64_t bd = umma::SmemDescriptor(b_addr0 + buf * kTileBytes + s * 256, 128, 1024);
+            const std::uint64_t bd = umma::SmemDescriptor(b_addr0 + stage * kTileBytes + s * 256, 128, 1024);
             umma::Mma(d, ad, bd, idesc, s > 0);
         }
-        umma::Commit(&ts.mbar_mma[buf]);
+        umma::Commit(&ts.mbar_mma[acc]);
+    };
+    auto wait_load = [&](int tile) {
+        const int stage = tile % kStages;
+        if (!umma::MbarWait(&ts.mbar_load[stage], load_uses[stage] & 1u, kWaitLimit)) {
+            ts.failed = 1;
+        }
+        load_uses[stage] += 1;
     };
     if (tid == 0) {
-        for (int tile = 0; tile < 2 && tile < n_tiles; ++tile) {
+        for (int tile = 0; tile < kStages && tile < n_tiles; ++tile) {
             BulkLoad(b_tile + tile * kTileBytes, embed + static_cast<std::size_t>(tile) * kTileBytes, kTileBytes,
                      &ts.mbar_load[tile]);
         }
-        if (!umma::MbarWait(&ts.mbar_load[0], load_uses[0] & 1u, kWaitLimit)) {
-            ts.failed = 1;
-        }
-        load_uses[0] += 1;
+        wait_load(0);
         umma::FenceAfterSync();
         issue_mma(0);
     }
@@ -237,11 +244,7 @@ __device__ void ScoreTensorCores(const TcParams &q, ChunkState &cs, TcState &ts,
     for (int tile = 0; tile < n_tiles; ++tile) {
         const int buf = tile & 1;
         if (tid == 0 && tile + 1 < n_tiles) {
-            const int nb = (tile + 1) & 1;
-            if (!umma::MbarWait(&ts.mbar_load[nb], load_uses[nb] & 1u, kWaitLimit)) {
-                ts.failed = 1;
-            }
-            load_uses[nb] += 1;
+            wait_load(tile + 1);
             umma::FenceAfterSync();
             issue_mma(tile + 1);
         }
@@ -250,9 +253,11 @@ __device__ void ScoreTensorCores(const TcParams &q, ChunkState &cs, TcState &ts,
         }
         mma_uses[buf] += 1;
         umma::FenceAfterSync();
-        if (tid == 0 && tile + 2 < n_tiles) {
-            BulkLoad(b_tile + buf * kTileBytes, embed + static_cast<std::size_t>(tile + 2) * kTileBytes, kTileBytes,
-                     &ts.mbar_load[buf]);
+        if (tid == 0 && tile + kStages < n_tiles) {
+            // tile's MMA has completed, so its embedding stage is free for tile + kStages
+            const int stage = tile % kStages;
+            BulkLoad(b_tile + stage * kTileBytes, embed + static_cast<std::size_t>(tile + kStages) * kTileBytes,
+                     kTileBytes, &ts.mbar_load[stage]);
         }
         const bool last = tile + 1 == n_tiles;
 #pragma unroll
@@ -286,6 +291,9 @@ __device__ void ScoreTensorCores(const TcParams &q, ChunkState &cs, TcState &ts,
     for (int j = 0; j < kTopK; ++j) {
         cand_v[(row * 2 + half) * kTopK + j] = tv[j];
         cand_id[(row * 2 + half) * kTopK + j] = ti[j];
+    }
+    if (tid < kChunkGames) {
+        best_key[tid] = 0;
     }
     __syncthreads();
 
@@ -427,7 +435,7 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTcKernel(const TcParams q
     unsigned long long decisions = 0;
     unsigned long long encoded = 0;
     unsigned long long episodes = 0;
-    std::uint32_t load_uses[2] = {0, 0};
+    std::uint32_t load_uses[kStages] = {0, 0, 0};
     std::uint32_t mma_uses[2] = {0, 0};
     const std::uint32_t total_chunks = p.chunk_start[p.population];
 
@@ -435,8 +443,10 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTcKernel(const TcParams q
         umma::Alloc(&ts.tmem_base, kTmemColumns);
     }
     if (tid == 0) {
-        for (int b = 0; b < 2; ++b) {
+        for (int b = 0; b < kStages; ++b) {
             umma::MbarInit(&ts.mbar_load[b], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
             umma::MbarInit(&ts.mbar_mma[b], 1);
         }
         ts.failed = 0;
