@@ -30,9 +30,12 @@ sys.path.insert(0, str(ROOT))
 MEASURED = ROOT / "MEASURED_PEAKS.json"
 TRAFFIC = ROOT / "profiles" / "eval_fp32_traffic.json"
 KERNELS_PER_GENERATION = 7  # prepare, evaluate, finalize, summarize, select, plan slots, breed
-FORMS = {"fp32": 0, "tc-bf16": 1, "tc-fp16": 2}
+FORMS = {"fp32": 0, "tc-bf16": 1, "tc-fp16": 2, "tc-trunk-bf16": 3, "tc-trunk-fp16": 4}
 FORM_NAMES = {"fp32": "plain fp32", "tc-bf16": "tensor-core bf16 scoring, exact fp32 re-scoring",
-              "tc-fp16": "tensor-core fp16 scoring, exact fp32 re-scoring"}
+              "tc-fp16": "tensor-core fp16 scoring, exact fp32 re-scoring",
+              "tc-trunk-bf16": "tensor-core bf16 encoder+trunk+scoring, margin guard tau with exact fp32 fallback",
+              "tc-trunk-fp16": "tensor-core fp16 encoder+trunk+scoring, margin guard tau with exact fp32 fallback"}
+EXTRA_KERNELS = {"fp32": 0, "tc-bf16": 1, "tc-fp16": 1, "tc-trunk-bf16": 2, "tc-trunk-fp16": 2}
 
 
 def algorithmic_flops(steps: int, encoded: int, action_count: int) -> float:
@@ -167,6 +170,8 @@ def run_ours(args) -> None:
     rt = nwg.Runtime(wl.action_count, wl.population, wl.columns, stream=stream.cuda_stream)
     rt.set_cell_words(offsets, words)
     rt.set_form(FORMS[args.form])
+    if args.form.startswith("tc-trunk"):
+        rt.set_margin_guard(args.tau)
     rt.bootstrap(wl.population, seed=0 + rank)
     counts = nwg.capi.word_counts(training=wl.action_count, action_space=wl.action_count)
     cfg = nwg.capi.assembly_config(radius=wl.radius, p=wl.mutation_probability, sigma=wl.mutation_sigma)
@@ -197,6 +202,8 @@ def run_ours(args) -> None:
     kernel_ms = []
     rescored = 0
     full = 0
+    candidates = 0
+    fallbacks = 0
     barrier(world)
     torch.cuda.synchronize()
     with ClockSampler(local) as clocks:
@@ -209,6 +216,8 @@ def run_ours(args) -> None:
             kernel_ms.append(st.eval_kernel_ms)
             rescored += st.rescored_chunks
             full += st.full_rescores
+            candidates += st.candidate_chunks
+            fallbacks += st.fallback_steps
             gen += 1
         end.record(stream)
         torch.cuda.synchronize()
@@ -285,8 +294,11 @@ def run_ours(args) -> None:
         "e2e": {"value": e2e_total / (e2e_ms * 1e-3), "unit": "game-steps/s",
                 "h2d_bytes_per_step": int(offsets.nbytes + words.nbytes + 120),
                 "d2h_bytes_per_step": 4 + 48 + 24},
-        "gpu_launches": (KERNELS_PER_GENERATION + (1 if args.form != "fp32" else 0)) * args.steps,
-        "rescoring": {"chunks_per_step": rescored / max(steps, 1), "full_rescore_fraction": full / max(steps, 1)},
+        "gpu_launches": (KERNELS_PER_GENERATION + EXTRA_KERNELS[args.form]) * args.steps,
+        "rescoring": {"chunks_per_step": rescored / max(steps, 1), "full_rescore_fraction": full / max(steps, 1),
+                      "candidate_chunks_per_step": candidates / max(steps, 1),
+                      "fallback_fraction": fallbacks / max(steps, 1),
+                      "margin_tau": args.tau if args.form.startswith("tc-trunk") else None},
         "clocks": clock,
     }
     print(json.dumps(line), flush=True)
@@ -351,6 +363,7 @@ def main() -> None:
     ap.add_argument("--workload", choices=["full", "medium", "small"], default="full")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--form", choices=sorted(FORMS), default="fp32")
+    ap.add_argument("--tau", type=float, default=1e-3, help="margin guard of the tensor-core trunk forms")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define NWG_ABI_VERSION 1
+#define NWG_ABI_VERSION 2
 #define NWG_CATALOG_CAPACITY 4739
 
 enum {
@@ -139,8 +139,10 @@ typedef struct {
     double fitness_mean_fp64;   /* FP64 reductions for the adaptive shard-release statistics */
     double fitness_variance_fp64;
     double eval_kernel_ms;      /* device time of the last evaluation kernel (CUDA events on the runtime's stream) */
-    uint64_t rescored_chunks;   /* tensor-core form: 32-action chunks re-scored exactly in FP32 */
-    uint64_t full_rescores;     /* tensor-core form: game steps re-scored over every action */
+    uint64_t rescored_chunks;   /* tensor-core forms: 32-action chunks re-scored exactly in FP32 */
+    uint64_t full_rescores;     /* tensor-core forms: game steps re-scored in FP32 over every action */
+    uint64_t candidate_chunks;  /* tensor-core trunk forms: chunks re-scored from the 16-bit operands */
+    uint64_t fallback_steps;    /* tensor-core trunk forms: game steps decided by the exact FP32 path */
 } nwg_evaluation_stats;
 
 /* Evaluation forms (nwg_set_evaluation_form). */
@@ -148,6 +150,8 @@ enum {
     NWG_FORM_FP32 = 0,          /* plain form: every score an FP32 fused-multiply-add chain (default) */
     NWG_FORM_TC_BF16 = 1,       /* scores on tcgen05 with BF16 operands, near-top chunks re-scored in FP32 */
     NWG_FORM_TC_FP16 = 2,       /* as above with FP16 operands (tighter bound, fewer re-scored chunks) */
+    NWG_FORM_TC_TRUNK_BF16 = 3, /* encoder, trunk and scores on tcgen05 (BF16 operands), margin-guarded */
+    NWG_FORM_TC_TRUNK_FP16 = 4, /* as above with FP16 operands (the genome's FP16 weights stay exact) */
 };
 
 typedef struct {
@@ -184,11 +188,20 @@ int nwg_set_stream(nwg_runtime *runtime, void *cuda_stream);
 
 int nwg_get_info(const nwg_runtime *runtime, nwg_runtime_info *info);
 
-/* Selects how nwg_evaluate / nwg_advance score actions (NWG_FORM_*). No reference counterpart. Both tensor-core
- * forms keep the FP32 trunk, score on tcgen05 and re-score in FP32 every 32-action chunk within a proven error
- * bound of the best, so their guesses equal the plain form's; they keep a 16-bit embedding table per
- * individual on the device (about 128 bytes per action). */
+/* Selects how nwg_evaluate / nwg_advance score actions (NWG_FORM_*). No reference counterpart. The two
+ * tensor-core scoring forms keep the FP32 trunk, score on tcgen05 and re-score in FP32 every 32-action chunk
+ * within a proven error bound of the best, so their guesses equal the plain form's. The two tensor-core trunk
+ * forms also run the encoder and the trunk on tcgen05 and send uncertain steps through the exact FP32 path
+ * (nwg_set_margin_guard). All four keep a 16-bit embedding table per individual on the device (about 128
+ * bytes per action); the trunk forms add a 296 KB weight table per individual. */
 int nwg_set_evaluation_form(nwg_runtime *runtime, int form);
+
+/* Margin guard of the tensor-core trunk forms (NWG_FORM_TC_TRUNK_*). No reference counterpart. A game step whose
+ * top-2 margin among unguessed actions is below tau * scale, scale = max(|best score|, 0.1 * sum_k |p_k| *
+ * max_a |e_ak|) on the 16-bit scores, is recomputed by the exact FP32 path (the plain form's chains), so its
+ * guess is the plain form's. Default tau = 1e-3; tau = 0 disables the guard (uncertifiable steps still fall
+ * back); a huge tau sends every step through the exact path. Negative or non-finite tau is rejected. */
+int nwg_set_margin_guard(nwg_runtime *runtime, float tau);
 
 /* TryBootstrapRandomCurrentGenerationOnDevice (slab_runtime.hpp:123-124). */
 int nwg_bootstrap(nwg_runtime *runtime, size_t generation_size, uint32_t generation_seed, size_t generation_index);

@@ -77,10 +77,11 @@ class PendingInjection(C.Structure):
 class EvaluationStats(C.Structure):
     _fields_ = [("game_steps", C.c_uint64), ("episodes", C.c_uint64), ("encoded_turns", C.c_uint64),
                 ("fitness_mean_fp64", C.c_double), ("fitness_variance_fp64", C.c_double),
-                ("eval_kernel_ms", C.c_double), ("rescored_chunks", C.c_uint64), ("full_rescores", C.c_uint64)]
+                ("eval_kernel_ms", C.c_double), ("rescored_chunks", C.c_uint64), ("full_rescores", C.c_uint64),
+                ("candidate_chunks", C.c_uint64), ("fallback_steps", C.c_uint64)]
 
 
-FORM_FP32, FORM_TC_BF16, FORM_TC_FP16 = 0, 1, 2
+FORM_FP32, FORM_TC_BF16, FORM_TC_FP16, FORM_TC_TRUNK_BF16, FORM_TC_TRUNK_FP16 = 0, 1, 2, 3, 4
 
 
 class RuntimeInfo(C.Structure):
@@ -94,7 +95,7 @@ SHARD_RELEASE_FN = C.CFUNCTYPE(C.c_bool, _vp, C.POINTER(RuntimeWordCounts), C.PO
 
 EXPORTS = [
     "nwg_abi_version", "nwg_status_string", "nwg_upload_catalog", "nwg_create", "nwg_destroy", "nwg_set_stream",
-    "nwg_get_info", "nwg_set_evaluation_form", "nwg_bootstrap", "nwg_set_cell_words", "nwg_evaluate", "nwg_read_summary",
+    "nwg_get_info", "nwg_set_evaluation_form", "nwg_set_margin_guard", "nwg_bootstrap", "nwg_set_cell_words", "nwg_evaluate", "nwg_read_summary",
     "nwg_read_evaluation_stats", "nwg_advance", "nwg_swap_generations", "nwg_read_status",
     "nwg_download_current_generation", "nwg_download_slot", "nwg_upload_slot", "nwg_upload_current_generation",
     "nwg_download_assembly_plan", "nwg_device_slab", "nwg_evaluate_traced", "nwg_select_parents_device",
@@ -117,6 +118,7 @@ def lib() -> C.CDLL:
     L.nwg_get_info.argtypes = [_vp, C.POINTER(RuntimeInfo)]
     L.nwg_bootstrap.argtypes = [_vp, _sz, C.c_uint32, _sz]
     L.nwg_set_evaluation_form.argtypes = [_vp, C.c_int]
+    L.nwg_set_margin_guard.argtypes = [_vp, C.c_float]
     L.nwg_set_cell_words.argtypes = [_vp, _vp, _vp, _sz]
     L.nwg_evaluate.argtypes = [_vp, C.POINTER(RuntimeWordCounts), C.POINTER(ShardReleaseHistory)]
     L.nwg_read_summary.argtypes = [_vp, C.POINTER(FitnessSummary)]
@@ -239,6 +241,9 @@ class Runtime:
 
     def set_form(self, form: int) -> None:
         check(lib().nwg_set_evaluation_form(self.handle, form), "nwg_set_evaluation_form")
+
+    def set_margin_guard(self, tau: float) -> None:
+        check(lib().nwg_set_margin_guard(self.handle, tau), "nwg_set_margin_guard")
 
     def bootstrap(self, size: int, seed: int, generation_index: int = 0) -> None:
         check(lib().nwg_bootstrap(self.handle, size, seed, generation_index), "nwg_bootstrap")

@@ -76,12 +76,16 @@ struct nwg_runtime {
     int form = NWG_FORM_FP32;
     std::uint8_t *tc_tables = nullptr;
     std::size_t tc_tables_bytes = 0;
+    std::uint8_t *trunk_tables = nullptr;
+    float margin_tau = 1.0e-3f;
 
     // pinned host staging
     ShardRecord *host_shards = nullptr;
     int *host_status = nullptr;
     SummaryDevice *host_summary = nullptr;
-    unsigned long long *host_steps = nullptr;  // [5]: decisions, encoded turns, episodes, re-scored chunks, full
+    // [9]: decisions, encoded turns, episodes, re-scored chunks, full rows (scoring forms), then candidate
+    // chunks, fallback steps, exact chunks, exact rows (trunk forms)
+    unsigned long long *host_steps = nullptr;
     cudaEvent_t eval_begin = nullptr;
     cudaEvent_t eval_end = nullptr;
     std::uint64_t last_episodes = 0;
@@ -91,6 +95,8 @@ struct nwg_runtime {
 };
 
 namespace {
+
+constexpr int kStepCounters = 9;
 
 #define NWG_TRY(expr)                                \
     do {                                             \
@@ -277,7 +283,7 @@ void FreeRuntime(nwg_runtime *rt) {
                            rt->cur_eval,   rt->next_eval,    rt->cur_has,     rt->next_has,    rt->pairs,
                            rt->slot_used,  rt->status,       rt->summary,     rt->shards,      rt->cell_offsets,
                            rt->cell_words, rt->local_words,  rt->chunk_start, rt->score_sum,   rt->steps,
-                           rt->scratch,    rt->tc_tables};
+                           rt->scratch,    rt->tc_tables,    rt->trunk_tables};
     for (void *p : device_ptrs) {
         if (p != nullptr) {
             cudaFree(p);
@@ -349,7 +355,7 @@ int EvaluateImpl(nwg_runtime *rt, const nwg_runtime_word_counts *counts, const n
     NWG_TRY(cudaMemsetAsync(rt->cur_fitness, 0, rt->max_generation_size * sizeof(float), rt->stream));
     NWG_TRY(cudaMemsetAsync(rt->cur_eval, 0, rt->max_generation_size * sizeof(std::uint32_t), rt->stream));
     NWG_TRY(cudaMemsetAsync(rt->cur_has, 0, rt->max_generation_size, rt->stream));
-    NWG_TRY(cudaMemsetAsync(rt->steps, 0, 5 * sizeof(unsigned long long), rt->stream));
+    NWG_TRY(cudaMemsetAsync(rt->steps, 0, kStepCounters * sizeof(unsigned long long), rt->stream));
     NWG_TRY(LaunchEvalPrepare(src, population, static_cast<std::uint32_t>(g_catalog.count), rt->local_words,
                               rt->chunk_start, rt->score_sum, rt->status, rt->stream));
     EvalParams p{};
@@ -378,6 +384,17 @@ int EvaluateImpl(nwg_runtime *rt, const nwg_runtime_word_counts *counts, const n
         NWG_TRY(cudaEventRecord(rt->eval_begin, rt->stream));
         NWG_TRY(LaunchEvalFp32(p, rt->scratch_ctas, rt->stream));
         NWG_TRY(cudaEventRecord(rt->eval_end, rt->stream));
+    } else if (rt->form == NWG_FORM_TC_TRUNK_BF16 || rt->form == NWG_FORM_TC_TRUNK_FP16) {
+        const bool fp16 = rt->form == NWG_FORM_TC_TRUNK_FP16;
+        NWG_TRY(LaunchBuildTcTables(rt->slab, rt->pitch, rt->cur_slots, population, g_catalog.fixed_t,
+                                    static_cast<std::uint32_t>(g_catalog.pad), static_cast<std::uint32_t>(selectable),
+                                    rt->tc_tables, fp16, rt->stream));
+        NWG_TRY(LaunchBuildTrunkTables(rt->slab, rt->pitch, rt->cur_slots, population, rt->trunk_tables, fp16,
+                                       rt->stream));
+        NWG_TRY(cudaEventRecord(rt->eval_begin, rt->stream));
+        NWG_TRY(LaunchEvalTct(p, rt->tc_tables, TcTablePitch(static_cast<std::uint32_t>(selectable)), rt->trunk_tables,
+                              rt->margin_tau, fp16, rt->steps + 5, rt->scratch_ctas, rt->stream));
+        NWG_TRY(cudaEventRecord(rt->eval_end, rt->stream));
     } else {
         const bool fp16 = rt->form == NWG_FORM_TC_FP16;
         // |16-bit product - FP32 product| <= (2u + u^2)|p||e| with u = 2^-8 (BF16: p and e rounded) or 2^-11 (FP16:
@@ -396,7 +413,7 @@ int EvaluateImpl(nwg_runtime *rt, const nwg_runtime_word_counts *counts, const n
     NWG_TRY(LaunchSummarize(rt->cur_fitness, rt->cur_has, rt->cur_slots, population, rt->summary, rt->status,
                             rt->stream));
     NWG_TRY(cudaMemcpyAsync(rt->host_summary, rt->summary, sizeof(SummaryDevice), cudaMemcpyDeviceToHost, rt->stream));
-    NWG_TRY(cudaMemcpyAsync(rt->host_steps, rt->steps, 5 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+    NWG_TRY(cudaMemcpyAsync(rt->host_steps, rt->steps, kStepCounters * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                             rt->stream));
     rt->last_eval_population = population;
     rt->last_action_count = rt->action_count;
@@ -532,19 +549,19 @@ int nwg_create(const nwg_runtime_config *config, nwg_runtime **runtime_out) {
     alloc(&rt->local_words, max_gen * sizeof(std::uint32_t));
     alloc(&rt->chunk_start, (max_gen + 1) * sizeof(std::uint32_t));
     alloc(&rt->score_sum, max_gen * sizeof(std::uint32_t));
-    alloc(&rt->steps, 5 * sizeof(unsigned long long));
+    alloc(&rt->steps, kStepCounters * sizeof(unsigned long long));
     alloc(&rt->scratch, static_cast<std::size_t>(rt->scratch_ctas) * EvalScratchFloatsPerCta() * sizeof(float));
     ok = ok && cudaMallocHost(&rt->host_shards, NWG_CATALOG_CAPACITY * sizeof(ShardRecord)) == cudaSuccess;
     ok = ok && cudaMallocHost(&rt->host_status, sizeof(int)) == cudaSuccess;
     ok = ok && cudaMallocHost(&rt->host_summary, sizeof(SummaryDevice)) == cudaSuccess;
-    ok = ok && cudaMallocHost(&rt->host_steps, 5 * sizeof(unsigned long long)) == cudaSuccess;
+    ok = ok && cudaMallocHost(&rt->host_steps, kStepCounters * sizeof(unsigned long long)) == cudaSuccess;
     ok = ok && cudaEventCreate(&rt->eval_begin) == cudaSuccess && cudaEventCreate(&rt->eval_end) == cudaSuccess;
     if (!ok) {
         FreeRuntime(rt);
         return kCudaFailure;
     }
     std::memset(rt->host_summary, 0, sizeof(SummaryDevice));
-    std::memset(rt->host_steps, 0, 5 * sizeof(unsigned long long));
+    std::memset(rt->host_steps, 0, kStepCounters * sizeof(unsigned long long));
     *runtime_out = rt;
     return kOk;
 }
@@ -580,8 +597,14 @@ int nwg_get_info(const nwg_runtime *rt, nwg_runtime_info *info) {
 }
 
 int nwg_set_evaluation_form(nwg_runtime *rt, int form) {
-    if (rt == nullptr || form < NWG_FORM_FP32 || form > NWG_FORM_TC_FP16) {
+    if (rt == nullptr || form < NWG_FORM_FP32 || form > NWG_FORM_TC_TRUNK_FP16) {
         return kInvalidRuntimeConfig;
+    }
+    if ((form == NWG_FORM_TC_TRUNK_BF16 || form == NWG_FORM_TC_TRUNK_FP16) && rt->trunk_tables == nullptr) {
+        if (cudaMalloc(&rt->trunk_tables, rt->max_generation_size * TrunkTablePitch()) != cudaSuccess) {
+            rt->trunk_tables = nullptr;
+            return kCudaFailure;
+        }
     }
     if (form != NWG_FORM_FP32 && rt->tc_tables == nullptr) {
         const std::size_t bytes = rt->max_generation_size * TcTablePitch(static_cast<std::uint32_t>(rt->action_count));
@@ -592,6 +615,14 @@ int nwg_set_evaluation_form(nwg_runtime *rt, int form) {
         rt->tc_tables_bytes = bytes;
     }
     rt->form = form;
+    return kOk;
+}
+
+int nwg_set_margin_guard(nwg_runtime *rt, float tau) {
+    if (rt == nullptr || !(tau >= 0.0f) || !(tau <= 3.0e38f)) {
+        return kInvalidRuntimeConfig;
+    }
+    rt->margin_tau = tau;
     return kOk;
 }
 
@@ -705,8 +736,10 @@ int nwg_read_evaluation_stats(const nwg_runtime *rt, nwg_evaluation_stats *stats
     stats->game_steps = rt->host_steps[0];
     stats->encoded_turns = rt->host_steps[1];
     stats->episodes = rt->host_steps[2];
-    stats->rescored_chunks = rt->host_steps[3];
-    stats->full_rescores = rt->host_steps[4];
+    stats->rescored_chunks = rt->host_steps[3] + rt->host_steps[7];
+    stats->full_rescores = rt->host_steps[4] + rt->host_steps[8];
+    stats->candidate_chunks = rt->host_steps[5];
+    stats->fallback_steps = rt->host_steps[6];
     stats->fitness_mean_fp64 = rt->host_summary->mean_fp64;
     stats->fitness_variance_fp64 = rt->host_summary->variance_fp64;
     float ms = 0.0f;

@@ -231,8 +231,9 @@ __device__ __forceinline__ void SetupGames(const EvalParams &p, ChunkState &st, 
             }
         }
     }
-    // layer-1 accumulators start at the bias (the virgin-flag term of a non-virgin state adds a zero)
-    for (int idx = tid; idx < kScratchFloats / 4; idx += kEvalThreads) {
+    // layer-1 accumulators start at the bias (the virgin-flag term of a non-virgin state adds a zero);
+    // a form that keeps no FP32 layer-1 accumulators passes no scratch
+    for (int idx = tid; scratch != nullptr && idx < kScratchFloats / 4; idx += kEvalThreads) {
         const int o = (idx * 4) / kChunkGames;
         const float b = H2F(gh, kTrB1 + o);
         reinterpret_cast<float4 *>(scratch)[idx] = make_float4(b, b, b, b);

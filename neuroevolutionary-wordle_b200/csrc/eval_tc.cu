@@ -19,16 +19,15 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
-#include "eval_common.cuh"
-#include "umma.cuh"
+#include "tc_common.cuh"
 
 namespace nwg {
 namespace {
 
 using namespace evalx;
+using namespace tcx;
 
 constexpr int kTileN = 128;                  // actions per MMA tile
-constexpr int kTopK = 4;                     // chunk maxima kept per thread (per game half)
 constexpr std::uint32_t kTmemColumns = 256;  // two 128-column FP32 accumulators
 constexpr std::uint32_t kWaitLimit = 1u << 26;
 constexpr int kTileBytes = kTileN * kPolicy * 2;  // 16 KB of 16-bit embeddings per tile
@@ -67,93 +66,6 @@ struct TcParams {
     int fp16_operands;
     unsigned long long *tc_counters;  // [0] re-scored chunks, [1] games re-scored over every action
 };
-
-__device__ __forceinline__ std::uint32_t OrderedBits(float f) {
-    const std::uint32_t u = __float_as_uint(f);
-    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
-}
-
-__device__ __forceinline__ float FromOrderedBits(std::uint32_t u) {
-    return __uint_as_float((u & 0x80000000u) ? (u & 0x7FFFFFFFu) : ~u);
-}
-
-__device__ __forceinline__ unsigned long long PackKey(float score, std::uint32_t action) {
-    return (static_cast<unsigned long long>(OrderedBits(score)) << 32) | (0xFFFFFFFFu - action);
-}
-
-__device__ __forceinline__ void BulkLoad(void *dst, const void *src, std::uint32_t bytes, std::uint64_t *mbar) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(umma::SmemAddress(mbar)), "r"(bytes)
-                 : "memory");
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-            umma::SmemAddress(dst)),
-        "l"(src), "r"(bytes), "r"(umma::SmemAddress(mbar))
-        : "memory");
-}
-
-// Insert x (chunk id xi) into the descending list v[0..3].
-__device__ __forceinline__ void InsertTop4(float (&v)[kTopK], int (&id)[kTopK], float x, int xi) {
-#pragma unroll
-    for (int j = 0; j < kTopK; ++j) {
-        const bool c = x > v[j];
-        const float tv = c ? v[j] : x;
-        const int ti = c ? id[j] : xi;
-        v[j] = c ? x : v[j];
-        id[j] = c ? xi : id[j];
-        x = tv;
-        xi = ti;
-    }
-}
-
-// Exact FP32 score of action a for game g (the plain form's chain: output_embedding.hpp:98-119).
-// All 64 embedding values are loaded before the chain starts, so a call costs one memory latency.
-__device__ __forceinline__ float ExactScore(const EvalParams &p, const float *pv, int g, const __half *tail,
-                                            std::uint32_t a) {
-    float e[kPolicy];
-#pragma unroll
-    for (int k = 0; k < kFixedDim; ++k) {
-        e[k] = p.fixed_t[static_cast<std::size_t>(k) * p.action_pad + a];
-    }
-    const __half2 *row = reinterpret_cast<const __half2 *>(tail + static_cast<std::size_t>(a) * kTailDim);
-#pragma unroll
-    for (int j = 0; j < kTailDim / 2; ++j) {
-        const float2 f = __half22float2(row[j]);
-        e[kFixedDim + 2 * j] = f.x;
-        e[kFixedDim + 2 * j + 1] = f.y;
-    }
-    float s = 0.0f;
-#pragma unroll
-    for (int k = 0; k < kPolicy; ++k) {
-        s = __fmaf_rn(pv[k * kLd + g], e[k], s);
-    }
-    return s;
-}
-
-// Warp-cooperative exact re-scoring of chunk `chunk` (32 actions) for game g; folds the masked argmax
-// into st.best_key[g].
-__device__ __forceinline__ void RescoreChunk(const EvalParams &p, const ChunkState &cs, unsigned long long *best_key,
-                                             const float *pv, const __half *tail, int g, int chunk, int turns) {
-    const int lane = threadIdx.x & 31;
-    const std::uint32_t a = static_cast<std::uint32_t>(chunk) * 32u + lane;
-    unsigned long long key = 0;
-    if (a < p.action_count) {
-        const std::uint32_t code = p.codes[a];
-        bool masked = false;
-        for (int u = 0; u < turns; ++u) {
-            masked |= cs.guess[u][g] == code;
-        }
-        if (!masked) {
-            key = PackKey(ExactScore(p, pv, g, tail, a), a);
-        }
-    }
-    for (int off = 16; off > 0; off >>= 1) {
-        const unsigned long long other = __shfl_xor_sync(0xffffffffu, key, off);
-        key = other > key ? other : key;
-    }
-    if (lane == 0 && key != 0) {
-        atomicMax(&best_key[g], key);
-    }
-}
 
 template <bool kFp16>
 __device__ void ScoreTensorCores(const TcParams &q, ChunkState &cs, TcState &ts, const __half *gh, float *arena,
@@ -385,8 +297,8 @@ __device__ void ScoreTensorCores(const TcParams &q, ChunkState &cs, TcState &ts,
     const int first_full = ts.full_count;
     for (int k = warp; k < tasks; k += kEvalThreads / 32) {
         const std::uint32_t task = task_list[k];
-        RescoreChunk(p, cs, best_key, pv, tail, static_cast<int>(task >> 16), static_cast<int>(task & 0xFFFFu),
-                     turns_now);
+        const int tg = static_cast<int>(task >> 16);
+        RescoreChunk(p, cs, best_key + tg, pv + tg, kLd, tail, tg, static_cast<int>(task & 0xFFFFu), turns_now);
     }
     __syncthreads();
     // a game whose exact best stays below top - eps, or whose task list overflowed, is re-scored in full
@@ -409,7 +321,7 @@ __device__ void ScoreTensorCores(const TcParams &q, ChunkState &cs, TcState &ts,
     for (int i = 0; i < full_count; ++i) {
         const int g = full_rows[i];
         for (int chunk = warp; chunk < chunks_per_row; chunk += kEvalThreads / 32) {
-            RescoreChunk(p, cs, best_key, pv, tail, g, chunk, turns_now);
+            RescoreChunk(p, cs, best_key + g, pv + g, kLd, tail, g, chunk, turns_now);
         }
     }
     __syncthreads();

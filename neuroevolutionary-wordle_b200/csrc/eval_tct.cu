@@ -1,0 +1,1288 @@
+// Fitness evaluation, tensor-core trunk form: encoder, trunk and action scoring on tcgen05 with 16-bit
+// operands (FP16 or BF16) and FP32 accumulation in tensor memory; a margin guard sends every uncertain
+// game step through the exact FP32 path.
+//
+// A CTA of 256 threads owns a chunk of up to 128 games of one individual (the same chunks as the plain
+// form). Per game step, with t turns on the board:
+//   encoder   the new turn's 145 one-hot features x W_e1 (K = 160), + bias, ReLU, x W_e2 -> 64 values,
+//             kept as a 16-bit operand tile in the CTA's global scratch (one 16 KB tile per turn);
+//   layer 1   sum over the t turn tiles of enc_u x W1[:, 1 + 64u .. 64 + 64u]^T (N = 256), + bias, ReLU;
+//             with no turn on the board every row is relu(b1 + W1[:, 0]);
+//   layer 2   (K = 256, N = 128), + bias, ReLU;  layer 3  (K = 128, N = 64), + bias -> policy p~;
+//   scoring   p~ (16-bit) against the individual's 16-bit embedding table, 128 actions per MMA tile,
+//             keeping per game the four largest 32-action chunk maxima of each half of the columns.
+// Decision: the chunks within the guard bound of the best chunk free of guessed words are re-scored on
+// CUDA cores from the same 16-bit operands; the guess is the best unguessed action when its margin over
+// every other unguessed action is at least tau * scale, scale = max(|best score|, 0.1 * sum_k |p~_k| *
+// max_a |e_ak|). Otherwise (and whenever the tracked chunks cannot certify the margin) the game step
+// falls back: its policy is recomputed with the plain form's exact FP32 chains and its guess is the
+// exact FP32 argmax, found by re-scoring every chunk that the tensor-core maxima cannot rule out
+// (|s~ - s| <= sum_k |p~_k - p_k| max_a |e_ak| + accumulation slack).
+// All weight operands come from a per-individual table in the tensor-core layout (BuildTrunkTables);
+// every mbarrier wait is bounded and a wait that gives up records NWG_TIMEOUT.
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include "tc_common.cuh"
+
+namespace nwg {
+namespace {
+
+using namespace evalx;
+using namespace tcx;
+
+constexpr int kPageBytes = 16384;
+constexpr int kPages = 6;
+constexpr int kSmemBytes = kPages * kPageBytes;
+constexpr int kTileN = 128;
+constexpr int kEmbedStages = 5;  // scoring stages live in pages 1..5
+constexpr std::uint32_t kTmemColumns = 256;
+constexpr std::uint32_t kWaitLimit = 1u << 26;
+constexpr int kKe1 = 160;  // encoder input features (145) padded to a multiple of 16
+constexpr int kFallbackBatch = 8;
+
+// Per-individual trunk table (bytes): K-major canonical operand tiles, rows = output neurons.
+constexpr int kTblWe1 = 0;                                          // [128][160]
+constexpr int kTblWe2 = kTblWe1 + kEncoderHidden * kKe1 * 2;        // [64][128]
+constexpr int kTblW1 = kTblWe2 + kEncoderOut * kEncoderHidden * 2;  // 5 x [256][64]
+constexpr int kW1SlotBytes = kHidden0 * kEncoderOut * 2;
+constexpr int kTblW2 = kTblW1 + 5 * kW1SlotBytes;                   // 4 x [128][64]
+constexpr int kW2ChunkBytes = kHidden1 * 64 * 2;
+constexpr int kTblW3 = kTblW2 + 4 * kW2ChunkBytes;                  // [64][128]
+constexpr int kTrunkTableBytes = kTblW3 + kPolicy * kHidden1 * 2;
+static_assert(kTrunkTableBytes == 303104, "trunk table layout");
+static_assert(kTrunkTableBytes % (16 * 256) == 0, "table build grid covers whole 16-byte segments");
+
+// Post-scoring shared-memory layout (byte offsets into the page arena; page 0 keeps the policy operand).
+constexpr int kOffCandV = 1 * kPageBytes;                            // [128 games][2 halves][4] floats
+constexpr int kOffCandId = kOffCandV + kChunkGames * 2 * kTopK * 4;  // ids
+constexpr int kOffExcl = kOffCandId + kChunkGames * 2 * kTopK * 4;   // [128] max score outside the candidates
+constexpr int kOffTaskOff = kOffExcl + kChunkGames * 4;              // [128] first task of each game
+constexpr int kOffTaskCnt = kOffTaskOff + kChunkGames * 4;           // [128] candidate chunks per game
+constexpr int kOffFbKey = kOffTaskCnt + kChunkGames * 4;             // [8] exact best keys (u64)
+constexpr int kOffFbWin = kOffFbKey + kFallbackBatch * 8;            // [8] exact window low ends
+constexpr int kOffFbFull = kOffFbWin + kFallbackBatch * 4;           // [8] full re-score flags
+constexpr int kOffFbTasks = kOffFbFull + kFallbackBatch * 4;         // [64] exact tasks (batch game << 16 | chunk)
+constexpr int kOffFbCount = kOffFbTasks + kFallbackBatch * 2 * kTopK * 4;
+constexpr int kMaxCandTasks = kChunkGames * 2 * kTopK;
+constexpr int kOffTasks = 2 * kPageBytes;                   // [1024] (game << 16) | chunk
+constexpr int kOffResults = kOffTasks + kMaxCandTasks * 4;  // [1024][2] u64 top-2 keys
+static_assert(kOffResults + kMaxCandTasks * 16 <= kSmemBytes, "task buffers");
+// exact fallback buffers (reuse the task region once the approximate decisions are made)
+constexpr int kOffXEnc = 26624;                                                 // [8][5][64] f32
+constexpr int kOffXHid = kOffXEnc + kFallbackBatch * 5 * kEncoderOut * 4;       // [8][5][128] f32
+constexpr int kOffXH0 = kOffXHid;                                               // [8][256], once hid is dead
+constexpr int kOffXH1 = kOffXH0 + kFallbackBatch * kHidden0 * 4;                // [8][128]
+constexpr int kOffXP = kOffXH1 + kFallbackBatch * kHidden1 * 4;                 // [8][64]
+constexpr int kOffXStage = kOffXHid + kFallbackBatch * 5 * kEncoderHidden * 4;  // staged encoder weights
+static_assert(kOffFbCount + 16 <= kOffXEnc, "decision buffers overlap the fallback buffers");
+static_assert(kOffXP + kFallbackBatch * kPolicy * 4 <= kOffXStage, "fallback buffers");
+static_assert(kOffXStage + kEncoderHidden * kTurnFeatures * 2 <= kSmemBytes, "staged encoder weights");
+static_assert((kEncoderHidden * kTurnFeatures * 2) % 16 == 0, "W_e1 copies as 16-byte words");
+
+struct TctState {
+    std::uint64_t bar_load[kPages];  // bulk loads into page p (at most one outstanding per barrier)
+    std::uint64_t bar_free[2];       // trunk operand stages released by completed MMAs
+    std::uint64_t bar_mma;           // a trunk phase's MMAs have completed
+    std::uint64_t bar_acc[2];        // scoring accumulator buffers
+    std::uint64_t bar_drain;
+    std::uint32_t tmem_base;
+    int failed;
+    int n_fallback;
+    int scan[4];
+    int fallback_games[kChunkGames];
+    float be1[kEncoderHidden];
+    float be2[kEncoderOut];
+    float b1[kHidden0];
+    float b2[kHidden1];
+    float b3[kPolicy];
+    float virgin[kHidden0];  // relu(b1 + W1[:, 0])
+    float emax[kPolicy];
+    float s_part[2][kChunkGames];
+};
+
+struct TctParams {
+    EvalParams base;
+    const std::uint8_t *embed_tables;  // per individual: 256-byte header (emax[64]) + A_pad x 64 16-bit values
+    std::size_t embed_pitch;
+    const std::uint8_t *trunk_tables;  // per individual: kTrunkTableBytes
+    std::size_t trunk_pitch;
+    float tau;
+    unsigned long long *counters;  // [0] candidate chunks, [1] fallback steps, [2] exact chunks, [3] exact rows
+};
+
+template <bool kFp16>
+__device__ __forceinline__ std::uint32_t Pack2(float a, float b) {
+    if constexpr (kFp16) {
+        const __half2 h = __floats2half2_rn(a, b);
+        return *reinterpret_cast<const std::uint32_t *>(&h);
+    } else {
+        const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+        return *reinterpret_cast<const std::uint32_t *>(&h);
+    }
+}
+
+template <bool kFp16>
+__device__ __forceinline__ float2 Unpack2(std::uint32_t bits) {
+    if constexpr (kFp16) {
+        return __half22float2(*reinterpret_cast<const __half2 *>(&bits));
+    } else {
+        return __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&bits));
+    }
+}
+
+template <bool kFp16>
+__device__ __forceinline__ std::uint16_t One16() {
+    return kFp16 ? std::uint16_t{0x3C00} : std::uint16_t{0x3F80};
+}
+
+template <bool kFp16>
+__host__ __device__ constexpr std::uint32_t InstrDesc(int m, int n) {
+    return kFp16 ? (umma::InstrDescBf16(m, n) & ~((7u << 7) | (7u << 10))) : umma::InstrDescBf16(m, n);
+}
+
+// Stores 32 consecutive FP32 columns c0..c0+31 of row g, rounded to 16 bits, into a K-wide operand tile.
+template <bool kFp16>
+__device__ __forceinline__ void StoreRow32(std::uint8_t *tile, int g, int c0, int K, const float (&v)[32]) {
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+        uint4 w;
+        w.x = Pack2<kFp16>(v[8 * s + 0], v[8 * s + 1]);
+        w.y = Pack2<kFp16>(v[8 * s + 2], v[8 * s + 3]);
+        w.z = Pack2<kFp16>(v[8 * s + 4], v[8 * s + 5]);
+        w.w = Pack2<kFp16>(v[8 * s + 6], v[8 * s + 7]);
+        *reinterpret_cast<uint4 *>(tile + umma::TileOffset(g, c0 + 8 * s, K)) = w;
+    }
+}
+
+// D (+)= A x B^T over K (a multiple of 16), both operands K-major canonical tiles; one thread issues.
+__device__ __forceinline__ void MmaK(std::uint32_t d, const std::uint8_t *a, int a_k, const std::uint8_t *b, int b_k,
+                                     int k_steps, std::uint32_t idesc, bool accumulate) {
+    const std::uint32_t a_addr = umma::SmemAddress(a);
+    const std::uint32_t b_addr = umma::SmemAddress(b);
+    for (int s = 0; s < k_steps; ++s) {
+        const std::uint64_t ad = umma::SmemDescriptor(a_addr + s * 256, 128, (a_k / 8) * 128);
+        const std::uint64_t bd = umma::SmemDescriptor(b_addr + s * 256, 128, (b_k / 8) * 128);
+        umma::Mma(d, ad, bd, idesc, accumulate || s > 0);
+    }
+}
+
+// Approximate score (16-bit operands, FP32 accumulation) of action a for game g: the policy row of the
+// operand tile against the action's row of the embedding table.
+template <bool kFp16>
+__device__ __forceinline__ float ApproxScore(const std::uint8_t *a_tile, int g, const std::uint8_t *embed,
+                                             std::uint32_t a) {
+    const std::uint8_t *erow = embed + static_cast<std::size_t>(a >> 7) * (kTileN * kPolicy * 2) +
+                               umma::TileOffset(a & 127u, 0, kPolicy);
+    uint4 e[8];
+#pragma unroll
+    for (int kg = 0; kg < 8; ++kg) {
+        e[kg] = __ldg(reinterpret_cast<const uint4 *>(erow + kg * 128));
+    }
+    float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+    for (int kg = 0; kg < 8; ++kg) {
+        const uint4 pw = *reinterpret_cast<const uint4 *>(a_tile + umma::TileOffset(g, kg * 8, kPolicy));
+        const std::uint32_t pv[4] = {pw.x, pw.y, pw.z, pw.w};
+        const std::uint32_t ev[4] = {e[kg].x, e[kg].y, e[kg].z, e[kg].w};
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const float2 pp = Unpack2<kFp16>(pv[i]);
+            const float2 ee = Unpack2<kFp16>(ev[i]);
+            acc[i] = __fmaf_rn(pp.x, ee.x, acc[i]);
+            acc[i] = __fmaf_rn(pp.y, ee.y, acc[i]);
+        }
+    }
+    return (acc[0] + acc[1]) + (acc[2] + acc[3]);
+}
+
+template <bool kFp16>
+__global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams q) {
+    extern __shared__ __align__(1024) std::uint8_t smem[];
+    __shared__ ChunkState cs;
+    __shared__ TctState ts;
+    const EvalParams &p = q.base;
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5;
+    const int lane = tid & 31;
+    const int quad = warp & 3;
+    const int half = warp >> 2;
+    const int row = quad * 32 + lane;  // TMEM lane = game row this thread reads back
+    const std::uint32_t lane_bits = static_cast<std::uint32_t>(quad * 32) << 16;
+    auto page = [&](int i) { return smem + i * kPageBytes; };
+    std::uint8_t *enc_scratch =
+        reinterpret_cast<std::uint8_t *>(p.scratch + static_cast<std::size_t>(blockIdx.x) * kScratchFloats);
+    unsigned long long decisions = 0, encoded = 0, episodes = 0;
+    unsigned long long cand_chunks = 0, fallback_steps = 0, exact_chunks = 0, exact_rows = 0;
+    // thread 0 only: bulk loads issued / waited per barrier, commits per stage barrier
+    std::uint32_t load_issued[kPages] = {0, 0, 0, 0, 0, 0};
+    std::uint32_t load_waited[kPages] = {0, 0, 0, 0, 0, 0};
+    std::uint32_t free_commits[2] = {0, 0};
+    // every thread: commits to the phase and accumulator barriers
+    std::uint32_t mma_commits = 0;
+    std::uint32_t acc_commits[2] = {0, 0};
+    const std::uint32_t total_chunks = p.chunk_start[p.population];
+    const std::uint32_t idesc128 = InstrDesc<kFp16>(128, 128);
+    const std::uint32_t idesc64 = InstrDesc<kFp16>(128, 64);
+    const std::uint32_t idesc256 = InstrDesc<kFp16>(128, 256);
+    const int n_tiles = static_cast<int>((p.action_count + kTileN - 1) / kTileN);
+
+    if (tid < 32) {
+        umma::Alloc(&ts.tmem_base, kTmemColumns);
+    }
+    if (tid == 0) {
+        for (int b = 0; b < kPages; ++b) {
+            umma::MbarInit(&ts.bar_load[b], 1);
+        }
+        umma::MbarInit(&ts.bar_free[0], 1);
+        umma::MbarInit(&ts.bar_free[1], 1);
+        umma::MbarInit(&ts.bar_mma, 1);
+        umma::MbarInit(&ts.bar_acc[0], 1);
+        umma::MbarInit(&ts.bar_acc[1], 1);
+        umma::MbarInit(&ts.bar_drain, 1);
+        ts.failed = 0;
+    }
+    umma::FenceBeforeSync();
+    __syncthreads();
+    umma::FenceAfterSync();
+    const std::uint32_t tmem = ts.tmem_base;
+
+    auto wait_bar = [&](std::uint64_t *bar, std::uint32_t parity) {
+        if (*reinterpret_cast<volatile int *>(&ts.failed) != 0) {
+            return;
+        }
+        if (!umma::MbarWait(bar, parity, kWaitLimit)) {
+            ts.failed = 1;
+        }
+    };
+    // thread 0 only
+    auto load = [&](int b, void *dst, const void *src, std::uint32_t bytes) {
+        BulkLoad(dst, src, bytes, &ts.bar_load[b]);
+        ++load_issued[b];
+    };
+    auto wait_load = [&](int b) {
+        wait_bar(&ts.bar_load[b], load_waited[b] & 1u);
+        ++load_waited[b];
+    };
+    auto commit_free = [&](int s) {
+        umma::Commit(&ts.bar_free[s]);
+        ++free_commits[s];
+    };
+    auto wait_free = [&](int s) { wait_bar(&ts.bar_free[s], (free_commits[s] - 1u) & 1u); };
+    // every thread (uniform control flow)
+    auto commit_mma = [&]() {
+        if (tid == 0) {
+            umma::Commit(&ts.bar_mma);
+        }
+        ++mma_commits;
+    };
+    auto wait_mma = [&]() {
+        wait_bar(&ts.bar_mma, (mma_commits - 1u) & 1u);
+        umma::FenceAfterSync();
+    };
+    auto phase_sync = [&]() {  // generic smem writes -> visible to the tensor core; TMEM reads ordered
+        umma::FenceProxyAsyncShared();
+        umma::FenceBeforeSync();
+        __syncthreads();
+        umma::FenceAfterSync();
+    };
+
+    for (std::uint32_t chunk = blockIdx.x; chunk < total_chunks; chunk += gridDim.x) {
+        if (!BeginChunk(p, cs, chunk) || ts.failed) {
+            break;
+        }
+        const std::uint32_t ind = static_cast<std::uint32_t>(cs.individual);
+        const __half *gh = reinterpret_cast<const __half *>(p.slab + static_cast<std::size_t>(cs.slot) * p.pitch);
+        const std::uint8_t *ttab = q.trunk_tables + static_cast<std::size_t>(ind) * q.trunk_pitch;
+        const std::uint8_t *etab = q.embed_tables + static_cast<std::size_t>(ind) * q.embed_pitch;
+        const std::uint8_t *embed = etab + 256;
+        SetupGames(p, cs, gh, nullptr);
+        for (int i = tid; i < kHidden0; i += kEvalThreads) {
+            const float b = H2F(gh, kTrB1 + i);
+            ts.b1[i] = b;
+            const float v = __fmaf_rn(H2F(gh, kTrW1 + i * kModelInput), 1.0f, b);
+            ts.virgin[i] = v < 0.0f ? 0.0f : v;
+            if (i < kEncoderHidden) {
+                ts.be1[i] = H2F(gh, kEncB1 + i);
+                ts.b2[i] = H2F(gh, kTrB2 + i);
+            }
+            if (i < kPolicy) {
+                ts.be2[i] = H2F(gh, kEncB2 + i);
+                ts.b3[i] = H2F(gh, kTrB3 + i);
+                ts.emax[i] = reinterpret_cast<const float *>(etab)[i];
+            }
+        }
+        __syncthreads();
+
+        // ---- encoder: turn u of every game -> 16-bit tile in page 2 and in the CTA's scratch slot u ----
+        auto encode_turn = [&](int u) {
+            std::uint8_t *onehot = page(0);                // [128][160], 40 KB
+            std::uint8_t *we1 = page(0) + 128 * kKe1 * 2;  // [128][160], 40 KB (pages 2.5 .. 5)
+            std::uint8_t *a_h = page(0);                   // [128][128] hidden operand, after the first MMA
+            std::uint8_t *enc = page(2);                   // [128][64]
+            if (tid == 0) {
+                umma::FenceProxyAsyncShared();
+                load(2, we1, ttab + kTblWe1, 128 * kKe1 * 2);
+                load(5, page(5), ttab + kTblWe2, kEncoderOut * kEncoderHidden * 2);
+            }
+            for (int i = tid; i < 128 * kKe1 * 2 / 16; i += kEvalThreads) {
+                reinterpret_cast<uint4 *>(onehot)[i] = make_uint4(0, 0, 0, 0);
+            }
+            __syncthreads();
+            for (int i = tid; i < kChunkGames * 10; i += kEvalThreads) {
+                const int g = i / 10;
+                const int f = i - g * 10;
+                const std::uint32_t code = cs.guess[u][g];
+                const std::uint32_t tiles = cs.tiles[u][g];
+                const int feature = f < kWordLength ? f * kAlphabet + static_cast<int>(WordLetter(code, f))
+                                                    : kWordLength * kAlphabet + (f - kWordLength) * 3 +
+                                                          static_cast<int>((tiles >> (2 * (f - kWordLength))) & 3u);
+                *reinterpret_cast<std::uint16_t *>(onehot + umma::TileOffset(g, feature, kKe1)) = One16<kFp16>();
+            }
+            phase_sync();
+            if (tid == 0) {
+                wait_load(2);
+                umma::FenceAfterSync();
+                MmaK(tmem, onehot, kKe1, we1, kKe1, kKe1 / 16, idesc128, false);
+            }
+            commit_mma();
+            wait_mma();
+            {
+                float v[32];
+#pragma unroll
+                for (int j = 0; j < 2; ++j) {
+                    const int c0 = half * 64 + j * 32;
+                    umma::Load32(tmem + static_cast<std::uint32_t>(c0) + lane_bits, v);
+#pragma unroll
+                    for (int i = 0; i < 32; ++i) {
+                        const float h = v[i] + ts.be1[c0 + i];
+                        v[i] = h < 0.0f ? 0.0f : h;
+                    }
+                    StoreRow32<kFp16>(a_h, row, c0, kEncoderHidden, v);
+                }
+            }
+            phase_sync();
+            if (tid == 0) {
+                wait_load(5);
+                umma::FenceAfterSync();
+                MmaK(tmem + 128, a_h, kEncoderHidden, page(5), kEncoderHidden, kEncoderHidden / 16, idesc64, false);
+            }
+            commit_mma();
+            wait_mma();
+            {
+                float v[32];
+                const int c0 = half * 32;
+                umma::Load32(tmem + 128u + static_cast<std::uint32_t>(c0) + lane_bits, v);
+#pragma unroll
+                for (int i = 0; i < 32; ++i) {
+                    v[i] += ts.be2[c0 + i];
+                }
+                StoreRow32<kFp16>(enc, row, c0, kEncoderOut, v);
+                StoreRow32<kFp16>(enc_scratch + u * kPageBytes, row, c0, kEncoderOut, v);
+            }
+            asm volatile("fence.proxy.async.global;" ::: "memory");
+            phase_sync();
+        };
+
+        // ---- trunk at turn count t: leaves the 16-bit policy operand in page 0 ----
+        auto trunk = [&](int t, int step) {
+            std::uint8_t *h0 = page(0);  // [128][256], pages 0..3
+            if (t == 0) {
+                for (int i = tid; i < kChunkGames * (kHidden0 / 8); i += kEvalThreads) {
+                    const int g = i >> 5;
+                    const int c0 = (i & 31) * 8;
+                    uint4 w;
+                    w.x = Pack2<kFp16>(ts.virgin[c0 + 0], ts.virgin[c0 + 1]);
+                    w.y = Pack2<kFp16>(ts.virgin[c0 + 2], ts.virgin[c0 + 3]);
+                    w.z = Pack2<kFp16>(ts.virgin[c0 + 4], ts.virgin[c0 + 5]);
+                    w.w = Pack2<kFp16>(ts.virgin[c0 + 6], ts.virgin[c0 + 7]);
+                    *reinterpret_cast<uint4 *>(h0 + umma::TileOffset(g, c0, kHidden0)) = w;
+                }
+                if (tid == 0) {
+                    umma::FenceProxyAsyncShared();
+                    load(4, page(4), ttab + kTblW2, kW2ChunkBytes);
+                    load(5, page(5), ttab + kTblW2 + kW2ChunkBytes, kW2ChunkBytes);
+                }
+                phase_sync();
+            } else {
+                // layer 1: stage 0 = {enc page 2, W1 pages 3-4}, stage 1 = {enc page 5, W1 pages 0-1};
+                // turn t-1's tile is already in page 2
+                if (tid == 0) {
+                    umma::FenceProxyAsyncShared();
+                    load(3, page(3), ttab + kTblW1 + (t - 1) * kW1SlotBytes, kW1SlotBytes);
+                    if (t >= 2) {
+                        load(5, page(5), enc_scratch + (t - 2) * kPageBytes, kPageBytes);
+                        load(0, page(0), ttab + kTblW1 + (t - 2) * kW1SlotBytes, kW1SlotBytes);
+                    }
+                    for (int i = 0; i < t; ++i) {
+                        const int u = t - 1 - i;
+                        const int st = i & 1;
+                        const int enc_b = st == 0 ? 2 : 5;
+                        const int w_b = st == 0 ? 3 : 0;
+                        wait_load(w_b);
+                        if (i > 0) {
+                            wait_load(enc_b);
+                        }
+                        umma::FenceAfterSync();
+                        MmaK(tmem, page(enc_b), kEncoderOut, page(w_b), kEncoderOut, kEncoderOut / 16, idesc256,
+                             i > 0);
+                        commit_free(st);
+                        if (i + 2 < t) {
+                            wait_free(st);
+                            load(enc_b, page(enc_b), enc_scratch + (u - 2) * kPageBytes, kPageBytes);
+                            load(w_b, page(w_b), ttab + kTblW1 + (u - 2) * kW1SlotBytes, kW1SlotBytes);
+                        }
+                    }
+                }
+                commit_mma();
+                wait_mma();
+                if (tid == 0) {
+                    umma::FenceProxyAsyncShared();
+                    load(4, page(4), ttab + kTblW2, kW2ChunkBytes);
+                    load(5, page(5), ttab + kTblW2 + kW2ChunkBytes, kW2ChunkBytes);
+                }
+                float v[32];
+#pragma unroll 1
+                for (int j = 0; j < 4; ++j) {
+                    const int c0 = half * 128 + j * 32;
+                    umma::Load32(tmem + static_cast<std::uint32_t>(c0) + lane_bits, v);
+#pragma unroll
+                    for (int i = 0; i < 32; ++i) {
+                        const float h = v[i] + ts.b1[c0 + i];
+                        v[i] = h < 0.0f ? 0.0f : h;
+                    }
+                    StoreRow32<kFp16>(h0, row, c0, kHidden0, v);
+                }
+                phase_sync();
+            }
+            // layer 2: W2 chunks stream through pages 4 and 5; W3 follows into page 4
+            if (tid == 0) {
+                for (int kc = 0; kc < 4; ++kc) {
+                    const int b = 4 + (kc & 1);
+                    wait_load(b);
+                    umma::FenceAfterSync();
+                    MmaK(tmem, h0 + kc * 1024, kHidden0, page(b), 64, 4, idesc128, kc > 0);
+                    commit_free(kc & 1);
+                    if (kc < 2) {
+                        wait_free(kc & 1);
+                        load(b, page(b), ttab + kTblW2 + (kc + 2) * kW2ChunkBytes, kW2ChunkBytes);
+                    } else if (kc == 2) {
+                        wait_free(0);
+                        load(4, page(4), ttab + kTblW3, kPolicy * kHidden1 * 2);
+                    }
+                }
+            }
+            commit_mma();
+            wait_mma();
+            if (tid == 0) {
+                // the first embedding tiles whose pages are free already (stage s lives in page 1 + s)
+                umma::FenceProxyAsyncShared();
+                for (int e = 1; e < kEmbedStages; ++e) {
+                    if (e != 3 && e < n_tiles) {  // stage 3 (page 4) still holds W3
+                        load(1 + e, page(1 + e), embed + static_cast<std::size_t>(e) * kPageBytes, kPageBytes);
+                    }
+                }
+            }
+            {
+                std::uint8_t *h1 = page(0);  // [128][128]
+                float v[32];
+#pragma unroll 1
+                for (int j = 0; j < 2; ++j) {
+                    const int c0 = half * 64 + j * 32;
+                    umma::Load32(tmem + static_cast<std::uint32_t>(c0) + lane_bits, v);
+#pragma unroll
+                    for (int i = 0; i < 32; ++i) {
+                        const float h = v[i] + ts.b2[c0 + i];
+                        v[i] = h < 0.0f ? 0.0f : h;
+                    }
+                    StoreRow32<kFp16>(h1, row, c0, kHidden1, v);
+                }
+            }
+            phase_sync();
+            // layer 3
+            if (tid == 0) {
+                wait_load(4);
+                umma::FenceAfterSync();
+                MmaK(tmem + 128, page(0), kHidden1, page(4), kHidden1, kHidden1 / 16, idesc64, false);
+            }
+            commit_mma();
+            wait_mma();
+            if (tid == 0) {
+                umma::FenceProxyAsyncShared();
+                if (n_tiles > 0) {
+                    load(1, page(1), embed, kPageBytes);
+                }
+                if (n_tiles > 3) {
+                    load(4, page(4), embed + 3 * static_cast<std::size_t>(kPageBytes), kPageBytes);
+                }
+            }
+            {
+                float v[32];
+                const int c0 = half * 32;
+                umma::Load32(tmem + 128u + static_cast<std::uint32_t>(c0) + lane_bits, v);
+#pragma unroll
+                for (int i = 0; i < 32; ++i) {
+                    v[i] += ts.b3[c0 + i];
+                }
+                const std::int32_t e = cs.episode[row];
+                if (p.trace_policy != nullptr && !cs.done[row] && e >= 0 &&
+                    static_cast<std::uint32_t>(e) < p.trace_episodes) {
+                    const std::size_t slot = static_cast<std::size_t>(ind) * p.trace_episodes + e;
+                    float *dst = p.trace_policy + (slot * kMaxTurns + step) * kPolicy + c0;
+#pragma unroll
+                    for (int i = 0; i < 32; ++i) {
+                        dst[i] = v[i];
+                    }
+                }
+                StoreRow32<kFp16>(page(0), row, c0, kPolicy, v);
+                // score scale; a policy value beyond the 16-bit range makes it infinite, which sends the game
+                // step to the exact path
+                float s = 0.0f;
+                bool in_range = true;
+#pragma unroll
+                for (int i = 0; i < 32; i += 2) {
+                    const float2 r = Unpack2<kFp16>(Pack2<kFp16>(v[i], v[i + 1]));
+                    in_range &= fabsf(v[i]) < (kFp16 ? 65504.0f : 3.0e38f);
+                    in_range &= fabsf(v[i + 1]) < (kFp16 ? 65504.0f : 3.0e38f);
+                    s = __fmaf_rn(fabsf(r.x), ts.emax[c0 + i], s);
+                    s = __fmaf_rn(fabsf(r.y), ts.emax[c0 + i + 1], s);
+                }
+                ts.s_part[half][row] = in_range ? s : INFINITY;
+            }
+            phase_sync();
+        };
+
+        // ---- scoring: per game, the four largest 32-action chunk maxima of each half of the columns ----
+        auto score_tiles = [&]() {
+            const std::uint8_t *a_tile = page(0);
+            auto issue = [&](int tile) {
+                const int acc = tile & 1;
+                MmaK(tmem + static_cast<std::uint32_t>(acc * kTileN), a_tile, kPolicy, page(1 + tile % kEmbedStages),
+                     kPolicy, kPolicy / 16, idesc128, false);
+                umma::Commit(&ts.bar_acc[acc]);
+            };
+            if (tid == 0) {
+                wait_load(1);
+                umma::FenceAfterSync();
+                issue(0);
+            }
+            float tv[kTopK];
+            int ti[kTopK];
+#pragma unroll
+            for (int j = 0; j < kTopK; ++j) {
+                tv[j] = -INFINITY;
+                ti[j] = -1;
+            }
+            for (int tile = 0; tile < n_tiles; ++tile) {
+                const int buf = tile & 1;
+                if (tid == 0 && tile + 1 < n_tiles) {
+                    wait_load(1 + (tile + 1) % kEmbedStages);
+                    umma::FenceAfterSync();
+                    issue(tile + 1);
+                }
+                wait_bar(&ts.bar_acc[buf], acc_commits[buf] & 1u);
+                ++acc_commits[buf];
+                umma::FenceAfterSync();
+                if (tid == 0 && tile + kEmbedStages < n_tiles) {
+                    const int b = 1 + tile % kEmbedStages;  // tile's MMA has completed: its stage is free
+                    load(b, page(b), embed + static_cast<std::size_t>(tile + kEmbedStages) * kPageBytes, kPageBytes);
+                }
+                const bool last = tile + 1 == n_tiles;
+                {
+                    float v[64];
+                    umma::Load64(tmem + static_cast<std::uint32_t>(buf * kTileN + half * 64) + lane_bits, v);
+                    if (last) {
+#pragma unroll
+                        for (int j = 0; j < 64; ++j) {
+                            if (static_cast<std::uint32_t>(tile * kTileN + half * 64 + j) >= p.action_count) {
+                                v[j] = -INFINITY;
+                            }
+                        }
+                    }
+#pragma unroll
+                    for (int w = 16; w > 0; w >>= 1) {
+#pragma unroll
+                        for (int j = 0; j < w; ++j) {
+                            v[j] = fmaxf(v[j], v[j + w]);
+                            v[32 + j] = fmaxf(v[32 + j], v[32 + j + w]);
+                        }
+                    }
+                    InsertTop4(tv, ti, v[0], tile * 4 + half * 2);
+                    InsertTop4(tv, ti, v[32], tile * 4 + half * 2 + 1);
+                }
+                umma::FenceBeforeSync();
+                __syncthreads();
+            }
+            float *cand_v = reinterpret_cast<float *>(smem + kOffCandV);
+            int *cand_id = reinterpret_cast<int *>(smem + kOffCandId);
+#pragma unroll
+            for (int j = 0; j < kTopK; ++j) {
+                cand_v[(row * 2 + half) * kTopK + j] = tv[j];
+                cand_id[(row * 2 + half) * kTopK + j] = ti[j];
+            }
+            __syncthreads();
+        };
+
+        // Best tracked chunk maximum free of guessed words (by catalog index); `covered` turns false when the
+        // tracked lists cannot stand in for every chunk.
+        auto best_free_chunk = [&](int g, int t, bool &covered) {
+            const float *cand_v = reinterpret_cast<const float *>(smem + kOffCandV);
+            const int *cand_id = reinterpret_cast<const int *>(smem + kOffCandId);
+            float top = -INFINITY;
+            covered = true;
+            for (int h = 0; h < 2; ++h) {
+                bool found = false;
+                for (int j = 0; j < kTopK && !found; ++j) {
+                    const int id = cand_id[(g * 2 + h) * kTopK + j];
+                    bool masked = false;
+                    for (int u = 0; u < t; ++u) {
+                        masked |= cs.word_index[u][g] >= 0 && cs.word_index[u][g] / 32 == id;
+                    }
+                    if (id >= 0 && !masked) {
+                        top = fmaxf(top, cand_v[(g * 2 + h) * kTopK + j]);
+                        found = true;
+                    }
+                }
+                if (!found && cand_id[(g * 2 + h) * kTopK + kTopK - 1] >= 0) {
+                    covered = false;  // every tracked chunk of this half holds a guessed word
+                }
+            }
+            if (!(top > -INFINITY)) {
+                covered = false;
+            }
+            return top;
+        };
+        // Whether an untracked chunk may reach `floor`: a half whose list is full must end below it.
+        auto full_list_reaches = [&](int g, float floor) {
+            const float *cand_v = reinterpret_cast<const float *>(smem + kOffCandV);
+            const int *cand_id = reinterpret_cast<const int *>(smem + kOffCandId);
+            bool r = false;
+            for (int h = 0; h < 2; ++h) {
+                r |= cand_id[(g * 2 + h) * kTopK + kTopK - 1] >= 0 &&
+                     !(cand_v[(g * 2 + h) * kTopK + kTopK - 1] < floor);
+            }
+            return r;
+        };
+
+        // ---- decision from the 16-bit scores, certified by the top-2 margin ----
+        auto decide = [&](int t) {
+            const float *cand_v = reinterpret_cast<const float *>(smem + kOffCandV);
+            const int *cand_id = reinterpret_cast<const int *>(smem + kOffCandId);
+            float *excl = reinterpret_cast<float *>(smem + kOffExcl);
+            int *task_off = reinterpret_cast<int *>(smem + kOffTaskOff);
+            int *task_cnt = reinterpret_cast<int *>(smem + kOffTaskCnt);
+            std::uint32_t *tasks = reinterpret_cast<std::uint32_t *>(smem + kOffTasks);
+            unsigned long long *results = reinterpret_cast<unsigned long long *>(smem + kOffResults);
+            int n = 0;
+            float theta = 0.0f;
+            bool fallback = false;
+            if (tid == 0) {
+                ts.n_fallback = 0;
+            }
+            if (tid < kChunkGames) {
+                const int g = tid;
+                if (!cs.done[g]) {
+                    bool covered = true;
+                    const float top = best_free_chunk(g, t, covered);
+                    const float s_scale = ts.s_part[0][g] + ts.s_part[1][g];
+                    theta = top - q.tau * fmaxf(fabsf(top), 0.1f * s_scale);
+                    if (!(theta > -INFINITY) || full_list_reaches(g, theta)) {
+                        covered = false;
+                    }
+                    float x = -INFINITY;
+                    if (covered) {
+                        for (int e = 0; e < 2 * kTopK; ++e) {
+                            const int id = cand_id[g * 2 * kTopK + e];
+                            const float v = cand_v[g * 2 * kTopK + e];
+                            if (id >= 0) {
+                                if (v >= theta) {
+                                    ++n;
+                                } else {
+                                    x = fmaxf(x, v);
+                                }
+                            }
+                        }
+                    }
+                    excl[g] = x;
+                    fallback = !covered;
+                }
+            }
+            // block prefix sum of the candidate counts (threads 0..127)
+            int incl = n;
+            for (int off = 1; off < 32; off <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, incl, off);
+                if (lane >= off) {
+                    incl += y;
+                }
+            }
+            if (lane == 31 && warp < 4) {
+                ts.scan[warp] = incl;
+            }
+            __syncthreads();
+            int total = 0;
+            int before = 0;
+            for (int w = 0; w < 4; ++w) {
+                before += w < warp ? ts.scan[w] : 0;
+                total += ts.scan[w];
+            }
+            if (tid < kChunkGames) {
+                const int g = tid;
+                const int first = before + incl - n;
+                task_off[g] = first;
+                task_cnt[g] = n;
+                int k = first;
+                for (int e = 0; e < 2 * kTopK && n > 0; ++e) {
+                    const int id = cand_id[g * 2 * kTopK + e];
+                    if (id >= 0 && cand_v[g * 2 * kTopK + e] >= theta) {
+                        tasks[k++] = (static_cast<std::uint32_t>(g) << 16) | static_cast<std::uint32_t>(id);
+                    }
+                }
+                if (fallback) {
+                    ts.fallback_games[atomicAdd(&ts.n_fallback, 1)] = g;
+                }
+            }
+            __syncthreads();
+            // re-score each candidate chunk from the 16-bit operands: a warp per chunk (two chunks in flight),
+            // top-2 keys by (score, lower action index) from 32-bit warp reductions
+            auto task_bits = [&](std::uint32_t task) {
+                const int g = static_cast<int>(task >> 16);
+                const std::uint32_t a = (task & 0xFFFFu) * 32u + static_cast<std::uint32_t>(lane);
+                const bool valid = a < p.action_count;
+                const std::uint32_t code = valid ? __ldg(p.codes + a) : 0u;
+                const float s = ApproxScore<kFp16>(page(0), g, embed, valid ? a : 0u);
+                bool masked = !valid;
+                for (int u = 0; u < t; ++u) {
+                    masked |= cs.guess[u][g] == code;
+                }
+                return masked ? 0u : OrderedBits(s);
+            };
+            auto store_top2 = [&](int k, std::uint32_t task, std::uint32_t ob) {
+                const std::uint32_t a0 = (task & 0xFFFFu) * 32u;
+                const std::uint32_t m1 = __reduce_max_sync(0xffffffffu, ob);
+                const unsigned b1 = __ballot_sync(0xffffffffu, ob == m1 && m1 != 0u);
+                const int l1 = b1 != 0u ? __ffs(b1) - 1 : 0;
+                const std::uint32_t ob2 = lane == l1 ? 0u : ob;
+                const std::uint32_t m2 = __reduce_max_sync(0xffffffffu, ob2);
+                const unsigned b2 = __ballot_sync(0xffffffffu, ob2 == m2 && m2 != 0u);
+                if (lane == 0) {
+                    results[2 * k] = b1 != 0u ? (static_cast<unsigned long long>(m1) << 32) |
+                                                    (0xFFFFFFFFu - (a0 + static_cast<std::uint32_t>(l1)))
+                                              : 0ull;
+                    results[2 * k + 1] =
+                        b2 != 0u ? (static_cast<unsigned long long>(m2) << 32) |
+                                       (0xFFFFFFFFu - (a0 + static_cast<std::uint32_t>(__ffs(b2) - 1)))
+                                 : 0ull;
+                }
+            };
+            constexpr int kWarps = kEvalThreads / 32;
+            for (int k0 = warp; k0 < total; k0 += 2 * kWarps) {
+                const int k1 = k0 + kWarps;
+                const std::uint32_t task0 = tasks[k0];
+                const std::uint32_t task1 = k1 < total ? tasks[k1] : task0;
+                const std::uint32_t ob0 = task_bits(task0);
+                const std::uint32_t ob1 = task_bits(task1);
+                store_top2(k0, task0, ob0);
+                if (k1 < total) {
+                    store_top2(k1, task1, ob1);
+                }
+            }
+            __syncthreads();
+            if (tid < kChunkGames && !cs.done[tid] && !fallback) {
+                const int g = tid;
+                unsigned long long best = 0;
+                int best_task = -1;
+                for (int k = task_off[g]; k < task_off[g] + task_cnt[g]; ++k) {
+                    if (results[2 * k] > best) {
+                        best = results[2 * k];
+                        best_task = k;
+                    }
+                }
+                unsigned long long second = 0;
+                for (int k = task_off[g]; k < task_off[g] + task_cnt[g]; ++k) {
+                    const unsigned long long c = k == best_task ? results[2 * k + 1] : results[2 * k];
+                    second = c > second ? c : second;
+                }
+                bool ok = best != 0;
+                if (ok) {
+                    const float s1 = KeyScore(best);
+                    const float s2 = fmaxf(second != 0 ? KeyScore(second) : -INFINITY, excl[g]);
+                    const float s_scale = ts.s_part[0][g] + ts.s_part[1][g];
+                    ok = s1 - s2 >= q.tau * fmaxf(fabsf(s1), 0.1f * s_scale);
+                }
+                if (ok) {
+                    cs.best[g] = KeyAction(best);
+                } else {
+                    ts.fallback_games[atomicAdd(&ts.n_fallback, 1)] = g;
+                }
+            }
+            cand_chunks += tid == 0 ? static_cast<unsigned long long>(total) : 0ull;
+            __syncthreads();
+        };
+
+        // ---- exact FP32 path for the fallback games (the plain form's chains, bit for bit) ----
+        auto exact_fallback = [&](int t, int step) {
+            const int nf = ts.n_fallback;
+            fallback_steps += tid == 0 ? static_cast<unsigned long long>(nf) : 0ull;
+            float *hid = reinterpret_cast<float *>(smem + kOffXHid);  // [f][u][128]
+            float *enc = reinterpret_cast<float *>(smem + kOffXEnc);  // [f][u][64]
+            float *x0 = reinterpret_cast<float *>(smem + kOffXH0);    // [f][256]
+            float *x1 = reinterpret_cast<float *>(smem + kOffXH1);    // [f][128]
+            float *xp = reinterpret_cast<float *>(smem + kOffXP);     // [f][64]
+            std::uint8_t *stage = smem + kOffXStage;
+            unsigned long long *fb_key = reinterpret_cast<unsigned long long *>(smem + kOffFbKey);
+            float *fb_win = reinterpret_cast<float *>(smem + kOffFbWin);
+            int *fb_full = reinterpret_cast<int *>(smem + kOffFbFull);
+            std::uint32_t *fb_tasks = reinterpret_cast<std::uint32_t *>(smem + kOffFbTasks);
+            int *fb_count = reinterpret_cast<int *>(smem + kOffFbCount);
+            const __half *tail =
+                reinterpret_cast<const __half *>(reinterpret_cast<const std::uint8_t *>(gh) + kTailOffsetBytes);
+            const float *cand_v = reinterpret_cast<const float *>(smem + kOffCandV);
+            const int *cand_id = reinterpret_cast<const int *>(smem + kOffCandId);
+            for (int b0 = 0; b0 < nf; b0 += kFallbackBatch) {
+                const int nb = nf - b0 < kFallbackBatch ? nf - b0 : kFallbackBatch;
+                // encoder hidden layer of every turn (EncodeRound's gather chain), W_e1 staged in shared memory
+                {
+                    const uint4 *src = reinterpret_cast<const uint4 *>(gh + kEncW1);
+                    uint4 *dst = reinterpret_cast<uint4 *>(stage);
+                    for (int i = tid; i < kEncoderHidden * kTurnFeatures * 2 / 16; i += kEvalThreads) {
+                        dst[i] = __ldg(src + i);
+                    }
+                }
+                __syncthreads();
+                {
+                    const __half *we1 = reinterpret_cast<const __half *>(stage);
+                    for (int i = tid; i < nb * t * kEncoderHidden; i += kEvalThreads) {
+                        const int o = i & (kEncoderHidden - 1);
+                        const int fu = i >> 7;
+                        const int f = fu / t;
+                        const int u = fu - f * t;
+                        const int g = ts.fallback_games[b0 + f];
+                        const std::uint32_t code = cs.guess[u][g];
+                        const std::uint32_t tiles = cs.tiles[u][g];
+                        const __half *wr = we1 + o * kTurnFeatures;
+                        float h = ts.be1[o];
+                        for (int pos = 0; pos < kWordLength; ++pos) {
+                            h = __fmaf_rn(__half2float(wr[pos * kAlphabet + static_cast<int>(WordLetter(code, pos))]),
+                                          1.0f, h);
+                        }
+                        for (int pos = 0; pos < kWordLength; ++pos) {
+                            h = __fmaf_rn(__half2float(wr[kWordLength * kAlphabet + pos * 3 +
+                                                          static_cast<int>((tiles >> (2 * pos)) & 3u)]),
+                                          1.0f, h);
+                        }
+                        hid[(f * 5 + u) * kEncoderHidden + o] = h < 0.0f ? 0.0f : h;
+                    }
+                }
+                __syncthreads();
+                // encoder output layer: W_e2 staged transposed ([o][j]); thread (j, group) runs five chains at once
+                {
+                    __half *w2t = reinterpret_cast<__half *>(stage);
+                    for (int i = tid; i < kEncoderOut * kEncoderHidden / 8; i += kEvalThreads) {
+                        const int j = i & (kEncoderOut - 1);
+                        const int o0 = (i >> 6) * 8;
+                        const uint4 w4 = __ldg(reinterpret_cast<const uint4 *>(gh + kEncW2 + j * kEncoderHidden + o0));
+                        const __half *h8 = reinterpret_cast<const __half *>(&w4);
+#pragma unroll
+                        for (int e = 0; e < 8; ++e) {
+                            w2t[(o0 + e) * kEncoderOut + j] = h8[e];
+                        }
+                    }
+                }
+                __syncthreads();
+                {
+                    const __half *w2t = reinterpret_cast<const __half *>(stage);
+                    const int j = tid & (kEncoderOut - 1);
+                    const int grp = tid >> 6;
+                    const int pairs = nb * t;
+                    for (int q0 = grp; q0 < pairs; q0 += 20) {
+                        float acc[5];
+                        int base[5];
+#pragma unroll
+                        for (int r = 0; r < 5; ++r) {
+                            const int qq = q0 + 4 * r;
+                            const int f = qq < pairs ? qq / t : 0;
+                            const int u = qq < pairs ? qq - f * t : 0;
+                            base[r] = (f * 5 + u) * kEncoderHidden;
+                            acc[r] = ts.be2[j];
+                        }
+#pragma unroll 4
+                        for (int o = 0; o < kEncoderHidden; ++o) {
+                            const float w = __half2float(w2t[o * kEncoderOut + j]);
+#pragma unroll
+                            for (int r = 0; r < 5; ++r) {
+                                acc[r] = __fmaf_rn(hid[base[r] + o], w, acc[r]);
+                            }
+                        }
+#pragma unroll
+                        for (int r = 0; r < 5; ++r) {
+                            const int qq = q0 + 4 * r;
+                            if (qq < pairs) {
+                                const int f = qq / t;
+                                const int u = qq - f * t;
+                                enc[(f * 5 + u) * kEncoderOut + j] = acc[r];
+                            }
+                        }
+                    }
+                }
+                __syncthreads();
+                // layer 1: thread o, four batch games side by side; a turn's 64 weights are fetched before its chain
+                {
+                    const int o = tid;
+                    const __half *wrow = gh + kTrW1 + o * kModelInput;
+                    for (int f0 = 0; f0 < nb; f0 += 4) {
+                        float acc[4];
+                        if (t == 0) {
+                            const float v = __fmaf_rn(__half2float(wrow[0]), 1.0f, ts.b1[o]);
+#pragma unroll
+                            for (int r = 0; r < 4; ++r) {
+                                acc[r] = v;
+                            }
+                        } else {
+#pragma unroll
+                            for (int r = 0; r < 4; ++r) {
+                                acc[r] = ts.b1[o];
+                            }
+                            int ebase[4];
+#pragma unroll
+                            for (int r = 0; r < 4; ++r) {
+                                ebase[r] = (f0 + r < nb ? f0 + r : 0) * 5 * kEncoderOut;
+                            }
+                            for (int u = 0; u < t; ++u) {
+                                float w[kEncoderOut];
+#pragma unroll
+                                for (int k = 0; k < kEncoderOut; ++k) {
+                                    w[k] = __half2float(__ldg(wrow + 1 + kEncoderOut * u + k));
+                                }
+#pragma unroll
+                                for (int k = 0; k < kEncoderOut; ++k) {
+#pragma unroll
+                                    for (int r = 0; r < 4; ++r) {
+                                        acc[r] = __fmaf_rn(enc[ebase[r] + u * kEncoderOut + k], w[k], acc[r]);
+                                    }
+                                }
+                            }
+                        }
+#pragma unroll
+                        for (int r = 0; r < 4; ++r) {
+                            if (f0 + r < nb) {
+                                x0[(f0 + r) * kHidden0 + o] = acc[r] < 0.0f ? 0.0f : acc[r];
+                            }
+                        }
+                    }
+                }
+                __syncthreads();
+                // layer 2: thread (n, parity) over the batch games of its parity; 64 weights fetched per block
+                {
+                    const int n = tid & 127;
+                    const int par = tid >> 7;
+                    const uint4 *wrow = reinterpret_cast<const uint4 *>(gh + kTrW2 + n * kHidden0);
+                    int xbase[4];
+#pragma unroll
+                    for (int r = 0; r < 4; ++r) {
+                        const int f = par + 2 * r;
+                        xbase[r] = (f < nb ? f : 0) * kHidden0;
+                    }
+                    float acc[4];
+#pragma unroll
+                    for (int r = 0; r < 4; ++r) {
+                        acc[r] = ts.b2[n];
+                    }
+                    for (int k0 = 0; k0 < kHidden0; k0 += 64) {
+                        uint4 w4[8];
+#pragma unroll
+                        for (int i = 0; i < 8; ++i) {
+                            w4[i] = __ldg(wrow + k0 / 8 + i);
+                        }
+#pragma unroll
+                        for (int i = 0; i < 8; ++i) {
+                            const __half *h8 = reinterpret_cast<const __half *>(&w4[i]);
+#pragma unroll
+                            for (int e = 0; e < 8; ++e) {
+                                const float w = __half2float(h8[e]);
+#pragma unroll
+                                for (int r = 0; r < 4; ++r) {
+                                    acc[r] = __fmaf_rn(x0[xbase[r] + k0 + i * 8 + e], w, acc[r]);
+                                }
+                            }
+                        }
+                    }
+#pragma unroll
+                    for (int r = 0; r < 4; ++r) {
+                        const int f = par + 2 * r;
+                        if (f < nb) {
+                            x1[f * kHidden1 + n] = acc[r] < 0.0f ? 0.0f : acc[r];
+                        }
+                    }
+                }
+                __syncthreads();
+                // layer 3: thread (j, group of four) over two batch games
+                {
+                    const int j = tid & 63;
+                    const int grp = tid >> 6;
+                    const uint4 *wrow = reinterpret_cast<const uint4 *>(gh + kTrW3 + j * kHidden1);
+                    int xbase[2];
+#pragma unroll
+                    for (int r = 0; r < 2; ++r) {
+                        const int f = grp + 4 * r;
+                        xbase[r] = (f < nb ? f : 0) * kHidden1;
+                    }
+                    float acc[2] = {ts.b3[j], ts.b3[j]};
+                    for (int k0 = 0; k0 < kHidden1; k0 += 64) {
+                        uint4 w4[8];
+#pragma unroll
+                        for (int i = 0; i < 8; ++i) {
+                            w4[i] = __ldg(wrow + k0 / 8 + i);
+                        }
+#pragma unroll
+                        for (int i = 0; i < 8; ++i) {
+                            const __half *h8 = reinterpret_cast<const __half *>(&w4[i]);
+#pragma unroll
+                            for (int e = 0; e < 8; ++e) {
+                                const float w = __half2float(h8[e]);
+#pragma unroll
+                                for (int r = 0; r < 2; ++r) {
+                                    acc[r] = __fmaf_rn(x1[xbase[r] + k0 + i * 8 + e], w, acc[r]);
+                                }
+                            }
+                        }
+                    }
+#pragma unroll
+                    for (int r = 0; r < 2; ++r) {
+                        const int f = grp + 4 * r;
+                        if (f < nb) {
+                            xp[f * kPolicy + j] = acc[r];
+                        }
+                    }
+                }
+                if (tid == 0) {
+                    *fb_count = 0;
+                }
+                __syncthreads();
+                // exact policy into the trace; exact argmax over every chunk the 16-bit maxima cannot rule out
+                if (p.trace_policy != nullptr) {
+                    for (int i = tid; i < nb * kPolicy; i += kEvalThreads) {
+                        const int f = i >> 6;
+                        const int g = ts.fallback_games[b0 + f];
+                        const std::int32_t e = cs.episode[g];
+                        if (e >= 0 && static_cast<std::uint32_t>(e) < p.trace_episodes) {
+                            const std::size_t slot = static_cast<std::size_t>(ind) * p.trace_episodes + e;
+                            p.trace_policy[(slot * kMaxTurns + step) * kPolicy + (i & 63)] = xp[i];
+                        }
+                    }
+                }
+                if (tid < nb) {
+                    const int f = tid;
+                    const int g = ts.fallback_games[b0 + f];
+                    float dev = 0.0f;
+                    float mag = 0.0f;
+                    for (int k = 0; k < kPolicy; k += 2) {
+                        const std::uint32_t bits =
+                            *reinterpret_cast<const std::uint32_t *>(page(0) + umma::TileOffset(g, k, kPolicy));
+                        const float2 r = Unpack2<kFp16>(bits);
+                        dev = __fmaf_rn(fabsf(r.x - xp[f * kPolicy + k]), ts.emax[k], dev);
+                        dev = __fmaf_rn(fabsf(r.y - xp[f * kPolicy + k + 1]), ts.emax[k + 1], dev);
+                        mag = __fmaf_rn(fabsf(r.x), ts.emax[k], mag);
+                        mag = __fmaf_rn(fabsf(r.y), ts.emax[k + 1], mag);
+                    }
+                    const float err = dev * 1.001f + 1.0e-4f * mag;
+                    bool covered = true;
+                    const float top = best_free_chunk(g, t, covered);
+                    const float window = top - 2.0f * err;
+                    const bool full =
+                        !covered || !(err < INFINITY) || !(window > -INFINITY) || full_list_reaches(g, window);
+                    fb_key[f] = 0;
+                    fb_win[f] = top - err;
+                    if (!full) {
+                        for (int e = 0; e < 2 * kTopK; ++e) {
+                            const int id = cand_id[g * 2 * kTopK + e];
+                            if (id >= 0 && cand_v[g * 2 * kTopK + e] >= window) {
+                                fb_tasks[atomicAdd(fb_count, 1)] =
+                                    (static_cast<std::uint32_t>(f) << 16) | static_cast<std::uint32_t>(id);
+                            }
+                        }
+                    }
+                    fb_full[f] = full ? 1 : 0;
+                }
+                __syncthreads();
+                const int n_tasks = *fb_count;
+                for (int k = warp; k < n_tasks; k += kEvalThreads / 32) {
+                    const int f = static_cast<int>(fb_tasks[k] >> 16);
+                    RescoreChunk(p, cs, fb_key + f, xp + f * kPolicy, 1, tail, ts.fallback_games[b0 + f],
+                                 static_cast<int>(fb_tasks[k] & 0xFFFFu), t);
+                }
+                __syncthreads();
+                if (tid < nb && !fb_full[tid]) {
+                    const unsigned long long key = fb_key[tid];
+                    if (key == 0 || KeyScore(key) < fb_win[tid]) {
+                        fb_full[tid] = 1;  // the exact best stays below what the window guarantees
+                    }
+                }
+                __syncthreads();
+                const int chunks_per_row = static_cast<int>((p.action_count + 31) / 32);
+                for (int f = 0; f < nb; ++f) {
+                    if (fb_full[f]) {
+                        for (int c = warp; c < chunks_per_row; c += kEvalThreads / 32) {
+                            RescoreChunk(p, cs, fb_key + f, xp + f * kPolicy, 1, tail, ts.fallback_games[b0 + f], c,
+                                         t);
+                        }
+                    }
+                }
+                __syncthreads();
+                if (tid < nb) {
+                    const unsigned long long key = fb_key[tid];
+                    cs.best[ts.fallback_games[b0 + tid]] = key == 0 ? -1 : KeyAction(key);
+                }
+                if (tid == 0) {
+                    exact_chunks += static_cast<unsigned long long>(n_tasks);
+                    for (int f = 0; f < nb; ++f) {
+                        exact_rows += fb_full[f] ? 1ull : 0ull;
+                    }
+                }
+                __syncthreads();
+            }
+        };
+
+        if (cs.cls == 1 && CountActive(cs) > 0) {
+            encode_turn(0);
+            encode_turn(1);
+            encoded += tid == 0 ? 2ull * cs.active : 0ull;
+        }
+        for (int step = 0; step < kMaxTurns; ++step) {
+            if (CountActive(cs) == 0 || ts.failed) {
+                break;
+            }
+            const int t = cs.cls == 0 ? step : step + 2;
+            if (step > 0) {
+                encode_turn(t - 1);
+                encoded += tid == 0 ? static_cast<unsigned long long>(cs.active) : 0ull;
+            }
+            trunk(t, step);
+            score_tiles();
+            if (ts.failed) {
+                break;
+            }
+            decide(t);
+            if (ts.n_fallback > 0) {
+                exact_fallback(t, step);
+            }
+            AppendGuesses(p, cs, step, decisions);
+        }
+        FinishChunk(p, cs, ind, episodes);
+    }
+    FlushCounters(p, decisions, encoded, episodes);
+    if (tid == 0 && q.counters != nullptr) {
+        atomicAdd(q.counters + 0, cand_chunks);
+        atomicAdd(q.counters + 1, fallback_steps);
+        atomicAdd(q.counters + 2, exact_chunks);
+        atomicAdd(q.counters + 3, exact_rows);
+    }
+    __syncthreads();
+    if (tid == 0 && ts.failed) {
+        SetStatus(p.status, kTimeout);
+        // let tensor-core work and bulk copies still in flight finish before the CTA releases its resources
+        umma::Commit(&ts.bar_drain);
+        (void)umma::MbarWait(&ts.bar_drain, 0, 1u << 22);
+        for (int b = 0; b < kPages; ++b) {
+            while (load_waited[b] < load_issued[b]) {
+                (void)umma::MbarWait(&ts.bar_load[b], load_waited[b] & 1u, 1u << 22);
+                ++load_waited[b];
+            }
+        }
+    }
+    umma::FenceBeforeSync();
+    __syncthreads();
+    if (tid < 32) {
+        umma::Dealloc(tmem, kTmemColumns);
+    }
+}
+
+// Per individual: every trunk weight matrix as a 16-bit K-major canonical operand (kTblWe1 .. kTblW3).
+// One thread writes one 16-byte segment (8 values of one row).
+template <bool kFp16>
+__global__ void BuildTrunkTablesKernel(const std::uint8_t *slab, std::size_t pitch, const std::uint32_t *slots,
+                                       std::uint8_t *tables, std::size_t table_pitch) {
+    const std::uint32_t ind = blockIdx.y;
+    const int off = (blockIdx.x * blockDim.x + threadIdx.x) * 16;
+    const __half *gh = reinterpret_cast<const __half *>(slab + static_cast<std::size_t>(slots[ind]) * pitch);
+    int local, K, base, ld, col0, kvalid;
+    if (off < kTblWe2) {
+        local = off - kTblWe1, K = kKe1, base = kEncW1, ld = kTurnFeatures, col0 = 0, kvalid = kTurnFeatures;
+    } else if (off < kTblW1) {
+        local = off - kTblWe2, K = kEncoderHidden, base = kEncW2, ld = kEncoderHidden, col0 = 0, kvalid = K;
+    } else if (off < kTblW2) {
+        const int u = (off - kTblW1) / kW1SlotBytes;
+        local = (off - kTblW1) - u * kW1SlotBytes, K = kEncoderOut, base = kTrW1, ld = kModelInput;
+        col0 = 1 + kEncoderOut * u, kvalid = K;
+    } else if (off < kTblW3) {
+        const int kc = (off - kTblW2) / kW2ChunkBytes;
+        local = (off - kTblW2) - kc * kW2ChunkBytes, K = 64, base = kTrW2, ld = kHidden0, col0 = 64 * kc, kvalid = K;
+    } else {
+        local = off - kTblW3, K = kHidden1, base = kTrW3, ld = kHidden1, col0 = 0, kvalid = K;
+    }
+    const int seg = local / 16;
+    const int r = (seg / K) * 8 + (seg & 7);
+    const int k0 = ((seg >> 3) % (K / 8)) * 8;
+    std::uint16_t v[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const int k = k0 + i;
+        const __half h = k < kvalid ? gh[base + r * ld + col0 + k] : __float2half_rn(0.0f);
+        v[i] = kFp16 ? __half_as_ushort(h) : __bfloat16_as_ushort(__float2bfloat16_rn(__half2float(h)));
+    }
+    uint4 w;
+    w.x = v[0] | (static_cast<std::uint32_t>(v[1]) << 16);
+    w.y = v[2] | (static_cast<std::uint32_t>(v[3]) << 16);
+    w.z = v[4] | (static_cast<std::uint32_t>(v[5]) << 16);
+    w.w = v[6] | (static_cast<std::uint32_t>(v[7]) << 16);
+    *reinterpret_cast<uint4 *>(tables + static_cast<std::size_t>(ind) * table_pitch + off) = w;
+}
+
+}  // namespace
+
+std::size_t TrunkTablePitch() { return kTrunkTableBytes; }
+
+cudaError_t LaunchBuildTrunkTables(const std::uint8_t *slab, std::size_t pitch, const std::uint32_t *slots,
+                                   std::uint32_t population, std::uint8_t *tables, bool fp16, cudaStream_t stream) {
+    const dim3 grid(kTrunkTableBytes / 16 / 256, population);
+    if (fp16) {
+        BuildTrunkTablesKernel<true><<<grid, 256, 0, stream>>>(slab, pitch, slots, tables, kTrunkTableBytes);
+    } else {
+        BuildTrunkTablesKernel<false><<<grid, 256, 0, stream>>>(slab, pitch, slots, tables, kTrunkTableBytes);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t LaunchEvalTct(const EvalParams &params, const std::uint8_t *embed_tables, std::size_t embed_pitch,
+                          const std::uint8_t *trunk_tables, float tau, bool fp16, unsigned long long *counters,
+                          int cta_count, cudaStream_t stream) {
+    static bool configured[2] = {false, false};
+    if (!configured[fp16 ? 1 : 0]) {
+        cudaError_t e = fp16 ? cudaFuncSetAttribute(EvalTctKernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                    kSmemBytes)
+                             : cudaFuncSetAttribute(EvalTctKernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                    kSmemBytes);
+        if (e != cudaSuccess) {
+            return e;
+        }
+        configured[fp16 ? 1 : 0] = true;
+    }
+    if (cta_count <= 0) {
+        return cudaSuccess;
+    }
+    TctParams q{};
+    q.base = params;
+    q.embed_tables = embed_tables;
+    q.embed_pitch = embed_pitch;
+    q.trunk_tables = trunk_tables;
+    q.trunk_pitch = kTrunkTableBytes;
+    q.tau = tau;
+    q.counters = counters;
+    if (fp16) {
+        EvalTctKernel<true><<<cta_count, kEvalThreads, kSmemBytes, stream>>>(q);
+    } else {
+        EvalTctKernel<false><<<cta_count, kEvalThreads, kSmemBytes, stream>>>(q);
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace nwg

@@ -95,6 +95,14 @@ cudaError_t LaunchBuildTcTables(const std::uint8_t *slab, std::size_t pitch, con
 cudaError_t LaunchEvalTc(const EvalParams &params, const std::uint8_t *tables, std::size_t table_pitch, float kappa,
                          bool fp16, unsigned long long *tc_counters, int cta_count, cudaStream_t stream);
 
+// ---- fitness evaluation, tensor-core trunk form ----
+std::size_t TrunkTablePitch();
+cudaError_t LaunchBuildTrunkTables(const std::uint8_t *slab, std::size_t pitch, const std::uint32_t *slots,
+                                   std::uint32_t population, std::uint8_t *tables, bool fp16, cudaStream_t stream);
+cudaError_t LaunchEvalTct(const EvalParams &params, const std::uint8_t *embed_tables, std::size_t embed_pitch,
+                          const std::uint8_t *trunk_tables, float tau, bool fp16, unsigned long long *counters,
+                          int cta_count, cudaStream_t stream);
+
 struct SummaryDevice {
     float best_fitness;
     float average_fitness;
