@@ -197,9 +197,10 @@ int nwg_get_info(const nwg_runtime *runtime, nwg_runtime_info *info);
 int nwg_set_evaluation_form(nwg_runtime *runtime, int form);
 
 /* Margin guard of the tensor-core trunk forms (NWG_FORM_TC_TRUNK_*). No reference counterpart. A game step whose
- * top-2 margin among unguessed actions is below tau * scale, scale = max(|best score|, 0.1 * sum_k |p_k| *
- * max_a |e_ak|) on the 16-bit scores, is recomputed by the exact FP32 path (the plain form's chains), so its
- * guess is the plain form's. Default tau = 1e-3; tau = 0 disables the guard (uncertifiable steps still fall
+ * top-2 margin among unguessed actions, on the 16-bit scores, is not positive or is below tau * spread, with
+ * spread = sqrt(sum_k p_k^2 var_a(e_ak)) the game's score scale (an estimate of the standard deviation of its
+ * scores over the actions), is recomputed by the exact FP32 path (the plain form's chains), so its guess is the
+ * plain form's. Default tau = 1e-3; tau = 0 keeps only the positive-margin test (uncertifiable steps still fall
  * back); a huge tau sends every step through the exact path. Negative or non-finite tau is rejected. */
 int nwg_set_margin_guard(nwg_runtime *runtime, float tau);
 

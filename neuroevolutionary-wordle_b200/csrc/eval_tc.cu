@@ -411,8 +411,10 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTcKernel(const TcParams q
     }
 }
 
-// Per individual: emax[k] = max over the selectable actions of |e_ak| (header), and the embeddings as
-// 16-bit values in the K-major core-matrix layout, 1 KB per 8 actions, zero past the last action.
+// Per individual: emax[k] = max over the selectable actions of |e_ak| (header), the embeddings as 16-bit
+// values in the K-major core-matrix layout, 1 KB per 8 actions, zero past the last action, and after the
+// last tile, per tile, the column moments (sum_a e_ak, sum_a e_ak^2) over the tile's actions as float2[64],
+// each summed in a fixed order so that every run gets the same bits.
 template <bool kFp16>
 __global__ void BuildTcTablesKernel(const std::uint8_t *slab, std::size_t pitch, const std::uint32_t *slots,
                                     const float *fixed_t, std::uint32_t action_pad, std::uint32_t action_count,
@@ -425,10 +427,14 @@ __global__ void BuildTcTablesKernel(const std::uint8_t *slab, std::size_t pitch,
     unsigned int *emax_bits = reinterpret_cast<unsigned int *>(table);
     std::uint8_t *out = table + 256 + static_cast<std::size_t>(tile) * kTileBytes;
     __shared__ unsigned int block_max[kPolicy];
+    __shared__ float2 part[4][kPolicy];
     if (threadIdx.x < kPolicy) {
         block_max[threadIdx.x] = 0;
     }
     __syncthreads();
+    // thread t owns column t % 64 and actions t / 64, t / 64 + 4, ... of the tile
+    float sum = 0.0f;
+    float sum_sq = 0.0f;
     for (int idx = threadIdx.x; idx < kTileN * kPolicy; idx += blockDim.x) {
         const int a_local = idx >> 6;
         const int k = idx & 63;
@@ -438,6 +444,8 @@ __global__ void BuildTcTablesKernel(const std::uint8_t *slab, std::size_t pitch,
             v = k < kFixedDim ? fixed_t[static_cast<std::size_t>(k) * action_pad + a]
                               : __half2float(tail[static_cast<std::size_t>(a) * kTailDim + (k - kFixedDim)]);
             atomicMax(&block_max[k], __float_as_uint(fabsf(v)));
+            sum += v;
+            sum_sq = __fmaf_rn(v, v, sum_sq);
         }
         std::uint16_t bits;
         if constexpr (kFp16) {
@@ -447,9 +455,16 @@ __global__ void BuildTcTablesKernel(const std::uint8_t *slab, std::size_t pitch,
         }
         *reinterpret_cast<std::uint16_t *>(out + umma::TileOffset(a_local, k, kPolicy)) = bits;
     }
+    part[threadIdx.x >> 6][threadIdx.x & 63] = make_float2(sum, sum_sq);
     __syncthreads();
     if (threadIdx.x < kPolicy && block_max[threadIdx.x] != 0) {
         atomicMax(&emax_bits[threadIdx.x], block_max[threadIdx.x]);
+    }
+    if (threadIdx.x < kPolicy) {
+        const int k = threadIdx.x;
+        const float2 m = make_float2(((part[0][k].x + part[1][k].x) + part[2][k].x) + part[3][k].x,
+                                     ((part[0][k].y + part[1][k].y) + part[2][k].y) + part[3][k].y);
+        reinterpret_cast<float2 *>(table + 256 + static_cast<std::size_t>(tiles) * kTileBytes)[tile * kPolicy + k] = m;
     }
 }
 
@@ -457,7 +472,7 @@ __global__ void BuildTcTablesKernel(const std::uint8_t *slab, std::size_t pitch,
 
 std::size_t TcTablePitch(std::uint32_t action_count) {
     const std::size_t tiles = (action_count + kTileN - 1) / kTileN;
-    return 256 + tiles * static_cast<std::size_t>(kTileBytes);
+    return 256 + tiles * static_cast<std::size_t>(kTileBytes + kPolicy * sizeof(float2));
 }
 
 cudaError_t LaunchBuildTcTables(const std::uint8_t *slab, std::size_t pitch, const std::uint32_t *slots,

@@ -13,8 +13,11 @@
 //             keeping per game the four largest 32-action chunk maxima of each half of the columns.
 // Decision: the chunks within the guard bound of the best chunk free of guessed words are re-scored on
 // CUDA cores from the same 16-bit operands; the guess is the best unguessed action when its margin over
-// every other unguessed action is at least tau * scale, scale = max(|best score|, 0.1 * sum_k |p~_k| *
-// max_a |e_ak|). Otherwise (and whenever the tracked chunks cannot certify the margin) the game step
+// every other unguessed action is positive and at least tau * spread, where the spread
+// sqrt(sum_k p~_k^2 var_a(e_ak)) estimates the standard deviation of the game's scores over the actions
+// (the per-column embedding variances come with the embedding table; unlike the best score's magnitude the
+// spread ignores a shift common to every action). Otherwise (and whenever the tracked chunks cannot certify
+// the margin) the game step
 // falls back: its policy is recomputed with the plain form's exact FP32 chains and its guess is the
 // exact FP32 argmax, found by re-scoring every chunk that the tensor-core maxima cannot rule out
 // (|s~ - s| <= sum_k |p~_k - p_k| max_a |e_ak| + accumulation slack).
@@ -90,7 +93,7 @@ struct TctState {
     int failed;
     int n_fallback;
     int scan[4];
-    int fallback_games[kChunkGames];
+    std::uint8_t fallback_games[kChunkGames];  // game rows (< 128)
     float be1[kEncoderHidden];
     float be2[kEncoderOut];
     float b1[kHidden0];
@@ -98,6 +101,7 @@ struct TctState {
     float b3[kPolicy];
     float virgin[kHidden0];  // relu(b1 + W1[:, 0])
     float emax[kPolicy];
+    float var[kPolicy];  // per-column variance of the embeddings over the selectable actions
     float s_part[2][kChunkGames];
 };
 
@@ -310,6 +314,17 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
                 ts.be2[i] = H2F(gh, kEncB2 + i);
                 ts.b3[i] = H2F(gh, kTrB3 + i);
                 ts.emax[i] = reinterpret_cast<const float *>(etab)[i];
+                const float2 *moments = reinterpret_cast<const float2 *>(embed + static_cast<std::size_t>(n_tiles) *
+                                                                                     kPageBytes);
+                float sum = 0.0f;
+                float sum_sq = 0.0f;
+                for (int tile = 0; tile < n_tiles; ++tile) {
+                    const float2 m = moments[tile * kPolicy + i];
+                    sum += m.x;
+                    sum_sq += m.y;
+                }
+                const float mean = sum / static_cast<float>(p.action_count);
+                ts.var[i] = fmaxf(sum_sq / static_cast<float>(p.action_count) - mean * mean, 0.0f);
             }
         }
         __syncthreads();
@@ -535,8 +550,8 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
                     }
                 }
                 StoreRow32<kFp16>(page(0), row, c0, kPolicy, v);
-                // score scale; a policy value beyond the 16-bit range makes it infinite, which sends the game
-                // step to the exact path
+                // squared score spread; a policy value beyond the 16-bit range makes it infinite, which sends
+                // the game step to the exact path
                 float s = 0.0f;
                 bool in_range = true;
 #pragma unroll
@@ -544,8 +559,8 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
                     const float2 r = Unpack2<kFp16>(Pack2<kFp16>(v[i], v[i + 1]));
                     in_range &= fabsf(v[i]) < (kFp16 ? 65504.0f : 3.0e38f);
                     in_range &= fabsf(v[i + 1]) < (kFp16 ? 65504.0f : 3.0e38f);
-                    s = __fmaf_rn(fabsf(r.x), ts.emax[c0 + i], s);
-                    s = __fmaf_rn(fabsf(r.y), ts.emax[c0 + i + 1], s);
+                    s = __fmaf_rn(r.x * r.x, ts.var[c0 + i], s);
+                    s = __fmaf_rn(r.y * r.y, ts.var[c0 + i + 1], s);
                 }
                 ts.s_part[half][row] = in_range ? s : INFINITY;
             }
@@ -684,8 +699,8 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
                 if (!cs.done[g]) {
                     bool covered = true;
                     const float top = best_free_chunk(g, t, covered);
-                    const float s_scale = ts.s_part[0][g] + ts.s_part[1][g];
-                    theta = top - q.tau * fmaxf(fabsf(top), 0.1f * s_scale);
+                    const float spread = sqrtf(ts.s_part[0][g] + ts.s_part[1][g]);
+                    theta = top - q.tau * spread;
                     if (!(theta > -INFINITY) || full_list_reaches(g, theta)) {
                         covered = false;
                     }
@@ -738,7 +753,7 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
                     }
                 }
                 if (fallback) {
-                    ts.fallback_games[atomicAdd(&ts.n_fallback, 1)] = g;
+                    ts.fallback_games[atomicAdd(&ts.n_fallback, 1)] = static_cast<std::uint8_t>(g);
                 }
             }
             __syncthreads();
@@ -806,13 +821,13 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
                 if (ok) {
                     const float s1 = KeyScore(best);
                     const float s2 = fmaxf(second != 0 ? KeyScore(second) : -INFINITY, excl[g]);
-                    const float s_scale = ts.s_part[0][g] + ts.s_part[1][g];
-                    ok = s1 - s2 >= q.tau * fmaxf(fabsf(s1), 0.1f * s_scale);
+                    const float spread = sqrtf(ts.s_part[0][g] + ts.s_part[1][g]);
+                    ok = s1 - s2 > 0.0f && s1 - s2 >= q.tau * spread;
                 }
                 if (ok) {
                     cs.best[g] = KeyAction(best);
                 } else {
-                    ts.fallback_games[atomicAdd(&ts.n_fallback, 1)] = g;
+                    ts.fallback_games[atomicAdd(&ts.n_fallback, 1)] = static_cast<std::uint8_t>(g);
                 }
             }
             cand_chunks += tid == 0 ? static_cast<unsigned long long>(total) : 0ull;
