@@ -82,6 +82,10 @@ static_assert(kOffFbCount + 16 <= kOffXEnc, "decision buffers overlap the fallba
 static_assert(kOffXP + kFallbackBatch * kPolicy * 4 <= kOffXStage, "fallback buffers");
 static_assert(kOffXStage + kEncoderHidden * kTurnFeatures * 2 <= kSmemBytes, "staged encoder weights");
 static_assert((kEncoderHidden * kTurnFeatures * 2) % 16 == 0, "W_e1 copies as 16-byte words");
+constexpr int kStageLd = 66;   // halfs per staged 64-wide weight row (33 words: conflict-free column reads)
+constexpr int kStageLd3 = 130; // halfs per staged W3 row (65 words)
+static_assert(kOffXStage + kHidden0 * kStageLd * 2 <= kSmemBytes, "staged layer-1 slice");
+static_assert(kOffXStage + kPolicy * kStageLd3 * 2 <= kSmemBytes, "staged W3");
 
 struct TctState {
     std::uint64_t bar_load[kPages];  // bulk loads into page p (at most one outstanding per barrier)
@@ -198,6 +202,40 @@ __device__ __forceinline__ float ApproxScore(const std::uint8_t *a_tile, int g, 
         }
     }
     return (acc[0] + acc[1]) + (acc[2] + acc[3]);
+}
+
+// Copies `rows` rows of `cols` (a multiple of 32) 16-bit values, source row stride src_ld, destination row
+// stride dst_ld, into shared memory: a warp per row so that each load instruction reads consecutive halfs,
+// with 16 rows' loads issued before any store.
+template <int kCols>
+__device__ __forceinline__ void StageRows(__half *__restrict__ dst, int dst_ld, const __half *__restrict__ src,
+                                          int src_ld, int rows) {
+    constexpr int kBatch = 16;
+    constexpr int kPer = kCols / 32;
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    for (int r0 = warp; r0 < rows; r0 += kBatch * (kEvalThreads / 32)) {
+        __half v[kBatch][kPer];
+#pragma unroll
+        for (int i = 0; i < kBatch; ++i) {
+            const int r = r0 + i * (kEvalThreads / 32);
+#pragma unroll
+            for (int c = 0; c < kPer; ++c) {
+                v[i][c] = r < rows ? __ldg(src + static_cast<std::size_t>(r) * src_ld + c * 32 + lane)
+                                   : __float2half_rn(0.0f);
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < kBatch; ++i) {
+            const int r = r0 + i * (kEvalThreads / 32);
+            if (r < rows) {
+#pragma unroll
+                for (int c = 0; c < kPer; ++c) {
+                    dst[r * dst_ld + c * 32 + lane] = v[i][c];
+                }
+            }
+        }
+    }
 }
 
 template <bool kFp16>
@@ -940,48 +978,47 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
                     }
                 }
                 __syncthreads();
-                // layer 1: thread o, four batch games side by side; a turn's 64 weights are fetched before its chain
+                // layer 1: thread o, all batch games side by side (the chains continue across the turns in
+                // ascending input order); each turn's 256 x 64 weight slice is staged in shared memory first
                 {
                     const int o = tid;
-                    const __half *wrow = gh + kTrW1 + o * kModelInput;
-                    for (int f0 = 0; f0 < nb; f0 += 4) {
-                        float acc[4];
-                        if (t == 0) {
-                            const float v = __fmaf_rn(__half2float(wrow[0]), 1.0f, ts.b1[o]);
+                    const __half *w1s = reinterpret_cast<const __half *>(stage);
+                    float acc[kFallbackBatch];
+                    int ebase[kFallbackBatch];
 #pragma unroll
-                            for (int r = 0; r < 4; ++r) {
-                                acc[r] = v;
+                    for (int r = 0; r < kFallbackBatch; ++r) {
+                        ebase[r] = (r < nb ? r : 0) * 5 * kEncoderOut;
+                        acc[r] = t == 0 ? __fmaf_rn(H2F(gh, kTrW1 + o * kModelInput), 1.0f, ts.b1[o]) : ts.b1[o];
+                    }
+                    for (int u = 0; u < t; ++u) {
+                        __syncthreads();
+                        StageRows<kEncoderOut>(reinterpret_cast<__half *>(stage), kStageLd, gh + kTrW1 + 1 + kEncoderOut * u,
+                                               kModelInput, kHidden0);
+                        __syncthreads();
+                        if (nb <= 4) {
+#pragma unroll 4
+                            for (int k = 0; k < kEncoderOut; ++k) {
+                                const float w = __half2float(w1s[o * kStageLd + k]);
+#pragma unroll
+                                for (int r = 0; r < 4; ++r) {
+                                    acc[r] = __fmaf_rn(enc[ebase[r] + u * kEncoderOut + k], w, acc[r]);
+                                }
                             }
                         } else {
+#pragma unroll 2
+                            for (int k = 0; k < kEncoderOut; ++k) {
+                                const float w = __half2float(w1s[o * kStageLd + k]);
 #pragma unroll
-                            for (int r = 0; r < 4; ++r) {
-                                acc[r] = ts.b1[o];
-                            }
-                            int ebase[4];
-#pragma unroll
-                            for (int r = 0; r < 4; ++r) {
-                                ebase[r] = (f0 + r < nb ? f0 + r : 0) * 5 * kEncoderOut;
-                            }
-                            for (int u = 0; u < t; ++u) {
-                                float w[kEncoderOut];
-#pragma unroll
-                                for (int k = 0; k < kEncoderOut; ++k) {
-                                    w[k] = __half2float(__ldg(wrow + 1 + kEncoderOut * u + k));
-                                }
-#pragma unroll
-                                for (int k = 0; k < kEncoderOut; ++k) {
-#pragma unroll
-                                    for (int r = 0; r < 4; ++r) {
-                                        acc[r] = __fmaf_rn(enc[ebase[r] + u * kEncoderOut + k], w[k], acc[r]);
-                                    }
+                                for (int r = 0; r < kFallbackBatch; ++r) {
+                                    acc[r] = __fmaf_rn(enc[ebase[r] + u * kEncoderOut + k], w, acc[r]);
                                 }
                             }
                         }
+                    }
 #pragma unroll
-                        for (int r = 0; r < 4; ++r) {
-                            if (f0 + r < nb) {
-                                x0[(f0 + r) * kHidden0 + o] = acc[r] < 0.0f ? 0.0f : acc[r];
-                            }
+                    for (int r = 0; r < kFallbackBatch; ++r) {
+                        if (r < nb) {
+                            x0[r * kHidden0 + o] = acc[r] < 0.0f ? 0.0f : acc[r];
                         }
                     }
                 }
@@ -990,7 +1027,6 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
                 {
                     const int n = tid & 127;
                     const int par = tid >> 7;
-                    const uint4 *wrow = reinterpret_cast<const uint4 *>(gh + kTrW2 + n * kHidden0);
                     int xbase[4];
 #pragma unroll
                     for (int r = 0; r < 4; ++r) {
@@ -1002,22 +1038,17 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
                     for (int r = 0; r < 4; ++r) {
                         acc[r] = ts.b2[n];
                     }
+                    const __half *w2s = reinterpret_cast<const __half *>(stage);
                     for (int k0 = 0; k0 < kHidden0; k0 += 64) {
-                        uint4 w4[8];
+                        __syncthreads();
+                        StageRows<64>(reinterpret_cast<__half *>(stage), kStageLd, gh + kTrW2 + k0, kHidden0, kHidden1);
+                        __syncthreads();
+#pragma unroll 4
+                        for (int k = 0; k < 64; ++k) {
+                            const float w = __half2float(w2s[n * kStageLd + k]);
 #pragma unroll
-                        for (int i = 0; i < 8; ++i) {
-                            w4[i] = __ldg(wrow + k0 / 8 + i);
-                        }
-#pragma unroll
-                        for (int i = 0; i < 8; ++i) {
-                            const __half *h8 = reinterpret_cast<const __half *>(&w4[i]);
-#pragma unroll
-                            for (int e = 0; e < 8; ++e) {
-                                const float w = __half2float(h8[e]);
-#pragma unroll
-                                for (int r = 0; r < 4; ++r) {
-                                    acc[r] = __fmaf_rn(x0[xbase[r] + k0 + i * 8 + e], w, acc[r]);
-                                }
+                            for (int r = 0; r < 4; ++r) {
+                                acc[r] = __fmaf_rn(x0[xbase[r] + k0 + k], w, acc[r]);
                             }
                         }
                     }
@@ -1034,7 +1065,6 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
                 {
                     const int j = tid & 63;
                     const int grp = tid >> 6;
-                    const uint4 *wrow = reinterpret_cast<const uint4 *>(gh + kTrW3 + j * kHidden1);
                     int xbase[2];
 #pragma unroll
                     for (int r = 0; r < 2; ++r) {
@@ -1042,23 +1072,15 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
                         xbase[r] = (f < nb ? f : 0) * kHidden1;
                     }
                     float acc[2] = {ts.b3[j], ts.b3[j]};
-                    for (int k0 = 0; k0 < kHidden1; k0 += 64) {
-                        uint4 w4[8];
+                    StageRows<kHidden1>(reinterpret_cast<__half *>(stage), kStageLd3, gh + kTrW3, kHidden1, kPolicy);
+                    __syncthreads();
+                    const __half *w3s = reinterpret_cast<const __half *>(stage);
+#pragma unroll 4
+                    for (int k = 0; k < kHidden1; ++k) {
+                        const float w = __half2float(w3s[j * kStageLd3 + k]);
 #pragma unroll
-                        for (int i = 0; i < 8; ++i) {
-                            w4[i] = __ldg(wrow + k0 / 8 + i);
-                        }
-#pragma unroll
-                        for (int i = 0; i < 8; ++i) {
-                            const __half *h8 = reinterpret_cast<const __half *>(&w4[i]);
-#pragma unroll
-                            for (int e = 0; e < 8; ++e) {
-                                const float w = __half2float(h8[e]);
-#pragma unroll
-                                for (int r = 0; r < 2; ++r) {
-                                    acc[r] = __fmaf_rn(x1[xbase[r] + k0 + i * 8 + e], w, acc[r]);
-                                }
-                            }
+                        for (int r = 0; r < 2; ++r) {
+                            acc[r] = __fmaf_rn(x1[xbase[r] + k], w, acc[r]);
                         }
                     }
 #pragma unroll
