@@ -11,7 +11,8 @@
 //      at a time: each lane computes four consecutive uniforms, a ballot finds the hits, the hit list
 //      is resolved in order (a fresh normal pair consumes two more draw positions and leaves its
 //      second value cached for the next hit, as the generator's normal does), and the lanes then apply
-//      the hits' normals in parallel.
+//      the hits' normals in parallel, 32 queued hits at a time (each value's load issued before its normal
+//      is computed, so the read of the child image overlaps the generator's arithmetic).
 // Every uniform, 32-bit draw and normal is produced by the toolkit generator itself (curand_init at the
 // draw's position, then curand_uniform / curand / curand_normal), so the child image is bit-identical
 // to the reference's serial walk.
@@ -24,7 +25,8 @@ namespace nwg {
 namespace {
 
 constexpr int kBreedWarps = 8;
-constexpr int kEventCapacity = 128;
+constexpr int kEventCapacity = 256;  // queued hits: one window adds at most 128
+constexpr int kFlushAt = 32;
 
 struct LayerSpan {
     int weights;
@@ -100,12 +102,24 @@ __device__ __forceinline__ int NextHit(unsigned long long lo, unsigned long long
 
 __device__ __forceinline__ void ApplyNormal(__half *values, std::uint32_t v, const Stream &s, unsigned long long pair,
                                             bool second, float sigma) {
+    const float old = __half2float(values[v]);
     curandStatePhilox4_32_10_t state = StateAt(s, pair);
     float n = curand_normal(&state);
     if (second) {
         n = curand_normal(&state);
     }
-    values[v] = __float2half(__fmaf_rn(sigma, n, __half2float(values[v])));
+    values[v] = __float2half(__fmaf_rn(sigma, n, old));
+}
+
+// Applies the queued hits (each value is hit at most once per walk, so the order does not matter).
+__device__ __forceinline__ void FlushEvents(__half *values, const Stream &s, float sigma, EventList &ev, int &n_events,
+                                            int lane) {
+    __syncwarp();
+    for (int e = lane; e < n_events; e += 32) {
+        ApplyNormal(values, ev.value[e], s, ev.pair[e], ev.second[e] != 0, sigma);
+    }
+    __syncwarp();
+    n_events = 0;
 }
 
 // Per-value Bernoulli(p) mutation with sigma * N(0, 1) on hits, over values[0, count).
@@ -142,6 +156,7 @@ __device__ void MutateRun(__half *values, std::uint32_t count, Stream &s, float 
         return;
     }
     std::uint32_t v = 0;
+    int n_events = 0;
     while (v < count) {
         const unsigned long long window = s.position & ~3ull;
         int r = static_cast<int>(s.position - window);
@@ -159,7 +174,6 @@ __device__ void MutateRun(__half *values, std::uint32_t count, Stream &s, float 
         const std::uint32_t m3 = __reduce_or_sync(0xffffffffu, (lane >> 3) == 3 ? shifted : 0u);
         const unsigned long long lo = static_cast<unsigned long long>(m0) | (static_cast<unsigned long long>(m1) << 32);
         const unsigned long long hi = static_cast<unsigned long long>(m2) | (static_cast<unsigned long long>(m3) << 32);
-        int n_events = 0;
         while (v < count && r < 128) {
             const int h = NextHit(lo, hi, r);
             const std::uint32_t misses = static_cast<std::uint32_t>(h - r);
@@ -195,11 +209,12 @@ __device__ void MutateRun(__half *values, std::uint32_t count, Stream &s, float 
             ++v;
         }
         s.position = window + r;
-        __syncwarp();
-        for (int e = lane; e < n_events; e += 32) {
-            ApplyNormal(values, ev.value[e], s, ev.pair[e], ev.second[e] != 0, sigma);
+        if (n_events >= kFlushAt) {
+            FlushEvents(values, s, sigma, ev, n_events, lane);
         }
-        __syncwarp();
+    }
+    if (n_events > 0) {
+        FlushEvents(values, s, sigma, ev, n_events, lane);
     }
 }
 
