@@ -3,7 +3,13 @@
 Workload: population 4,096 on a 64x64 toroidal grid, 4,739 synthetic catalog words all active, 256
 secrets per cell drawn from a 2,315-word secret subset (3 episodes per secret), radius-1 rank selection,
 reference crossover temperatures, mutation p = 0.05, sigma = 0.02. Genomes are the reference's FP16
-layout (bootstrap He-normal weights, N(0, 0.05) tails) and the arithmetic is FP32 (plain form).
+layout (bootstrap He-normal weights, N(0, 0.05) tails).
+
+The headline form (default --form tc-trunk-fp16) runs encoder, trunk and scoring on tcgen05 with FP16
+operands and a top-2 margin guard (tau = 1e-3) that sends uncertain game steps through the exact FP32
+path. The plain FP32 form is timed on the same workload in the same process and reported beside it
+("plain_fp32"), with the guess agreement and fitness delta of the headline form against it over the
+whole population ("agreement_with_plain"). --form fp32 benchmarks the plain form alone.
 
 Prints one JSON line (rank 0). `--impl reference` times the reference's own CPU path (its host-callable
 model, scoring and Wordle code composed into its episode loop, built in oracle/_ref) on a bounded sample
@@ -29,6 +35,7 @@ sys.path.insert(0, str(ROOT))
 
 MEASURED = ROOT / "MEASURED_PEAKS.json"
 TRAFFIC = ROOT / "profiles" / "eval_fp32_traffic.json"
+TRAFFIC_TCT = ROOT / "profiles" / "eval_tct_traffic.json"
 KERNELS_PER_GENERATION = 7  # prepare, evaluate, finalize, summarize, select, plan slots, breed
 FORMS = {"fp32": 0, "tc-bf16": 1, "tc-fp16": 2, "tc-trunk-bf16": 3, "tc-trunk-fp16": 4}
 FORM_NAMES = {"fp32": "plain fp32", "tc-bf16": "tensor-core bf16 scoring, exact fp32 re-scoring",
@@ -36,6 +43,11 @@ FORM_NAMES = {"fp32": "plain fp32", "tc-bf16": "tensor-core bf16 scoring, exact 
               "tc-trunk-bf16": "tensor-core bf16 encoder+trunk+scoring, margin guard tau with exact fp32 fallback",
               "tc-trunk-fp16": "tensor-core fp16 encoder+trunk+scoring, margin guard tau with exact fp32 fallback"}
 EXTRA_KERNELS = {"fp32": 0, "tc-bf16": 1, "tc-fp16": 1, "tc-trunk-bf16": 2, "tc-trunk-fp16": 2}
+DTYPES = {"fp32": "fp32 (fp16-stored genomes)",
+          "tc-bf16": "bf16 tensor-core scores, fp32 trunk and exact fp32 re-scoring",
+          "tc-fp16": "fp16 tensor-core scores, fp32 trunk and exact fp32 re-scoring",
+          "tc-trunk-bf16": "bf16 tensor-core operands, fp32 accumulation; exact fp32 path for guarded steps",
+          "tc-trunk-fp16": "fp16 tensor-core operands, fp32 accumulation; exact fp32 path for guarded steps"}
 
 
 def algorithmic_flops(steps: int, encoded: int, action_count: int) -> float:
@@ -157,6 +169,66 @@ def cpu_reference_rate(catalog, offsets, words, genomes_u16, action_count, sampl
     return float(steps.sum()) / dt, dt, int(steps.sum())
 
 
+def time_generations(rt, torch, stream, world, local, steps_count, gen, counts, cfg, sample_clocks=False):
+    """Times `steps_count` generations (barrier + synchronize on both sides, CUDA events on the runtime's stream)."""
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    agg = {"steps": 0, "encoded": 0, "kernel_ms": [], "rescored": 0, "full": 0, "candidates": 0, "fallbacks": 0}
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local) if sample_clocks else None
+    if clocks is not None:
+        clocks.__enter__()
+    start.record(stream)
+    for _ in range(steps_count):
+        rt.advance(seed=1000 + gen, counts=counts, config=cfg)
+        st = rt.stats()
+        agg["steps"] += st.game_steps
+        agg["encoded"] += st.encoded_turns
+        agg["kernel_ms"].append(st.eval_kernel_ms)
+        agg["rescored"] += st.rescored_chunks
+        agg["full"] += st.full_rescores
+        agg["candidates"] += st.candidate_chunks
+        agg["fallbacks"] += st.fallback_steps
+        gen += 1
+    end.record(stream)
+    torch.cuda.synchronize()
+    if clocks is not None:
+        clocks.__exit__(None, None, None)
+    barrier(world)
+    agg["ms"] = max_over_ranks(start.elapsed_time(end), world)
+    agg["clocks"] = clocks.summary() if clocks is not None else None
+    return agg, gen
+
+
+def agreement_sample(rt, torch, counts, form, tau, episodes):
+    """Guess agreement and fitness delta of `form` against the plain form on the current generation.
+
+    A game step counts as comparable while every earlier choice of the game agreed in both runs."""
+    p = rt.population
+    out = {}
+    for f in (0, form):
+        rt.set_form(f)
+        if f != 0:
+            rt.set_margin_guard(tau)
+        choices = torch.full((p, episodes, 6), -1, dtype=torch.int32, device="cuda")
+        rt.evaluate_traced(counts, episodes, choices.data_ptr())
+        torch.cuda.synchronize()
+        out[f] = (choices.cpu().numpy(), rt.current_generation()["fitness"].copy())
+    a, b = out[form][0], out[0][0]
+    valid = (a >= 0) | (b >= 0)
+    differ = a != b
+    ok = valid & ~differ
+    cont = np.concatenate([np.ones(a.shape[:2] + (1,), bool), np.cumprod(ok, axis=2)[:, :, :-1].astype(bool)], 2)
+    total = int((cont & valid).sum())
+    same = int((cont & ok).sum())
+    dfit = np.abs(out[form][1].astype(np.float64) - out[0][1].astype(np.float64))
+    return {"identical_guess_fraction": same / max(total, 1), "comparable_game_steps": total,
+            "games": int(valid[:, :, 0].sum()), "fitness_delta_max": float(dfit.max()),
+            "fitness_delta_mean": float(dfit.mean()),
+            "individuals_with_changed_fitness": int((dfit > 0).sum())}
+
+
 def run_ours(args) -> None:
     import torch
 
@@ -169,8 +241,9 @@ def run_ours(args) -> None:
     stream = torch.cuda.current_stream()
     rt = nwg.Runtime(wl.action_count, wl.population, wl.columns, stream=stream.cuda_stream)
     rt.set_cell_words(offsets, words)
+    trunk_form = args.form.startswith("tc-trunk")
     rt.set_form(FORMS[args.form])
-    if args.form.startswith("tc-trunk"):
+    if trunk_form:
         rt.set_margin_guard(args.tau)
     rt.bootstrap(wl.population, seed=0 + rank)
     counts = nwg.capi.word_counts(training=wl.action_count, action_space=wl.action_count)
@@ -195,35 +268,9 @@ def run_ours(args) -> None:
         gen += 1
 
     # ---- device-resident timed region ----
-    start = torch.cuda.Event(enable_timing=True)
-    end = torch.cuda.Event(enable_timing=True)
-    steps = 0
-    encoded = 0
-    kernel_ms = []
-    rescored = 0
-    full = 0
-    candidates = 0
-    fallbacks = 0
-    barrier(world)
-    torch.cuda.synchronize()
-    with ClockSampler(local) as clocks:
-        start.record(stream)
-        for _ in range(args.steps):
-            rt.advance(seed=1000 + gen, counts=counts, config=cfg)
-            st = rt.stats()
-            steps += st.game_steps
-            encoded += st.encoded_turns
-            kernel_ms.append(st.eval_kernel_ms)
-            rescored += st.rescored_chunks
-            full += st.full_rescores
-            candidates += st.candidate_chunks
-            fallbacks += st.fallback_steps
-            gen += 1
-        end.record(stream)
-        torch.cuda.synchronize()
-    barrier(world)
-    ms = max_over_ranks(start.elapsed_time(end), world)
-    clock = clocks.summary()
+    agg, gen = time_generations(rt, torch, stream, world, local, args.steps, gen, counts, cfg, sample_clocks=True)
+    ms = agg["ms"]
+    steps = agg["steps"]
     total_steps = sum_over_ranks(float(steps), world)
 
     # ---- end-to-end through the public API with host buffers ----
@@ -247,19 +294,51 @@ def run_ours(args) -> None:
     e2e_ms = max_over_ranks(e2e_start.elapsed_time(e2e_end), world)
     e2e_total = sum_over_ranks(float(e2e_steps), world)
 
+    # ---- the plain FP32 form on the same workload, and the trunk form's agreement with it ----
+    plain = None
+    agree = None
+    if args.form != "fp32" and not args.no_plain:
+        if rank == 0 and trunk_form:
+            agree = agreement_sample(rt, torch, counts, FORMS[args.form], args.tau, 3 * wl.secrets_per_cell)
+        rt.set_form(0)
+        for _ in range(1):
+            rt.advance(seed=1000 + gen, counts=counts, config=cfg)
+            gen += 1
+        pagg, gen = time_generations(rt, torch, stream, world, local, args.steps, gen, counts, cfg)
+        plain_value = sum_over_ranks(float(pagg["steps"]), world) / (pagg["ms"] * 1e-3)
+        plain = {"value": plain_value, "unit": "game-steps/s", "ms_per_step": pagg["ms"] / args.steps,
+                 "eval_kernel_ms": sum(pagg["kernel_ms"]) / len(pagg["kernel_ms"]),
+                 "speedup_of_this_form": (total_steps / (ms * 1e-3)) / plain_value,
+                 "note": "plain FP32 form, same workload and process, after this form's timed generations"}
+
     if rank != 0:
         rt.close()
         return
     pk = peaks()
     mean_steps = steps / args.steps
-    mean_encoded = encoded / args.steps
-    kernel_mean_ms = sum(kernel_ms) / len(kernel_ms)
+    mean_encoded = agg["encoded"] / args.steps
+    kernel_mean_ms = sum(agg["kernel_ms"]) / len(agg["kernel_ms"])
     flops = algorithmic_flops(int(mean_steps), int(mean_encoded), wl.action_count)
     achieved_tflops = flops / (kernel_mean_ms * 1e-3) / 1e12
     fp32_peak = 148 * 128 * 2 * pk["sm_max_mhz"] * 1e6 / 1e12
+    traffic_file = TRAFFIC_TCT if trunk_form else TRAFFIC
     traffic = None
-    if TRAFFIC.exists():
-        traffic = json.loads(TRAFFIC.read_text()).get("bytes_per_launch")
+    if traffic_file.exists() and (trunk_form or args.form == "fp32"):
+        traffic = json.loads(traffic_file.read_text()).get("bytes_per_launch")
+    if trunk_form or args.form in ("tc-bf16", "tc-fp16"):
+        kernel = "EvalTctKernel" if trunk_form else "EvalTcKernel"
+        roofline = {"kernel": kernel, "bound": "tensor", "achieved": achieved_tflops, "peak": pk["bf16_tflops"],
+                    "unit": "TFLOP/s", "frac": achieved_tflops / pk["bf16_tflops"], "traffic": traffic,
+                    "peak_source": f"dense bf16 burst ({pk['source']}); fp16 operands run at the same rate",
+                    "frac_of_fp32_peak": achieved_tflops / fp32_peak}
+    else:
+        roofline = {"kernel": "EvalFp32Kernel", "bound": "fp32", "achieved": achieved_tflops, "peak": fp32_peak,
+                    "unit": "TFLOP/s", "frac": achieved_tflops / fp32_peak, "traffic": traffic,
+                    "peak_source": f"148 SMs x 128 FFMA/clk x 2 x {pk['sm_max_mhz']:.0f} MHz "
+                                   f"(sm_max_mhz {pk['source']})",
+                    "frac_of_bf16_tensor_peak": achieved_tflops / pk["bf16_tflops"]}
+    roofline.update({"kernel_ms_per_launch": kernel_mean_ms, "algorithmic_flop_per_launch": flops,
+                     "game_steps_per_launch": mean_steps})
     value = total_steps / (ms * 1e-3)
     line = {
         "metric": "game-steps/s",
@@ -272,7 +351,7 @@ def run_ours(args) -> None:
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "fp32 (fp16-stored genomes)",
+        "dtype": DTYPES[args.form],
         "data": "synthetic",
         "impl": "ours",
         "generations_per_s": args.steps / (ms * 1e-3),
@@ -280,26 +359,23 @@ def run_ours(args) -> None:
                    f"{wl.columns}", "action_count": wl.action_count, "secrets_per_cell": wl.secrets_per_cell,
                    "secret_subset": wl.secret_subset, "episodes_per_secret": 3, "selection_radius": wl.radius,
                    "mutation_probability": wl.mutation_probability, "mutation_sigma": wl.mutation_sigma,
-                   "form": FORM_NAMES[args.form], "parallelism": f"{world} independent populations (one per GPU)",
+                   "form": FORM_NAMES[args.form], "margin_tau": args.tau if trunk_form else None,
+                   "parallelism": f"{world} independent populations (one per GPU)",
                    "l2": "inputs larger than L2 (genome slab "
                          f"{wl.population * nwg.capi.genome_stride_bytes(wl.action_count) / 1e9:.2f} GB)"},
-        "roofline": {"kernel": "EvalFp32Kernel", "bound": "fp32", "achieved": achieved_tflops,
-                     "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved_tflops / fp32_peak,
-                     "traffic": traffic, "peak_source": f"148 SMs x 128 FFMA/clk x 2 x {pk['sm_max_mhz']:.0f} MHz "
-                                                         f"(sm_max_mhz {pk['source']})",
-                     "frac_of_bf16_tensor_peak": achieved_tflops / pk["bf16_tflops"],
-                     "kernel_ms_per_launch": kernel_mean_ms, "algorithmic_flop_per_launch": flops,
-                     "game_steps_per_launch": mean_steps},
+        "roofline": roofline,
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_total / (e2e_ms * 1e-3), "unit": "game-steps/s",
                 "h2d_bytes_per_step": int(offsets.nbytes + words.nbytes + 120),
                 "d2h_bytes_per_step": 4 + 48 + 24},
         "gpu_launches": (KERNELS_PER_GENERATION + EXTRA_KERNELS[args.form]) * args.steps,
-        "rescoring": {"chunks_per_step": rescored / max(steps, 1), "full_rescore_fraction": full / max(steps, 1),
-                      "candidate_chunks_per_step": candidates / max(steps, 1),
-                      "fallback_fraction": fallbacks / max(steps, 1),
-                      "margin_tau": args.tau if args.form.startswith("tc-trunk") else None},
-        "clocks": clock,
+        "rescoring": {"chunks_per_step": agg["rescored"] / max(steps, 1),
+                      "full_rescore_fraction": agg["full"] / max(steps, 1),
+                      "candidate_chunks_per_step": agg["candidates"] / max(steps, 1),
+                      "fallback_fraction": agg["fallbacks"] / max(steps, 1)},
+        "plain_fp32": plain,
+        "agreement_with_plain": agree,
+        "clocks": agg["clocks"],
     }
     print(json.dumps(line), flush=True)
     rt.close()
@@ -362,7 +438,8 @@ def main() -> None:
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["full", "medium", "small"], default="full")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--form", choices=sorted(FORMS), default="fp32")
+    ap.add_argument("--form", choices=sorted(FORMS), default="tc-trunk-fp16")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain FP32 comparison and the agreement sample")
     ap.add_argument("--tau", type=float, default=1e-3, help="margin guard of the tensor-core trunk forms")
     args = ap.parse_args()
     if args.impl == "reference":
