@@ -284,6 +284,7 @@ class Runtime:
         check(lib().nwg_advance(self.handle, seed, C.byref(counts), C.byref(config) if config else None,
                                 C.byref(pending) if pending else None, pf, None, sr, None,
                                 C.byref(history) if history else None), "nwg_advance")
+        self.action_count = self.info().action_count  # an injection widens the action space
 
     def status(self) -> int:
         v = C.c_int()

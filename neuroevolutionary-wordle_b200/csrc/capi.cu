@@ -34,6 +34,7 @@ struct Catalog {
     std::size_t count = 0;
     std::size_t pad = 0;
     int device = -1;
+    std::vector<std::uint32_t> host_codes;  // packed words, for the hint grids of injected words
 };
 
 Catalog g_catalog;
@@ -222,6 +223,75 @@ int SetHostStatus(nwg_runtime *rt, int code) {
     cudaMemcpyAsync(rt->status, rt->host_status, sizeof(int), cudaMemcpyHostToDevice, rt->stream);
     cudaStreamSynchronize(rt->stream);
     return code;
+}
+
+// ---- hint grids of a newly released word (wordle/hint_grid.hpp:76-162) ----
+constexpr std::uint32_t kAllYellow = 0x155u;  // every position's 2-bit tile is 1 (yellow)
+
+std::uint32_t RotateCode(std::uint32_t code, int rotation) {  // hint_grid.hpp:19-27 (rotate left)
+    std::uint8_t letters[kWordLength];
+    for (int p = 0; p < kWordLength; ++p) {
+        letters[p] = static_cast<std::uint8_t>(WordLetter(code, (p + rotation) % kWordLength));
+    }
+    return PackWord(letters);
+}
+
+int CountTiles(std::uint32_t feedback, std::uint32_t tile) {
+    int n = 0;
+    for (int p = 0; p < kWordLength; ++p) {
+        n += ((feedback >> (2 * p)) & 3u) == tile;
+    }
+    return n;
+}
+
+struct HintGroup {
+    int turns[3] = {0, 0, 0};
+    std::uint32_t guess[3][4] = {};
+    std::uint16_t tiles[3][4] = {};
+};
+
+// The cyclic grid (the word's distinct left rotations whose feedback is all yellow), then the first two
+// distinct letter swaps whose feedback is three green and two yellow; false when the word has no such group.
+bool BuildHintGroup(std::uint32_t word, HintGroup &g) {
+    g = HintGroup{};
+    for (int rotation = 1; rotation < kWordLength; ++rotation) {
+        const std::uint32_t guess = RotateCode(word, rotation);
+        bool seen = guess == word;
+        for (int t = 0; t < g.turns[0]; ++t) {
+            seen |= g.guess[0][t] == guess;
+        }
+        const std::uint32_t fb = FeedbackPacked(guess, word);
+        if (seen || fb != kAllYellow) {
+            continue;
+        }
+        g.guess[0][g.turns[0]] = guess;
+        g.tiles[0][g.turns[0]] = static_cast<std::uint16_t>(fb);
+        ++g.turns[0];
+    }
+    int selected = 0;
+    for (int i = 0; i < kWordLength && selected < 2; ++i) {
+        for (int j = i + 1; j < kWordLength && selected < 2; ++j) {
+            if (WordLetter(word, i) == WordLetter(word, j)) {
+                continue;
+            }
+            std::uint8_t letters[kWordLength];
+            for (int p = 0; p < kWordLength; ++p) {
+                letters[p] = static_cast<std::uint8_t>(WordLetter(word, p));
+            }
+            std::swap(letters[i], letters[j]);
+            const std::uint32_t guess = PackWord(letters);
+            const std::uint32_t fb = FeedbackPacked(guess, word);
+            if (CountTiles(fb, kGreen) != 3 || CountTiles(fb, kYellow) != 2 ||
+                (selected == 1 && g.guess[1][0] == guess)) {
+                continue;
+            }
+            g.turns[1 + selected] = 1;
+            g.guess[1 + selected][0] = guess;
+            g.tiles[1 + selected][0] = static_cast<std::uint16_t>(fb);
+            ++selected;
+        }
+    }
+    return selected == 2;
 }
 
 __global__ void PlanChildSlotsKernel(const std::uint32_t *pairs, std::uint32_t child_count,
@@ -421,6 +491,152 @@ int EvaluateImpl(nwg_runtime *rt, const nwg_runtime_word_counts *counts, const n
     return kOk;
 }
 
+// Action-space growth (slab_runtime.cu:1464-1482, genotype_slab/device_runtime.cu:1338-1432, :518-617).
+// Instead of compacting and re-laying the referenced parents in place at the wider stride (the reference's
+// single-CTA PrepareSlabForExpandedActionCountKernel), the children are bred straight from the parents'
+// slots into a fresh slab laid out at the new width (the breeding kernel reads and writes different pitches),
+// which is the same byte movement the assembly does anyway; the old slab is then released. The new rows of
+// every child are then injected on the device (inject.cu).
+int AdvanceWithInjection(nwg_runtime *rt, std::uint32_t generation_seed, const nwg_generation_assembly_config &cfg,
+                         const nwg_pending_injection &injection, const std::vector<HintGroup> &hints,
+                         std::size_t next_action_count, std::size_t next_size) {
+    const std::size_t n = injection.injection_count;
+    const std::size_t new_pitch = SlotPitchBytes(next_action_count);
+    const std::size_t new_slots = SlotsForBudget(rt->slab_byte_budget, next_action_count);
+    if (new_slots < next_size || new_slots >= 0xFFFFFFFFull) {
+        return SetHostStatus(rt, kSlabRepackFailed);
+    }
+    // per injected word and grid: up to four turns (packed guess, packed feedback); grids sorted by turn count
+    std::vector<std::uint32_t> codes(n * 12, 0);
+    std::vector<std::uint16_t> tiles(n * 12, 0);
+    std::vector<std::uint32_t> order(3 * n);
+    std::vector<int4> chunks;
+    for (std::size_t i = 0; i < n; ++i) {
+        for (int g = 0; g < 3; ++g) {
+            for (int t = 0; t < hints[i].turns[g]; ++t) {
+                codes[(i * 3 + g) * 4 + t] = hints[i].guess[g][t];
+                tiles[(i * 3 + g) * 4 + t] = hints[i].tiles[g][t];
+            }
+        }
+    }
+    for (int g = 0; g < 3; ++g) {
+        std::uint32_t *ord = order.data() + g * n;
+        for (std::size_t i = 0; i < n; ++i) {
+            ord[i] = static_cast<std::uint32_t>(i);
+        }
+        std::stable_sort(ord, ord + n, [&](std::uint32_t a, std::uint32_t b) {
+            return hints[a].turns[g] < hints[b].turns[g];
+        });
+        std::size_t k = 0;
+        while (k < n) {
+            const int turns = hints[ord[k]].turns[g];
+            std::size_t e = k;
+            while (e < n && e - k < static_cast<std::size_t>(kChunkGames) && hints[ord[e]].turns[g] == turns) {
+                ++e;
+            }
+            chunks.push_back(make_int4(g, turns, static_cast<int>(g * n + k), static_cast<int>(e - k)));
+            k = e;
+        }
+    }
+    std::vector<std::uint32_t> identity(next_size);
+    for (std::size_t c = 0; c < next_size; ++c) {
+        identity[c] = static_cast<std::uint32_t>(c);
+    }
+    std::uint8_t *new_slab = nullptr;
+    std::uint8_t *new_used = nullptr;
+    std::uint32_t *d_codes = nullptr, *d_order = nullptr;
+    std::uint16_t *d_tiles = nullptr;
+    int4 *d_chunks = nullptr;
+    float *d_sums = nullptr;
+    auto release = [&]() {
+        void *ptrs[] = {d_codes, d_order, d_tiles, d_chunks, d_sums};
+        for (void *p : ptrs) {
+            if (p != nullptr) {
+                cudaFree(p);
+            }
+        }
+    };
+    bool ok = cudaMalloc(&new_slab, new_slots * new_pitch) == cudaSuccess &&
+              cudaMalloc(&new_used, new_slots) == cudaSuccess &&
+              cudaMalloc(&d_codes, codes.size() * sizeof(std::uint32_t)) == cudaSuccess &&
+              cudaMalloc(&d_tiles, tiles.size() * sizeof(std::uint16_t)) == cudaSuccess &&
+              cudaMalloc(&d_order, order.size() * sizeof(std::uint32_t)) == cudaSuccess &&
+              cudaMalloc(&d_chunks, chunks.size() * sizeof(int4)) == cudaSuccess &&
+              cudaMalloc(&d_sums, static_cast<std::size_t>(rt->scratch_ctas) * n * kTailDim * sizeof(float)) ==
+                  cudaSuccess;
+    ok = ok && cudaMemsetAsync(new_slab, 0, new_slots * new_pitch, rt->stream) == cudaSuccess &&
+         cudaMemsetAsync(new_used, 0, new_slots, rt->stream) == cudaSuccess &&
+         cudaMemcpyAsync(d_codes, codes.data(), codes.size() * sizeof(std::uint32_t), cudaMemcpyHostToDevice,
+                         rt->stream) == cudaSuccess &&
+         cudaMemcpyAsync(d_tiles, tiles.data(), tiles.size() * sizeof(std::uint16_t), cudaMemcpyHostToDevice,
+                         rt->stream) == cudaSuccess &&
+         cudaMemcpyAsync(d_order, order.data(), order.size() * sizeof(std::uint32_t), cudaMemcpyHostToDevice,
+                         rt->stream) == cudaSuccess &&
+         cudaMemcpyAsync(d_chunks, chunks.data(), chunks.size() * sizeof(int4), cudaMemcpyHostToDevice,
+                         rt->stream) == cudaSuccess &&
+         cudaMemcpyAsync(rt->next_slots, identity.data(), next_size * sizeof(std::uint32_t), cudaMemcpyHostToDevice,
+                         rt->stream) == cudaSuccess;
+    BreedParams bp{};
+    bp.parent_slab = rt->slab;
+    bp.parent_pitch = rt->pitch;
+    bp.parent_slots = rt->cur_slots;
+    bp.child_slab = new_slab;
+    bp.child_pitch = new_pitch;
+    bp.child_slots = rt->next_slots;
+    bp.pairs = rt->pairs;
+    bp.child_count = static_cast<std::uint32_t>(next_size);
+    bp.action_count = static_cast<std::uint32_t>(rt->action_count);  // the parents' rows
+    bp.generation_seed = generation_seed;
+    bp.generation_index = rt->cur_gen_index;
+    bp.crossover_l1 = cfg.breeding.crossover_temperature_level1;
+    bp.crossover_l2 = cfg.breeding.crossover_temperature_level2;
+    bp.crossover_l3 = cfg.breeding.crossover_temperature_level3;
+    bp.mutation_probability = cfg.mutation.mutation_probability;
+    bp.mutation_sigma = cfg.mutation.mutation_sigma;
+    bp.row_scale_probability = cfg.mutation.output_tail_row_scale_mutation_probability;
+    bp.status = rt->status;
+    ok = ok && LaunchBreed(bp, rt->stream) == cudaSuccess;
+    ok = ok && LaunchInject(new_slab, new_pitch, rt->next_slots, static_cast<std::uint32_t>(next_size),
+                            static_cast<std::uint32_t>(rt->action_count), static_cast<std::uint32_t>(n), d_codes,
+                            d_tiles, d_chunks, d_order, static_cast<int>(chunks.size()), rt->scratch, d_sums,
+                            rt->scratch_ctas, rt->status, rt->stream) == cudaSuccess;
+    ok = ok && cudaMemsetAsync(rt->next_fitness, 0, rt->max_generation_size * sizeof(float), rt->stream) == cudaSuccess &&
+         cudaMemsetAsync(rt->next_eval, 0, rt->max_generation_size * sizeof(std::uint32_t), rt->stream) ==
+             cudaSuccess &&
+         cudaMemsetAsync(rt->next_has, 0, rt->max_generation_size, rt->stream) == cudaSuccess;
+    const int st = ok ? Sync(rt) : kCudaFailure;
+    release();
+    if (st != kOk) {
+        cudaFree(new_slab);
+        cudaFree(new_used);
+        return st;
+    }
+    // the children now own the widened slab
+    cudaFree(rt->slab);
+    cudaFree(rt->slot_used);
+    rt->slab = new_slab;
+    rt->slot_used = new_used;
+    rt->action_count = next_action_count;
+    rt->stride = GenomeStrideBytes(next_action_count);
+    rt->pitch = new_pitch;
+    rt->slot_count = new_slots;
+    if (rt->tc_tables != nullptr) {
+        // the 16-bit embedding tables are sized by the action count
+        cudaFree(rt->tc_tables);
+        rt->tc_tables = nullptr;
+        const std::size_t bytes = rt->max_generation_size * TcTablePitch(static_cast<std::uint32_t>(next_action_count));
+        if (cudaMalloc(&rt->tc_tables, bytes) != cudaSuccess) {
+            rt->tc_tables = nullptr;
+            rt->form = NWG_FORM_FP32;
+            return SetHostStatus(rt, kCudaFailure);
+        }
+        rt->tc_tables_bytes = bytes;
+    }
+    rt->next_gen_index = rt->cur_gen_index + 1;
+    rt->next_gen_size = next_size;
+    return nwg_swap_generations(rt);
+}
+
 }  // namespace
 
 extern "C" {
@@ -491,6 +707,7 @@ int nwg_upload_catalog(const uint8_t *letters, size_t word_count) {
     }
     g_catalog.count = word_count;
     g_catalog.pad = pad;
+    g_catalog.host_codes.assign(codes.begin(), codes.begin() + static_cast<std::ptrdiff_t>(word_count));
     cudaGetDevice(&g_catalog.device);
     return kOk;
 }
@@ -790,12 +1007,28 @@ int nwg_advance(nwg_runtime *rt, uint32_t generation_seed, const nwg_runtime_wor
     if (shard_release != nullptr && !shard_release(rt, counts, &injection, shard_release_user)) {
         return SetHostStatus(rt, kInvalidAssemblyConfig);
     }
+    // slab_runtime.cu:678-683, :919-939: the next width, then the next population from the generation byte
+    // budget at that width
+    std::size_t next_action_count = rt->action_count;
+    std::vector<HintGroup> hints;
     if (injection.enabled) {
-        // action-space growth (output-embedding injection with widening repack) is not built yet
-        return SetHostStatus(rt, kUnsupported);
+        if (injection.injection_count == 0 || injection.first_catalog_word_index != rt->action_count) {
+            return SetHostStatus(rt, kInvalidAssemblyConfig);
+        }
+        next_action_count = rt->action_count + injection.injection_count;
+        // injection_ops.cuh:31-37 and output_embedding_injection.hpp:123-131: the new words must exist in the
+        // catalog and each must have a hint-grid group
+        if (next_action_count > g_catalog.count) {
+            return SetHostStatus(rt, kOutputEmbeddingInjectionFailed);
+        }
+        hints.resize(injection.injection_count);
+        for (std::size_t i = 0; i < injection.injection_count; ++i) {
+            if (!BuildHintGroup(g_catalog.host_codes[rt->action_count + i], hints[i])) {
+                return SetHostStatus(rt, kOutputEmbeddingInjectionFailed);
+            }
+        }
     }
-    // slab_runtime.cu:919-939: next population from the generation byte budget at the next width
-    std::size_t next_size = FloorRows(SlotsForBudget(rt->generation_byte_budget, rt->action_count,
+    std::size_t next_size = FloorRows(SlotsForBudget(rt->generation_byte_budget, next_action_count,
                                                      rt->max_generation_size),
                                       rt->grid_column_count);
     next_size = std::min(next_size, rt->cur_gen_size);
@@ -824,6 +1057,9 @@ int nwg_advance(nwg_runtime *rt, uint32_t generation_seed, const nwg_runtime_wor
         if (!post_fitness(rt, counts, post_fitness_user)) {
             return SetHostStatus(rt, kInvalidAssemblyConfig);
         }
+    }
+    if (injection.enabled) {
+        return AdvanceWithInjection(rt, generation_seed, cfg, injection, hints, next_action_count, next_size);
     }
     PlanChildSlotsKernel<<<1, 1024, 0, rt->stream>>>(rt->pairs, static_cast<std::uint32_t>(next_size), rt->cur_slots,
                                                      static_cast<std::uint32_t>(rt->cur_gen_size), rt->slot_used,

@@ -151,6 +151,13 @@ struct BreedParams {
 };
 cudaError_t LaunchBreed(const BreedParams &params, cudaStream_t stream);
 
+// ---- output-embedding injection (action-space growth) ----
+cudaError_t LaunchInject(std::uint8_t *slab, std::size_t pitch, const std::uint32_t *child_slots,
+                         std::uint32_t child_count, std::uint32_t parent_action_count, std::uint32_t injection_count,
+                         const std::uint32_t *guess_codes, const std::uint16_t *tiles, const int4 *chunks,
+                         const std::uint32_t *order, int chunk_count, float *scratch, float *sums, int cta_count,
+                         int *status, cudaStream_t stream);
+
 // ---- bootstrap ----
 cudaError_t LaunchBootstrap(std::uint8_t *slab, std::size_t pitch, const std::uint32_t *slots,
                             std::uint32_t population, std::uint64_t generation_index, std::uint32_t seed,

@@ -11,6 +11,7 @@
 
 #include <math.h>
 #include <stdint.h>
+#include <stdlib.h>
 #include <string.h>
 
 /* ---- fp16 storage (common/float16.hpp:9-13): IEEE binary16, round to nearest even ---- */
@@ -769,4 +770,192 @@ void nwo_summarize(const float *fitness, size_t count, float *best, float *avera
     *best = b;
     *average = count ? sum / (float)count : 0.0f;
     *best_index = bi;
+}
+
+/* ---- output-embedding injection for action-space growth ---- */
+
+static void rotate_word_left(const uint8_t w[5], size_t rotation, uint8_t out[5]) { /* hint_grid.hpp:19-27 */
+    for (size_t p = 0; p < 5; ++p) {
+        out[p] = w[(p + rotation) % 5];
+    }
+}
+
+static size_t count_tiles(const uint8_t fb[5], uint8_t tile) { /* hint_grid.hpp:39-50 */
+    size_t n = 0;
+    for (size_t p = 0; p < 5; ++p) {
+        n += fb[p] == tile;
+    }
+    return n;
+}
+
+/* hint_grid.hpp:76-105: the solution's left rotations whose feedback is all yellow, in rotation order. */
+static int build_cyclic_hint_grid(const uint8_t solution[5], grid_t *g) {
+    memset(g, 0, sizeof *g);
+    if (!valid_word(solution)) {
+        return 0;
+    }
+    memcpy(g->solution, solution, 5);
+    uint8_t appended[4][5];
+    size_t appended_count = 0;
+    for (size_t rotation = 1; rotation < 5; ++rotation) {
+        uint8_t guess[5];
+        rotate_word_left(solution, rotation, guess);
+        int seen = words_equal(guess, solution);
+        for (size_t k = 0; k < appended_count; ++k) {
+            seen |= words_equal(appended[k], guess);
+        }
+        if (seen) {
+            continue;
+        }
+        uint8_t fb[5];
+        if (!nwo_feedback(guess, solution, fb) || count_tiles(fb, 1) != 5) {
+            continue;
+        }
+        if (!grid_append(g, guess, -1)) {
+            return 0;
+        }
+        memcpy(appended[appended_count++], guess, 5);
+    }
+    return 1;
+}
+
+/* hint_grid.hpp:107-125: the solution with two different letters swapped, if that reads 3 green + 2 yellow. */
+static int build_swap_hint_grid(const uint8_t solution[5], size_t first, size_t second, grid_t *g) {
+    memset(g, 0, sizeof *g);
+    if (!valid_word(solution) || first >= 5 || second >= 5 || first == second || solution[first] == solution[second]) {
+        return 0;
+    }
+    uint8_t guess[5];
+    memcpy(guess, solution, 5);
+    guess[first] = solution[second];
+    guess[second] = solution[first];
+    uint8_t fb[5];
+    if (!nwo_feedback(guess, solution, fb) || count_tiles(fb, 0) != 3 || count_tiles(fb, 1) != 2) {
+        return 0;
+    }
+    memcpy(g->solution, solution, 5);
+    return grid_append(g, guess, -1);
+}
+
+/* hint_grid.hpp:127-162: the cyclic grid, then the first two swap grids with different guesses. */
+int nwo_hint_grid_group(const uint8_t solution[5], size_t turn_counts[3], uint8_t guesses[3][4][5],
+                        uint8_t feedbacks[3][4][5]) {
+    grid_t grids[3];
+    memset(grids, 0, sizeof grids);
+    memset(turn_counts, 0, 3 * sizeof(size_t));
+    memset(guesses, 0, 3 * 4 * 5);
+    memset(feedbacks, 0, 3 * 4 * 5);
+    if (!build_cyclic_hint_grid(solution, &grids[0])) {
+        return 0;
+    }
+    size_t selected = 0;
+    int ok = 0;
+    for (size_t first = 0; first < 5 && !ok; ++first) {
+        for (size_t second = first + 1; second < 5 && !ok; ++second) {
+            grid_t swap;
+            if (!build_swap_hint_grid(solution, first, second, &swap)) {
+                continue;
+            }
+            int seen = 0;
+            for (size_t k = 0; k < selected; ++k) {
+                seen |= words_equal(grids[1 + k].guess[0], swap.guess[0]);
+            }
+            if (seen) {
+                continue;
+            }
+            grids[1 + selected] = swap;
+            ++selected;
+            ok = selected == 2;
+        }
+    }
+    if (!ok) {
+        return 0;
+    }
+    for (size_t g = 0; g < 3; ++g) {
+        turn_counts[g] = grids[g].turn_count;
+        for (size_t t = 0; t < grids[g].turn_count; ++t) {
+            memcpy(guesses[g][t], grids[g].guess[t], 5);
+            memcpy(feedbacks[g][t], grids[g].feedback[t], 5);
+        }
+    }
+    return 1;
+}
+
+/* output_embedding_injection.hpp:66-75 (the device build contracts `sum += v * v`). */
+static float trainable_tail_norm(const uint16_t row[NWO_TAIL_DIM]) {
+    float sum = 0.0f;
+    for (size_t k = 0; k < NWO_TAIL_DIM; ++k) {
+        const float v = h2f(row[k]);
+        sum = mac(v, v, sum);
+    }
+    return sqrtf(sum);
+}
+
+static int cmp_float(const void *a, const void *b) {
+    const float x = *(const float *)a;
+    const float y = *(const float *)b;
+    return (x > y) - (x < y);
+}
+
+/* output_embedding_injection.hpp:77-102: median of the rows' norms (mean of the two middle ones). */
+float nwo_median_tail_norm(const uint16_t *genome, size_t row_count) {
+    float *norms = (float *)malloc(row_count * sizeof(float));
+    for (size_t a = 0; a < row_count; ++a) {
+        norms[a] = trainable_tail_norm(genome + POLICY_END + NWO_TAIL_DIM * a);
+    }
+    qsort(norms, row_count, sizeof(float), cmp_float);
+    const size_t upper = row_count / 2;
+    const float median = (row_count % 2) != 0 ? norms[upper] : 0.5f * (norms[upper - 1] + norms[upper]);
+    free(norms);
+    return median;
+}
+
+/* device/injection_ops.cuh:22-64 with output_embedding_injection.hpp:117-199: for each new word, the mean of
+ * the policy's 38 trainable outputs over its three hint grids (rounded to FP16), rescaled to the median norm
+ * of the genome's existing rows. */
+int nwo_inject_tails(uint16_t *genome, size_t parent_action_count, const uint8_t *catalog_letters,
+                     size_t catalog_count, size_t first, size_t count) {
+    if (genome == NULL || parent_action_count == 0 || count == 0 || first != parent_action_count) {
+        return 2;
+    }
+    if (first >= catalog_count || count > catalog_count - first) {
+        return 1;
+    }
+    const float target = nwo_median_tail_norm(genome, parent_action_count);
+    const float third = 1.0f / 3.0f;
+    for (size_t i = 0; i < count; ++i) {
+        size_t turns[3];
+        uint8_t guesses[3][4][5];
+        uint8_t feedbacks[3][4][5];
+        if (!nwo_hint_grid_group(catalog_letters + 5 * (first + i), turns, guesses, feedbacks)) {
+            return 2;
+        }
+        float sums[NWO_TAIL_DIM];
+        memset(sums, 0, sizeof sums);
+        for (size_t g = 0; g < 3; ++g) {
+            float policy[64];
+            if (!nwo_policy_forward(genome, turns[g], &guesses[g][0][0], &feedbacks[g][0][0], 0, policy)) {
+                return 2;
+            }
+            for (size_t k = 0; k < NWO_TAIL_DIM; ++k) {
+                sums[k] += policy[26 + k];
+            }
+        }
+        uint16_t *row = genome + POLICY_END + NWO_TAIL_DIM * (parent_action_count + i);
+        for (size_t k = 0; k < NWO_TAIL_DIM; ++k) {
+            row[k] = f2h(sums[k] * third);
+        }
+        float scale = 0.0f;
+        if (target > 1.0e-6f) {
+            const float current = trainable_tail_norm(row);
+            if (!(current > 1.0e-6f)) {
+                return 2;
+            }
+            scale = target / current;
+        }
+        for (size_t k = 0; k < NWO_TAIL_DIM; ++k) {
+            row[k] = f2h(h2f(row[k]) * scale);
+        }
+    }
+    return 0;
 }

@@ -142,6 +142,21 @@ size_t nwo_bootstrap_normals_per_thread(size_t action_count, size_t tid);
 /* Population summary (slab_runtime.cu:588-631). */
 void nwo_summarize(const float *fitness, size_t count, float *best, float *average, size_t *best_index);
 
+/* Hint-grid group of a word (wordle/hint_grid.hpp:127-162): the cyclic grid and two swap grids; per grid its
+ * turn count and turn rows (guess letters, feedback 0 green / 1 yellow / 2 grey). Returns 0 when the word
+ * has no such group. */
+int nwo_hint_grid_group(const uint8_t solution[5], size_t turn_counts[3], uint8_t guesses[3][4][5],
+                        uint8_t feedbacks[3][4][5]);
+
+/* Median norm of the first row_count tail rows (genetic_algorithm/output_embedding_injection.hpp:77-102). */
+float nwo_median_tail_norm(const uint16_t *genome, size_t row_count);
+
+/* Output-embedding injection of `count` new catalog words into a genome whose tail already holds
+ * `parent_action_count` rows and has room for `count` more (device/injection_ops.cuh:22-64).
+ * Returns 0 on success, 1 for an invalid catalog range, 2 when injection fails. */
+int nwo_inject_tails(uint16_t *genome, size_t parent_action_count, const uint8_t *catalog_letters,
+                     size_t catalog_count, size_t first, size_t count);
+
 #ifdef __cplusplus
 }
 #endif

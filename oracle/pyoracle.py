@@ -111,6 +111,10 @@ def lib() -> C.CDLL:
     L.nwo_bootstrap_normals_per_thread.restype = _sz
     L.nwo_bootstrap_normals_per_thread.argtypes = [_sz, _sz]
     L.nwo_summarize.argtypes = [_f32p, _sz, _f32p, _f32p, C.POINTER(_sz)]
+    L.nwo_hint_grid_group.argtypes = [_u8p, C.POINTER(_sz), _u8p, _u8p]
+    L.nwo_median_tail_norm.restype = C.c_float
+    L.nwo_median_tail_norm.argtypes = [_u16p, _sz]
+    L.nwo_inject_tails.argtypes = [_u16p, _sz, _u8p, _sz, _sz, _sz]
     return L
 
 
@@ -223,6 +227,28 @@ def bootstrap_genome(action_count: int, normals: np.ndarray, per_thread: int) ->
     return g
 
 
+def hint_grid_group(word: np.ndarray):
+    """(turn counts[3], guesses[3][4][5], feedbacks[3][4][5]) of a word's hint grids, or None."""
+    turns = (_sz * 3)()
+    guesses = np.zeros((3, 4, 5), np.uint8)
+    fbs = np.zeros((3, 4, 5), np.uint8)
+    w = np.ascontiguousarray(np.asarray(word, np.uint8))
+    ok = lib().nwo_hint_grid_group(_ptr(w, _u8p), turns, _ptr(guesses, _u8p), _ptr(fbs, _u8p))
+    return (list(turns), guesses, fbs) if ok else None
+
+
+def median_tail_norm(genome: np.ndarray, rows: int) -> float:
+    return float(lib().nwo_median_tail_norm(_ptr(np.ascontiguousarray(genome, np.uint16), _u16p), rows))
+
+
+def inject_tails(genome: np.ndarray, parent_action_count: int, catalog: np.ndarray, first: int, count: int):
+    """(status, genome with rows parent_action_count .. + count injected); genome needs room for the rows."""
+    g = np.array(genome, np.uint16, copy=True)
+    cat = np.ascontiguousarray(np.asarray(catalog, np.uint8))
+    st = lib().nwo_inject_tails(_ptr(g, _u16p), parent_action_count, _ptr(cat, _u8p), len(cat), first, count)
+    return st, g
+
+
 def summarize(fitness: np.ndarray):
     best = C.c_float()
     avg = C.c_float()
@@ -302,4 +328,5 @@ def ref_dev() -> C.CDLL | None:
     L.refdev_breed.argtypes = [C.c_void_p, _sz, C.c_void_p, _sz, C.c_void_p, _sz, _sz, C.c_uint32, _sz, C.c_float,
                                C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, C.c_void_p]
     L.refdev_bootstrap.argtypes = [C.c_void_p, _sz, _sz, _sz, C.c_uint32, _sz, C.c_void_p]
+    L.refdev_inject.argtypes = [C.c_void_p, _sz, _sz, _sz, _sz, _sz, C.c_void_p, C.c_void_p]
     return L

@@ -9,7 +9,9 @@
 //                       and policy vectors of every decision recorded;
 //   - refdev_select:    slab_runtime.cu:633-675 (BuildSlabAssemblyPlanKernel body);
 //   - refdev_breed:     genotype_slab/device_runtime.cu:448-516 (breed + mutate body);
-//   - refdev_bootstrap: genotype_slab/device_runtime.cu:258-314 (initialisation body).
+//   - refdev_bootstrap: genotype_slab/device_runtime.cu:258-314 (initialisation body);
+//   - refdev_inject:    genotype_slab/device_runtime.cu:594-599 (output-embedding injection of a bred child,
+//                       device/injection_ops.cuh:22-64), one warp per genome.
 // The reference's slab allocator (free-list spin lock) is never called: children and
 // organisms are written to caller-provided slots.
 #include <cuda_runtime.h>
@@ -19,6 +21,7 @@
 
 #include "genetic_algorithm/device/evaluation_ops.cuh"
 #include "genetic_algorithm/device/genome_ops.cuh"
+#include "genetic_algorithm/device/injection_ops.cuh"
 #include "genetic_algorithm/device/selection_ops.cuh"
 #include "training_folder/training_data.cu"
 
@@ -164,6 +167,21 @@ __global__ void BootstrapKernel(std::uint8_t *slab, std::size_t pitch, std::size
                                                   blockDim.x);
 }
 
+__global__ void InjectKernel(std::uint8_t *genomes, std::size_t pitch, std::size_t count,
+                             std::size_t parent_action_count, std::size_t first, std::size_t injection_count,
+                             int *status) {
+    __shared__ ga::OutputEmbeddingInjectionWarpScratch<32> scratch;
+    const std::size_t genome = blockIdx.x;
+    if (genome >= count) {
+        return;
+    }
+    const auto result = ga::device_injection_ops::TryInjectExpandedOutputEmbeddingTailsConcurrently<32>(
+        genomes + genome * pitch, parent_action_count, first, injection_count, scratch);
+    if (threadIdx.x == 0) {
+        status[genome] = static_cast<int>(result);
+    }
+}
+
 } // namespace
 
 extern "C" {
@@ -242,6 +260,13 @@ int refdev_bootstrap(void *slab, std::size_t pitch, std::size_t population, std:
                      std::uint32_t seed, std::size_t action_count, void *stream) {
     BootstrapKernel<<<static_cast<unsigned>(population), 256, 0, static_cast<cudaStream_t>(stream)>>>(
         static_cast<std::uint8_t *>(slab), pitch, population, generation_index, seed, action_count);
+    return cudaGetLastError() == cudaSuccess ? 1 : 0;
+}
+
+int refdev_inject(void *genomes, std::size_t pitch, std::size_t count, std::size_t parent_action_count,
+                  std::size_t first, std::size_t injection_count, int *status, void *stream) {
+    InjectKernel<<<static_cast<unsigned>(count), 32, 0, static_cast<cudaStream_t>(stream)>>>(
+        static_cast<std::uint8_t *>(genomes), pitch, count, parent_action_count, first, injection_count, status);
     return cudaGetLastError() == cudaSuccess ? 1 : 0;
 }
 

@@ -111,7 +111,7 @@ def test_invalid_configs_are_rejected():
     with pytest.raises(G.nwg.NwgError) as err:
         rt.evaluate(bad)
     assert err.value.status == 5
-    pending = G.nwg.capi.PendingInjection(True, 180, 10)
+    pending = G.nwg.capi.PendingInjection(True, 180, 10)  # words 180..189 are beyond the 180-word catalog
     with pytest.raises(G.nwg.NwgError) as err:
         rt.advance(seed=1, counts=counts, pending=pending)
-    assert err.value.status == 18
+    assert err.value.status == 15
