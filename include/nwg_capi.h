@@ -7,8 +7,9 @@
  * reference function it replaces. Conventions:
  *   - plain pointers and sizes, no C++ or torch types;
  *   - every call returns an nwg status code: 0 is success, 1..16 are the reference's
- *     DeviceSlabGARuntimeStatusCode values (slab_runtime.hpp:21-39), 17 and 18 are
- *     additions (a bounded device wait that gave up; a feature this runtime rejects);
+ *     DeviceSlabGARuntimeStatusCode values (slab_runtime.hpp:21-39), 17..19 are
+ *     additions (a bounded device wait that gave up; a feature this runtime rejects;
+ *     a checkpoint that fails its checks, where the reference returns false);
  *   - the last failure is also kept as the runtime's sticky status, readable with
  *     nwg_read_status, as the reference keeps its device status int;
  *   - all device work of a runtime is issued on its stream (nwg_set_stream), and a call
@@ -27,7 +28,7 @@
 extern "C" {
 #endif
 
-#define NWG_ABI_VERSION 2
+#define NWG_ABI_VERSION 3
 #define NWG_CATALOG_CAPACITY 4739
 
 enum {
@@ -50,6 +51,7 @@ enum {
     NWG_SLAB_REPACK_FAILED = 16,
     NWG_TIMEOUT = 17,
     NWG_UNSUPPORTED = 18,
+    NWG_INVALID_CHECKPOINT = 19,
 };
 
 typedef struct nwg_runtime nwg_runtime;
@@ -228,6 +230,103 @@ int nwg_advance(nwg_runtime *runtime, uint32_t generation_seed, const nwg_runtim
                 const nwg_generation_assembly_config *config, const nwg_pending_injection *pending,
                 nwg_post_fitness_fn post_fitness, void *post_fitness_user, nwg_shard_release_fn shard_release,
                 void *shard_release_user, const nwg_shard_release_history *history);
+
+/* The two halves of nwg_advance (TryPreparePrebreedingBoundaryOnDevice and TryAssemblePreparedGenerationOnDevice,
+ * slab_runtime.cu:1374-1680). prepare evaluates the current generation, runs the callbacks, sizes the next
+ * generation and plans its parents; assemble breeds (and, when an injection is pending, widens and injects) the
+ * planned children and swaps them in. Between the two the runtime sits at the pre-breeding boundary that
+ * checkpoints capture. assemble without a prepared generation returns NWG_INVALID_ASSEMBLY_PLAN. */
+int nwg_prepare_generation(nwg_runtime *runtime, uint32_t generation_seed, const nwg_runtime_word_counts *counts,
+                           const nwg_generation_assembly_config *config, const nwg_pending_injection *pending,
+                           nwg_post_fitness_fn post_fitness, void *post_fitness_user,
+                           nwg_shard_release_fn shard_release, void *shard_release_user,
+                           const nwg_shard_release_history *history);
+int nwg_assemble_prepared(nwg_runtime *runtime);
+
+/* GenotypeSlabLayout (genotype_slab/layout.hpp:20-25). */
+typedef struct {
+    size_t action_count;
+    size_t slot_stride_bytes;
+    size_t slot_count;
+    size_t slab_bytes;
+} nwg_slab_layout;
+
+/* CellularGridShape (spatial/grid.hpp:17-21). */
+typedef struct {
+    size_t row_count;
+    size_t column_count;
+    size_t cell_count;
+} nwg_grid_shape;
+
+/* RuntimeCheckpoint (slab_runtime.hpp:86-117) with its vectors as arrays: the pre-breeding boundary of one
+ * generation step (evaluated, parents planned, nothing bred yet). Arrays filled by nwg_checkpoint_capture or
+ * nwg_checkpoint_read are malloc-owned; release them with nwg_checkpoint_free. A caller-built checkpoint may
+ * point anywhere (nwg_checkpoint_write and nwg_checkpoint_restore only read it). */
+typedef struct {
+    uint32_t schema_version;              /* 3 */
+    uint32_t genome_layout_version;       /* 1 */
+    uint32_t resume_phase;                /* 1: before recombination and mutation */
+    uint64_t checksum;                    /* nwg_checkpoint_checksum */
+    uint64_t training_data_identity_hash; /* nwg_checkpoint_identity_hash */
+    uint32_t generation_seed;
+    nwg_runtime_word_counts runtime_word_counts;
+    nwg_shard_release_history training_shard_release_history;
+    nwg_generation_assembly_config assembly_config;
+    nwg_pending_injection pending_output_embedding_injection;
+    nwg_runtime_config runtime_config;
+    nwg_slab_layout slab_layout;
+    nwg_grid_shape current_grid_shape;
+    nwg_grid_shape next_grid_shape;
+    nwg_grid_shape epicenter_grid_shape;
+    size_t generation_index;
+    size_t individual_count;
+    uint32_t *slot_indices;        /* [individual_count]; 0xFFFFFFFF for a parent no child references */
+    float *fitness;                /* [individual_count] */
+    uint32_t *evaluation_counts;   /* [individual_count] */
+    uint8_t *has_fitness;          /* [individual_count] */
+    size_t child_count;
+    uint32_t *parent_pairs;        /* [child_count][2] (SlabParentPair) */
+    size_t live_count;
+    uint32_t *live_organisms;      /* [live_count] organism (individual) index of each genome record */
+    uint8_t *live_genomes;         /* [live_count][slab_layout.slot_stride_bytes] genome images */
+} nwg_checkpoint;
+
+/* TryCreatePrebreedingCheckpointOnDevice (slab_runtime.hpp:151-157): nwg_prepare_generation, then the boundary
+ * downloaded into *checkpoint (slab_runtime.cu:1260-1372). The runtime stays prepared: nwg_assemble_prepared
+ * continues it exactly as nwg_advance would have. catalog_letters (catalog_count rows of 5 letter indices) may be
+ * NULL; when given it enters the training-data identity hash, like the reference's host catalog. When an
+ * injection is pending the checkpoint describes the widened slab, as the reference's does: the layout at the new
+ * action count, each parent's genome zero-padded to the new stride. */
+int nwg_checkpoint_capture(nwg_runtime *runtime, uint32_t generation_seed, const nwg_runtime_word_counts *counts,
+                           const nwg_generation_assembly_config *config, const nwg_pending_injection *pending,
+                           nwg_post_fitness_fn post_fitness, void *post_fitness_user,
+                           nwg_shard_release_fn shard_release, void *shard_release_user,
+                           const nwg_shard_release_history *history, const uint8_t *catalog_letters,
+                           size_t catalog_count, nwg_checkpoint *checkpoint);
+
+/* TryRestorePrebreedingCheckpointToDevice (slab_runtime.hpp:159): a new runtime holding the checkpoint's
+ * generation (fitness kept), genomes and parent plan, prepared for assembly. NWG_INVALID_CHECKPOINT when a check
+ * of the reference's fails (versions, resume phase, checksum, layout, records, plan). The new runtime evaluates in
+ * the plain form and has no per-cell word lists until they are set again. */
+int nwg_checkpoint_restore(const nwg_checkpoint *checkpoint, nwg_runtime **runtime_out);
+
+/* TryResumeGenerationFromCheckpointOnDevice (slab_runtime.hpp:161-162): assemble the restored boundary. */
+int nwg_checkpoint_resume(nwg_runtime *runtime);
+
+/* TryWriteRuntimeCheckpointAtomically / TryReadRuntimeCheckpoint (slab_runtime.hpp:164-167): the reference's file
+ * format byte for byte (little-endian, records at their LP64 sizes), written to path.tmp and renamed. write
+ * refuses a checkpoint whose checksum field is stale; read rejects a bad magic, version or checksum. */
+int nwg_checkpoint_write(const nwg_checkpoint *checkpoint, const char *path);
+int nwg_checkpoint_read(const char *path, nwg_checkpoint *checkpoint);
+void nwg_checkpoint_free(nwg_checkpoint *checkpoint);
+
+/* ComputeRuntimeCheckpointChecksum (slab_runtime.cu:1205-1248): FNV-1a 64 over the fields in file order. */
+uint64_t nwg_checkpoint_checksum(const nwg_checkpoint *checkpoint);
+
+/* The training-data identity hash of TryDownloadBoundaryCheckpointPayload (slab_runtime.cu:1283-1297): FNV-1a 64
+ * over the word counts, the release history (may be NULL) and the catalog (may be NULL). */
+uint64_t nwg_checkpoint_identity_hash(const nwg_runtime_word_counts *counts, const nwg_shard_release_history *history,
+                                      const uint8_t *catalog_letters, size_t catalog_count);
 
 /* SwapDeviceSlabGenerationBuffers (slab_runtime.hpp:181). */
 int nwg_swap_generations(nwg_runtime *runtime);

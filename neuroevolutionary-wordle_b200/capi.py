@@ -90,6 +90,28 @@ class RuntimeInfo(C.Structure):
                                    "current_generation_size")]
 
 
+class SlabLayout(C.Structure):
+    _fields_ = [(n, _sz) for n in ("action_count", "slot_stride_bytes", "slot_count", "slab_bytes")]
+
+
+class GridShape(C.Structure):
+    _fields_ = [(n, _sz) for n in ("row_count", "column_count", "cell_count")]
+
+
+class CheckpointRecord(C.Structure):
+    """nwg_checkpoint: RuntimeCheckpoint (slab_runtime.hpp:86-117) with its vectors as pointers."""
+    _fields_ = [("schema_version", C.c_uint32), ("genome_layout_version", C.c_uint32), ("resume_phase", C.c_uint32),
+                ("checksum", C.c_uint64), ("training_data_identity_hash", C.c_uint64),
+                ("generation_seed", C.c_uint32), ("runtime_word_counts", RuntimeWordCounts),
+                ("training_shard_release_history", ShardReleaseHistory), ("assembly_config", AssemblyConfig),
+                ("pending_output_embedding_injection", PendingInjection), ("runtime_config", RuntimeConfig),
+                ("slab_layout", SlabLayout), ("current_grid_shape", GridShape), ("next_grid_shape", GridShape),
+                ("epicenter_grid_shape", GridShape), ("generation_index", _sz), ("individual_count", _sz),
+                ("slot_indices", _vp), ("fitness", _vp), ("evaluation_counts", _vp), ("has_fitness", _vp),
+                ("child_count", _sz), ("parent_pairs", _vp), ("live_count", _sz), ("live_organisms", _vp),
+                ("live_genomes", _vp)]
+
+
 POST_FITNESS_FN = C.CFUNCTYPE(C.c_bool, _vp, C.POINTER(RuntimeWordCounts), _vp)
 SHARD_RELEASE_FN = C.CFUNCTYPE(C.c_bool, _vp, C.POINTER(RuntimeWordCounts), C.POINTER(PendingInjection), _vp)
 
@@ -99,7 +121,10 @@ EXPORTS = [
     "nwg_read_evaluation_stats", "nwg_advance", "nwg_swap_generations", "nwg_read_status",
     "nwg_download_current_generation", "nwg_download_slot", "nwg_upload_slot", "nwg_upload_current_generation",
     "nwg_download_assembly_plan", "nwg_device_slab", "nwg_evaluate_traced", "nwg_select_parents_device",
-    "nwg_breed_device", "nwg_bootstrap_device",
+    "nwg_breed_device", "nwg_bootstrap_device", "nwg_evaluate_noalloc", "nwg_prepare_generation",
+    "nwg_assemble_prepared", "nwg_checkpoint_capture", "nwg_checkpoint_restore", "nwg_checkpoint_resume",
+    "nwg_checkpoint_write", "nwg_checkpoint_read", "nwg_checkpoint_free", "nwg_checkpoint_checksum",
+    "nwg_checkpoint_identity_hash",
 ]
 
 
@@ -126,6 +151,20 @@ def lib() -> C.CDLL:
     L.nwg_advance.argtypes = [_vp, C.c_uint32, C.POINTER(RuntimeWordCounts), C.POINTER(AssemblyConfig),
                               C.POINTER(PendingInjection), POST_FITNESS_FN, _vp, SHARD_RELEASE_FN, _vp,
                               C.POINTER(ShardReleaseHistory)]
+    L.nwg_prepare_generation.argtypes = L.nwg_advance.argtypes
+    L.nwg_assemble_prepared.argtypes = [_vp]
+    L.nwg_checkpoint_capture.argtypes = L.nwg_advance.argtypes + [_vp, _sz, C.POINTER(CheckpointRecord)]
+    L.nwg_checkpoint_restore.argtypes = [C.POINTER(CheckpointRecord), C.POINTER(_vp)]
+    L.nwg_checkpoint_resume.argtypes = [_vp]
+    L.nwg_checkpoint_write.argtypes = [C.POINTER(CheckpointRecord), C.c_char_p]
+    L.nwg_checkpoint_read.argtypes = [C.c_char_p, C.POINTER(CheckpointRecord)]
+    L.nwg_checkpoint_free.argtypes = [C.POINTER(CheckpointRecord)]
+    L.nwg_checkpoint_free.restype = None
+    L.nwg_checkpoint_checksum.argtypes = [C.POINTER(CheckpointRecord)]
+    L.nwg_checkpoint_checksum.restype = C.c_uint64
+    L.nwg_checkpoint_identity_hash.argtypes = [C.POINTER(RuntimeWordCounts), C.POINTER(ShardReleaseHistory), _vp,
+                                               _sz]
+    L.nwg_checkpoint_identity_hash.restype = C.c_uint64
     L.nwg_swap_generations.argtypes = [_vp]
     L.nwg_read_status.argtypes = [_vp, C.POINTER(C.c_int)]
     L.nwg_download_current_generation.argtypes = [_vp, _vp, _vp, _vp, _vp, _sz, C.POINTER(_sz), C.POINTER(_sz)]
@@ -276,15 +315,59 @@ class Runtime:
         check(lib().nwg_read_evaluation_stats(self.handle, C.byref(s)), "nwg_read_evaluation_stats")
         return s
 
+    @classmethod
+    def _adopt(cls, handle: C.c_void_p) -> "Runtime":
+        """Wraps a runtime made by the library (a restored checkpoint's)."""
+        rt = cls.__new__(cls)
+        rt.handle = handle
+        rt._keep = []
+        info = rt.info()
+        rt.action_count = info.action_count
+        rt.population = info.max_generation_size
+        rt.columns = info.grid_column_count
+        return rt
+
+    def _boundary_args(self, seed, counts, config, pending, post_fitness, shard_release, history):
+        pf = POST_FITNESS_FN(post_fitness) if post_fitness else POST_FITNESS_FN()
+        sr = SHARD_RELEASE_FN(shard_release) if shard_release else SHARD_RELEASE_FN()
+        self._callbacks = (pf, sr)
+        return (self.handle, seed, C.byref(counts), C.byref(config) if config else None,
+                C.byref(pending) if pending else None, pf, None, sr, None, C.byref(history) if history else None)
+
     def advance(self, seed: int, counts: RuntimeWordCounts, config: AssemblyConfig | None = None,
                 pending: PendingInjection | None = None, post_fitness=None, shard_release=None,
                 history: ShardReleaseHistory | None = None) -> None:
-        pf = POST_FITNESS_FN(post_fitness) if post_fitness else POST_FITNESS_FN()
-        sr = SHARD_RELEASE_FN(shard_release) if shard_release else SHARD_RELEASE_FN()
-        check(lib().nwg_advance(self.handle, seed, C.byref(counts), C.byref(config) if config else None,
-                                C.byref(pending) if pending else None, pf, None, sr, None,
-                                C.byref(history) if history else None), "nwg_advance")
+        check(lib().nwg_advance(*self._boundary_args(seed, counts, config, pending, post_fitness, shard_release,
+                                                     history)), "nwg_advance")
         self.action_count = self.info().action_count  # an injection widens the action space
+
+    def prepare(self, seed: int, counts: RuntimeWordCounts, config: AssemblyConfig | None = None,
+                pending: PendingInjection | None = None, post_fitness=None, shard_release=None,
+                history: ShardReleaseHistory | None = None) -> None:
+        """The first half of advance: evaluate, run the callbacks, plan the next generation's parents."""
+        check(lib().nwg_prepare_generation(*self._boundary_args(seed, counts, config, pending, post_fitness,
+                                                                shard_release, history)), "nwg_prepare_generation")
+
+    def resume(self) -> None:
+        """TryResumeGenerationFromCheckpointOnDevice: assemble a restored boundary."""
+        check(lib().nwg_checkpoint_resume(self.handle), "nwg_checkpoint_resume")
+        self.action_count = self.info().action_count
+
+    def assemble(self) -> None:
+        """The second half of advance: breed (and widen/inject) the planned children and swap them in."""
+        check(lib().nwg_assemble_prepared(self.handle), "nwg_assemble_prepared")
+        self.action_count = self.info().action_count
+
+    def checkpoint(self, seed: int, counts: RuntimeWordCounts, config: AssemblyConfig | None = None,
+                   pending: PendingInjection | None = None, post_fitness=None, shard_release=None,
+                   history: ShardReleaseHistory | None = None, catalog: np.ndarray | None = None) -> "Checkpoint":
+        """prepare, then the pre-breeding boundary as a Checkpoint (the runtime stays prepared)."""
+        rec = CheckpointRecord()
+        cat = None if catalog is None else np.ascontiguousarray(catalog, np.uint8)
+        args = self._boundary_args(seed, counts, config, pending, post_fitness, shard_release, history)
+        check(lib().nwg_checkpoint_capture(*args, _np_ptr(cat), 0 if cat is None else len(cat), C.byref(rec)),
+              "nwg_checkpoint_capture")
+        return Checkpoint._take(rec)
 
     def status(self) -> int:
         v = C.c_int()
@@ -333,3 +416,83 @@ class Runtime:
         pitch = _sz()
         check(lib().nwg_device_slab(self.handle, C.byref(ptr), C.byref(pitch)), "nwg_device_slab")
         return ptr.value, pitch.value
+
+
+class Checkpoint:
+    """A RuntimeCheckpoint (slab_runtime.hpp:86-117) on the host: the scalar records in `record` (a
+    CheckpointRecord whose pointers are kept pointing at the numpy arrays below) and the arrays as numpy."""
+
+    _ARRAYS = (("slot_indices", np.uint32), ("fitness", np.float32), ("evaluation_counts", np.uint32),
+               ("has_fitness", np.uint8))
+
+    def __init__(self, record: CheckpointRecord, slot_indices, fitness, evaluation_counts, has_fitness,
+                 parent_pairs, live_organisms, live_genomes):
+        self.record = record
+        self.slot_indices = np.ascontiguousarray(slot_indices, np.uint32)
+        self.fitness = np.ascontiguousarray(fitness, np.float32)
+        self.evaluation_counts = np.ascontiguousarray(evaluation_counts, np.uint32)
+        self.has_fitness = np.ascontiguousarray(has_fitness, np.uint8)
+        self.parent_pairs = np.ascontiguousarray(parent_pairs, np.uint32).reshape(-1, 2)
+        self.live_organisms = np.ascontiguousarray(live_organisms, np.uint32)
+        self.live_genomes = np.ascontiguousarray(live_genomes, np.uint8).reshape(len(self.live_organisms), -1)
+        self._bind()
+
+    def _bind(self) -> None:
+        r = self.record
+        r.individual_count = len(self.slot_indices)
+        r.child_count = len(self.parent_pairs)
+        r.live_count = len(self.live_organisms)
+        for name in ("slot_indices", "fitness", "evaluation_counts", "has_fitness", "parent_pairs", "live_organisms",
+                     "live_genomes"):
+            setattr(r, name, _np_ptr(getattr(self, name)))
+
+    @classmethod
+    def _take(cls, rec: CheckpointRecord) -> "Checkpoint":
+        """Copies a library-filled record's arrays into numpy and frees the library's copies."""
+        def arr(ptr, n, dt):
+            if n == 0 or not ptr:
+                return np.zeros(0, dt)
+            return np.ctypeslib.as_array(C.cast(ptr, C.POINTER(np.ctypeslib.as_ctypes_type(dt))), (n,)).copy()
+        n, k, live = rec.individual_count, rec.child_count, rec.live_count
+        stride = rec.slab_layout.slot_stride_bytes
+        try:
+            out = cls(CheckpointRecord.from_buffer_copy(rec), arr(rec.slot_indices, n, np.uint32),
+                      arr(rec.fitness, n, np.float32), arr(rec.evaluation_counts, n, np.uint32),
+                      arr(rec.has_fitness, n, np.uint8), arr(rec.parent_pairs, 2 * k, np.uint32),
+                      arr(rec.live_organisms, live, np.uint32), arr(rec.live_genomes, live * stride, np.uint8))
+        finally:
+            lib().nwg_checkpoint_free(C.byref(rec))
+        return out
+
+    def checksum(self) -> int:
+        self._bind()
+        return lib().nwg_checkpoint_checksum(C.byref(self.record))
+
+    def seal(self) -> None:
+        """Stores the current checksum (after the fields were edited)."""
+        self.record.checksum = self.checksum()
+
+    def write(self, path) -> None:
+        self._bind()
+        check(lib().nwg_checkpoint_write(C.byref(self.record), str(path).encode()), "nwg_checkpoint_write")
+
+    @classmethod
+    def read(cls, path) -> "Checkpoint":
+        rec = CheckpointRecord()
+        check(lib().nwg_checkpoint_read(str(path).encode(), C.byref(rec)), "nwg_checkpoint_read")
+        return cls._take(rec)
+
+    def restore(self) -> Runtime:
+        """A new runtime at this checkpoint's boundary; Runtime.resume() (= assemble) continues it."""
+        self._bind()
+        handle = _vp()
+        check(lib().nwg_checkpoint_restore(C.byref(self.record), C.byref(handle)), "nwg_checkpoint_restore")
+        return Runtime._adopt(handle)
+
+
+def identity_hash(counts: RuntimeWordCounts, history: ShardReleaseHistory | None = None,
+                  catalog: np.ndarray | None = None) -> int:
+    cat = None if catalog is None else np.ascontiguousarray(catalog, np.uint8)
+    return lib().nwg_checkpoint_identity_hash(C.byref(counts), C.byref(history) if history else None, _np_ptr(cat),
+                                              0 if cat is None else len(cat))
+

@@ -79,6 +79,15 @@ struct nwg_runtime {
     std::size_t tc_tables_bytes = 0;
     std::uint8_t *trunk_tables = nullptr;
     float margin_tau = 1.0e-3f;
+    // a generation prepared for assembly (evaluated and planned; nwg_prepare_generation / checkpoint restore)
+    bool prepared = false;
+    std::uint32_t prepared_seed = 0;
+    nwg_generation_assembly_config prepared_config{};
+    nwg_pending_injection prepared_injection{};
+    std::size_t prepared_next_action_count = 0;
+    // the current generation holds released parents (slot 0xFFFFFFFF), as a restored boundary does; it can only
+    // be assembled, not evaluated
+    bool released_parents = false;
 
     // pinned host staging
     ShardRecord *host_shards = nullptr;
@@ -387,7 +396,7 @@ int EvaluateImpl(nwg_runtime *rt, const nwg_runtime_word_counts *counts, const n
         return kInvalidRuntimeConfig;
     }
     if (rt->max_generation_size == 0 || rt->cur_gen_size == 0 || rt->cur_gen_size > rt->max_generation_size ||
-        rt->cur_gen_size % rt->grid_column_count != 0) {
+        rt->cur_gen_size % rt->grid_column_count != 0 || rt->released_parents) {
         return kInvalidGeneration;
     }
     NWG_TRY(cudaMemsetAsync(rt->status, 0, sizeof(int), rt->stream));
@@ -501,6 +510,7 @@ int AdvanceWithInjection(nwg_runtime *rt, std::uint32_t generation_seed, const n
                          const nwg_pending_injection &injection, const std::vector<HintGroup> &hints,
                          std::size_t next_action_count, std::size_t next_size) {
     const std::size_t n = injection.injection_count;
+    const std::size_t parent_action_count = injection.first_catalog_word_index;
     const std::size_t new_pitch = SlotPitchBytes(next_action_count);
     const std::size_t new_slots = SlotsForBudget(rt->slab_byte_budget, next_action_count);
     if (new_slots < next_size || new_slots >= 0xFFFFFFFFull) {
@@ -585,7 +595,7 @@ int AdvanceWithInjection(nwg_runtime *rt, std::uint32_t generation_seed, const n
     bp.child_slots = rt->next_slots;
     bp.pairs = rt->pairs;
     bp.child_count = static_cast<std::uint32_t>(next_size);
-    bp.action_count = static_cast<std::uint32_t>(rt->action_count);  // the parents' rows
+    bp.action_count = static_cast<std::uint32_t>(parent_action_count);  // the parents' rows
     bp.generation_seed = generation_seed;
     bp.generation_index = rt->cur_gen_index;
     bp.crossover_l1 = cfg.breeding.crossover_temperature_level1;
@@ -597,7 +607,7 @@ int AdvanceWithInjection(nwg_runtime *rt, std::uint32_t generation_seed, const n
     bp.status = rt->status;
     ok = ok && LaunchBreed(bp, rt->stream) == cudaSuccess;
     ok = ok && LaunchInject(new_slab, new_pitch, rt->next_slots, static_cast<std::uint32_t>(next_size),
-                            static_cast<std::uint32_t>(rt->action_count), static_cast<std::uint32_t>(n), d_codes,
+                            static_cast<std::uint32_t>(parent_action_count), static_cast<std::uint32_t>(n), d_codes,
                             d_tiles, d_chunks, d_order, static_cast<int>(chunks.size()), rt->scratch, d_sums,
                             rt->scratch_ctas, rt->status, rt->stream) == cudaSuccess;
     ok = ok && cudaMemsetAsync(rt->next_fitness, 0, rt->max_generation_size * sizeof(float), rt->stream) == cudaSuccess &&
@@ -639,6 +649,142 @@ int AdvanceWithInjection(nwg_runtime *rt, std::uint32_t generation_seed, const n
 
 }  // namespace
 
+namespace nwg {
+
+int CreateShapedRuntime(const RuntimeShape &shape, nwg_runtime **out) {
+    *out = nullptr;
+    const std::size_t max_gen = shape.max_generation_size;
+    const std::size_t slot_count = shape.slot_count;
+    if (shape.action_count == 0 || shape.grid_column_count == 0 || max_gen == 0 || slot_count == 0 ||
+        slot_count >= 0xFFFFFFFFull || shape.epicenter_rows == 0) {
+        return kInvalidRuntimeConfig;
+    }
+    nwg_runtime *rt = new (std::nothrow) nwg_runtime();
+    if (rt == nullptr) {
+        return kInvalidRuntimeConfig;
+    }
+    rt->action_count = shape.action_count;
+    rt->stride = GenomeStrideBytes(shape.action_count);
+    rt->pitch = SlotPitchBytes(shape.action_count);
+    rt->slot_count = slot_count;
+    rt->max_generation_size = max_gen;
+    rt->grid_column_count = shape.grid_column_count;
+    rt->generation_byte_budget = shape.generation_byte_budget;
+    rt->slab_byte_budget = shape.slab_bytes;
+    rt->host_spill_budget = shape.host_spill_budget;
+    rt->epicenter_rows = shape.epicenter_rows;
+    rt->scratch_ctas = EvalCtaCount(0xFFFFFFFFu);
+    bool ok = true;
+    auto alloc = [&](auto **ptr, std::size_t bytes) {
+        ok = ok && cudaMalloc(reinterpret_cast<void **>(ptr), bytes) == cudaSuccess;
+        if (ok) {
+            ok = cudaMemset(*ptr, 0, bytes) == cudaSuccess;
+        }
+    };
+    alloc(&rt->slab, slot_count * rt->pitch);
+    alloc(&rt->cur_slots, max_gen * sizeof(std::uint32_t));
+    alloc(&rt->next_slots, max_gen * sizeof(std::uint32_t));
+    alloc(&rt->cur_fitness, max_gen * sizeof(float));
+    alloc(&rt->next_fitness, max_gen * sizeof(float));
+    alloc(&rt->cur_eval, max_gen * sizeof(std::uint32_t));
+    alloc(&rt->next_eval, max_gen * sizeof(std::uint32_t));
+    alloc(&rt->cur_has, max_gen);
+    alloc(&rt->next_has, max_gen);
+    alloc(&rt->pairs, max_gen * 2 * sizeof(std::uint32_t));
+    alloc(&rt->slot_used, slot_count);
+    alloc(&rt->status, sizeof(int));
+    alloc(&rt->summary, sizeof(SummaryDevice));
+    alloc(&rt->shards, NWG_CATALOG_CAPACITY * sizeof(ShardRecord));
+    alloc(&rt->local_words, max_gen * sizeof(std::uint32_t));
+    alloc(&rt->chunk_start, (max_gen + 1) * sizeof(std::uint32_t));
+    alloc(&rt->score_sum, max_gen * sizeof(std::uint32_t));
+    alloc(&rt->steps, kStepCounters * sizeof(unsigned long long));
+    alloc(&rt->scratch, static_cast<std::size_t>(rt->scratch_ctas) * EvalScratchFloatsPerCta() * sizeof(float));
+    ok = ok && cudaMallocHost(&rt->host_shards, NWG_CATALOG_CAPACITY * sizeof(ShardRecord)) == cudaSuccess;
+    ok = ok && cudaMallocHost(&rt->host_status, sizeof(int)) == cudaSuccess;
+    ok = ok && cudaMallocHost(&rt->host_summary, sizeof(SummaryDevice)) == cudaSuccess;
+    ok = ok && cudaMallocHost(&rt->host_steps, kStepCounters * sizeof(unsigned long long)) == cudaSuccess;
+    ok = ok && cudaEventCreate(&rt->eval_begin) == cudaSuccess && cudaEventCreate(&rt->eval_end) == cudaSuccess;
+    if (!ok) {
+        FreeRuntime(rt);
+        return kCudaFailure;
+    }
+    std::memset(rt->host_summary, 0, sizeof(SummaryDevice));
+    std::memset(rt->host_steps, 0, kStepCounters * sizeof(unsigned long long));
+    *out = rt;
+    return kOk;
+}
+
+int ReadBoundary(const nwg_runtime *rt, BoundaryState *out) {
+    if (rt == nullptr || out == nullptr) {
+        return kInvalidRuntimeConfig;
+    }
+    if (!rt->prepared) {
+        return kInvalidAssemblyPlan;
+    }
+    out->seed = rt->prepared_seed;
+    out->config = rt->prepared_config;
+    out->injection = rt->prepared_injection;
+    out->action_count = rt->action_count;
+    out->next_action_count = rt->prepared_next_action_count;
+    out->stride = rt->stride;
+    out->slot_count = rt->slot_count;
+    out->slab_bytes = rt->slab_byte_budget;
+    out->generation_byte_budget = rt->generation_byte_budget;
+    out->host_spill_budget = rt->host_spill_budget;
+    out->max_generation_size = rt->max_generation_size;
+    out->grid_column_count = rt->grid_column_count;
+    out->epicenter_rows = rt->epicenter_rows;
+    out->generation_index = rt->cur_gen_index;
+    out->generation_size = rt->cur_gen_size;
+    out->planned_children = rt->planned_children;
+    return kOk;
+}
+
+int InstallBoundary(nwg_runtime *rt, const std::uint32_t *slots, const float *fitness, const std::uint32_t *eval,
+                    const std::uint8_t *has, std::size_t count, std::size_t generation_index,
+                    const std::uint32_t *pairs, std::size_t child_count, std::uint32_t seed,
+                    const nwg_generation_assembly_config &config, const nwg_pending_injection &injection,
+                    std::size_t next_action_count) {
+    if (count == 0 || count > rt->max_generation_size || child_count == 0 || child_count > rt->max_generation_size) {
+        return kInvalidCheckpoint;
+    }
+    bool released = false;
+    for (std::size_t i = 0; i < count; ++i) {
+        if (slots[i] == 0xFFFFFFFFu) {
+            released = true;
+        } else if (slots[i] >= rt->slot_count) {
+            return kInvalidCheckpoint;
+        }
+    }
+    for (std::size_t c = 0; c < 2 * child_count; ++c) {
+        if (pairs[c] >= count || slots[pairs[c]] == 0xFFFFFFFFu) {
+            return kInvalidCheckpoint;
+        }
+    }
+    NWG_TRY(cudaStreamSynchronize(rt->stream));
+    NWG_TRY(cudaMemcpy(rt->cur_slots, slots, count * sizeof(std::uint32_t), cudaMemcpyHostToDevice));
+    NWG_TRY(cudaMemcpy(rt->cur_fitness, fitness, count * sizeof(float), cudaMemcpyHostToDevice));
+    NWG_TRY(cudaMemcpy(rt->cur_eval, eval, count * sizeof(std::uint32_t), cudaMemcpyHostToDevice));
+    NWG_TRY(cudaMemcpy(rt->cur_has, has, count, cudaMemcpyHostToDevice));
+    NWG_TRY(cudaMemcpy(rt->pairs, pairs, child_count * 2 * sizeof(std::uint32_t), cudaMemcpyHostToDevice));
+    NWG_TRY(cudaMemset(rt->status, 0, sizeof(int)));
+    rt->cur_gen_index = generation_index;
+    rt->cur_gen_size = count;
+    rt->next_gen_index = 0;
+    rt->next_gen_size = 0;
+    rt->planned_children = child_count;
+    rt->released_parents = released;
+    rt->prepared = true;
+    rt->prepared_seed = seed;
+    rt->prepared_config = config;
+    rt->prepared_injection = injection;
+    rt->prepared_next_action_count = next_action_count;
+    return kOk;
+}
+
+}  // namespace nwg
+
 extern "C" {
 
 int nwg_abi_version(void) { return NWG_ABI_VERSION; }
@@ -665,6 +811,7 @@ const char *nwg_status_string(int status) {
     case NWG_SLAB_REPACK_FAILED: return "slab compaction/repacking failed";
     case NWG_TIMEOUT: return "a bounded device wait gave up";
     case NWG_UNSUPPORTED: return "request not supported by this runtime";
+    case NWG_INVALID_CHECKPOINT: return "invalid runtime checkpoint";
     default: return "unknown slab ga runtime status";
     }
 }
@@ -712,6 +859,9 @@ int nwg_upload_catalog(const uint8_t *letters, size_t word_count) {
     return kOk;
 }
 
+// TryCreateDeviceSlabGARuntimeBuffers (slab_runtime.cu:943-1003): slot count from the slab budget, generation
+// capacity from the generation budget (floored to whole grid rows); the slab's byte size is slot_count x stride
+// (genotype_slab/device_runtime.cu:1047-1050), which action-space growth re-divides at the wider stride.
 int nwg_create(const nwg_runtime_config *config, nwg_runtime **runtime_out) {
     if (runtime_out == nullptr) {
         return kInvalidRuntimeConfig;
@@ -727,60 +877,17 @@ int nwg_create(const nwg_runtime_config *config, nwg_runtime **runtime_out) {
     if (slot_count < max_gen || max_gen == 0 || slot_count >= 0xFFFFFFFFull) {
         return kInvalidRuntimeConfig;
     }
-    nwg_runtime *rt = new (std::nothrow) nwg_runtime();
-    if (rt == nullptr) {
-        return kInvalidRuntimeConfig;
-    }
-    rt->action_count = config->action_count;
-    rt->stride = GenomeStrideBytes(config->action_count);
-    rt->pitch = SlotPitchBytes(config->action_count);
-    rt->slot_count = slot_count;
-    rt->max_generation_size = max_gen;
-    rt->grid_column_count = config->grid_column_count;
-    rt->generation_byte_budget = max_gen * rt->stride;
-    rt->slab_byte_budget = config->genotype_slab_byte_budget_bytes;
-    rt->host_spill_budget = config->host_spillover_byte_budget_bytes;
-    rt->epicenter_rows = max_gen / config->grid_column_count;
-    rt->scratch_ctas = EvalCtaCount(0xFFFFFFFFu);
-    bool ok = true;
-    auto alloc = [&](auto **ptr, std::size_t bytes) {
-        ok = ok && cudaMalloc(reinterpret_cast<void **>(ptr), bytes) == cudaSuccess;
-        if (ok) {
-            ok = cudaMemset(*ptr, 0, bytes) == cudaSuccess;
-        }
-    };
-    alloc(&rt->slab, slot_count * rt->pitch);
-    alloc(&rt->cur_slots, max_gen * sizeof(std::uint32_t));
-    alloc(&rt->next_slots, max_gen * sizeof(std::uint32_t));
-    alloc(&rt->cur_fitness, max_gen * sizeof(float));
-    alloc(&rt->next_fitness, max_gen * sizeof(float));
-    alloc(&rt->cur_eval, max_gen * sizeof(std::uint32_t));
-    alloc(&rt->next_eval, max_gen * sizeof(std::uint32_t));
-    alloc(&rt->cur_has, max_gen);
-    alloc(&rt->next_has, max_gen);
-    alloc(&rt->pairs, max_gen * 2 * sizeof(std::uint32_t));
-    alloc(&rt->slot_used, slot_count);
-    alloc(&rt->status, sizeof(int));
-    alloc(&rt->summary, sizeof(SummaryDevice));
-    alloc(&rt->shards, NWG_CATALOG_CAPACITY * sizeof(ShardRecord));
-    alloc(&rt->local_words, max_gen * sizeof(std::uint32_t));
-    alloc(&rt->chunk_start, (max_gen + 1) * sizeof(std::uint32_t));
-    alloc(&rt->score_sum, max_gen * sizeof(std::uint32_t));
-    alloc(&rt->steps, kStepCounters * sizeof(unsigned long long));
-    alloc(&rt->scratch, static_cast<std::size_t>(rt->scratch_ctas) * EvalScratchFloatsPerCta() * sizeof(float));
-    ok = ok && cudaMallocHost(&rt->host_shards, NWG_CATALOG_CAPACITY * sizeof(ShardRecord)) == cudaSuccess;
-    ok = ok && cudaMallocHost(&rt->host_status, sizeof(int)) == cudaSuccess;
-    ok = ok && cudaMallocHost(&rt->host_summary, sizeof(SummaryDevice)) == cudaSuccess;
-    ok = ok && cudaMallocHost(&rt->host_steps, kStepCounters * sizeof(unsigned long long)) == cudaSuccess;
-    ok = ok && cudaEventCreate(&rt->eval_begin) == cudaSuccess && cudaEventCreate(&rt->eval_end) == cudaSuccess;
-    if (!ok) {
-        FreeRuntime(rt);
-        return kCudaFailure;
-    }
-    std::memset(rt->host_summary, 0, sizeof(SummaryDevice));
-    std::memset(rt->host_steps, 0, kStepCounters * sizeof(unsigned long long));
-    *runtime_out = rt;
-    return kOk;
+    const std::size_t stride = GenomeStrideBytes(config->action_count);
+    RuntimeShape shape{};
+    shape.action_count = config->action_count;
+    shape.slot_count = slot_count;
+    shape.slab_bytes = slot_count * stride;
+    shape.max_generation_size = max_gen;
+    shape.grid_column_count = config->grid_column_count;
+    shape.generation_byte_budget = max_gen * stride;
+    shape.host_spill_budget = config->host_spillover_byte_budget_bytes;
+    shape.epicenter_rows = max_gen / config->grid_column_count;
+    return CreateShapedRuntime(shape, runtime_out);
 }
 
 void nwg_destroy(nwg_runtime *runtime) {
@@ -847,6 +954,7 @@ int nwg_bootstrap(nwg_runtime *rt, size_t generation_size, uint32_t generation_s
     if (rt == nullptr) {
         return kInvalidRuntimeConfig;
     }
+    rt->prepared = false;
     if (generation_size == 0 || generation_size > rt->max_generation_size ||
         generation_size % rt->grid_column_count != 0) {
         return kInvalidGeneration;
@@ -872,6 +980,7 @@ int nwg_bootstrap(nwg_runtime *rt, size_t generation_size, uint32_t generation_s
     }
     rt->cur_gen_index = generation_index;
     rt->cur_gen_size = generation_size;
+    rt->released_parents = false;
     rt->next_gen_index = 0;
     rt->next_gen_size = 0;
     rt->planned_children = 0;
@@ -964,13 +1073,15 @@ int nwg_read_evaluation_stats(const nwg_runtime *rt, nwg_evaluation_stats *stats
     return kOk;
 }
 
-int nwg_advance(nwg_runtime *rt, uint32_t generation_seed, const nwg_runtime_word_counts *counts,
-                const nwg_generation_assembly_config *config, const nwg_pending_injection *pending,
-                nwg_post_fitness_fn post_fitness, void *post_fitness_user, nwg_shard_release_fn shard_release,
-                void *shard_release_user, const nwg_shard_release_history *history) {
+int nwg_prepare_generation(nwg_runtime *rt, uint32_t generation_seed, const nwg_runtime_word_counts *counts,
+                           const nwg_generation_assembly_config *config, const nwg_pending_injection *pending,
+                           nwg_post_fitness_fn post_fitness, void *post_fitness_user,
+                           nwg_shard_release_fn shard_release, void *shard_release_user,
+                           const nwg_shard_release_history *history) {
     if (rt == nullptr || counts == nullptr) {
         return kInvalidRuntimeConfig;
     }
+    rt->prepared = false;
     nwg_generation_assembly_config cfg{};
     cfg.parent_selection.cellular_breeding_radius = 2;  // selection.hpp:13-18, spatial/grid.hpp:11
     cfg.parent_selection.rank_exponent = 0.5f;
@@ -1058,8 +1169,38 @@ int nwg_advance(nwg_runtime *rt, uint32_t generation_seed, const nwg_runtime_wor
             return SetHostStatus(rt, kInvalidAssemblyConfig);
         }
     }
+    rt->prepared = true;
+    rt->prepared_seed = generation_seed;
+    rt->prepared_config = cfg;
+    rt->prepared_injection = injection;
+    rt->prepared_next_action_count = next_action_count;
+    return kOk;
+}
+
+// TryAssemblePreparedGenerationOnDevice (slab_runtime.cu:1511-1680): breed (and inject) the planned children,
+// then swap generations.
+int nwg_assemble_prepared(nwg_runtime *rt) {
+    if (rt == nullptr) {
+        return kInvalidRuntimeConfig;
+    }
+    if (!rt->prepared) {
+        return SetHostStatus(rt, kInvalidAssemblyPlan);
+    }
+    rt->prepared = false;
+    const std::uint32_t generation_seed = rt->prepared_seed;
+    const nwg_generation_assembly_config cfg = rt->prepared_config;
+    const nwg_pending_injection injection = rt->prepared_injection;
+    const std::size_t next_size = rt->planned_children;
     if (injection.enabled) {
-        return AdvanceWithInjection(rt, generation_seed, cfg, injection, hints, next_action_count, next_size);
+        std::vector<HintGroup> hints(injection.injection_count);
+        for (std::size_t i = 0; i < injection.injection_count; ++i) {
+            if (injection.first_catalog_word_index + i >= g_catalog.host_codes.size() ||
+                !BuildHintGroup(g_catalog.host_codes[injection.first_catalog_word_index + i], hints[i])) {
+                return SetHostStatus(rt, kOutputEmbeddingInjectionFailed);
+            }
+        }
+        return AdvanceWithInjection(rt, generation_seed, cfg, injection, hints, rt->prepared_next_action_count,
+                                    next_size);
     }
     PlanChildSlotsKernel<<<1, 1024, 0, rt->stream>>>(rt->pairs, static_cast<std::uint32_t>(next_size), rt->cur_slots,
                                                      static_cast<std::uint32_t>(rt->cur_gen_size), rt->slot_used,
@@ -1089,13 +1230,22 @@ int nwg_advance(nwg_runtime *rt, uint32_t generation_seed, const nwg_runtime_wor
     NWG_TRY(cudaMemsetAsync(rt->next_fitness, 0, rt->max_generation_size * sizeof(float), rt->stream));
     NWG_TRY(cudaMemsetAsync(rt->next_eval, 0, rt->max_generation_size * sizeof(std::uint32_t), rt->stream));
     NWG_TRY(cudaMemsetAsync(rt->next_has, 0, rt->max_generation_size, rt->stream));
-    st = Sync(rt);
+    const int st = Sync(rt);
     if (st != kOk) {
         return st;
     }
     rt->next_gen_index = rt->cur_gen_index + 1;
     rt->next_gen_size = next_size;
     return nwg_swap_generations(rt);
+}
+
+int nwg_advance(nwg_runtime *rt, uint32_t generation_seed, const nwg_runtime_word_counts *counts,
+                const nwg_generation_assembly_config *config, const nwg_pending_injection *pending,
+                nwg_post_fitness_fn post_fitness, void *post_fitness_user, nwg_shard_release_fn shard_release,
+                void *shard_release_user, const nwg_shard_release_history *history) {
+    const int st = nwg_prepare_generation(rt, generation_seed, counts, config, pending, post_fitness, post_fitness_user,
+                                          shard_release, shard_release_user, history);
+    return st != kOk ? st : nwg_assemble_prepared(rt);
 }
 
 int nwg_swap_generations(nwg_runtime *rt) {
@@ -1108,6 +1258,8 @@ int nwg_swap_generations(nwg_runtime *rt) {
     std::swap(rt->cur_has, rt->next_has);
     std::swap(rt->cur_gen_index, rt->next_gen_index);
     std::swap(rt->cur_gen_size, rt->next_gen_size);
+    rt->prepared = false;
+    rt->released_parents = false;
     return kOk;
 }
 
@@ -1194,6 +1346,8 @@ int nwg_upload_current_generation(nwg_runtime *rt, const uint32_t *slot_indices,
     }
     rt->cur_gen_size = count;
     rt->cur_gen_index = generation_index;
+    rt->prepared = false;
+    rt->released_parents = false;
     return kOk;
 }
 

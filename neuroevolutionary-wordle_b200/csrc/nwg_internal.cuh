@@ -6,6 +6,7 @@
 #include <cstddef>
 #include <cstdint>
 
+#include "../../include/nwg_capi.h"
 #include "nwg_layout.cuh"
 
 namespace nwg {
@@ -32,6 +33,7 @@ enum Status : int {
     kSlabRepackFailed = 16,
     kTimeout = 17,
     kUnsupported = 18,
+    kInvalidCheckpoint = 19,
 };
 
 __device__ inline void SetStatus(int *status, int code) { atomicCAS(status, 0, code); }
@@ -162,5 +164,37 @@ cudaError_t LaunchInject(std::uint8_t *slab, std::size_t pitch, const std::uint3
 cudaError_t LaunchBootstrap(std::uint8_t *slab, std::size_t pitch, const std::uint32_t *slots,
                             std::uint32_t population, std::uint64_t generation_index, std::uint32_t seed,
                             std::uint32_t action_count, cudaStream_t stream);
+
+// ---- the pre-breeding boundary, for checkpoints (checkpoint.cu) ----
+
+// What a prepared runtime holds between nwg_prepare_generation and nwg_assemble_prepared, in the reference's
+// terms: slab_bytes is GenotypeSlabLayout::slab_bytes (slot_count x stride at creation, kept across widening).
+struct BoundaryState {
+    std::uint32_t seed;
+    nwg_generation_assembly_config config;
+    nwg_pending_injection injection;
+    std::size_t action_count, next_action_count, stride, slot_count, slab_bytes;
+    std::size_t generation_byte_budget, host_spill_budget, max_generation_size, grid_column_count, epicenter_rows;
+    std::size_t generation_index, generation_size, planned_children;
+};
+
+// kInvalidAssemblyPlan when the runtime is not prepared.
+int ReadBoundary(const nwg_runtime *rt, BoundaryState *out);
+
+// A runtime with explicit sizes (a restored checkpoint's, slab_runtime.cu:1746-1765).
+struct RuntimeShape {
+    std::size_t action_count, slot_count, slab_bytes, max_generation_size, grid_column_count;
+    std::size_t generation_byte_budget, host_spill_budget, epicenter_rows;
+};
+int CreateShapedRuntime(const RuntimeShape &shape, nwg_runtime **out);
+
+// Installs a restored boundary: the current generation (slots may be 0xFFFFFFFF for released parents, which no
+// child references; evaluation is refused until the next swap), its fitness, the parent plan and the assembly
+// inputs; the runtime is left prepared.
+int InstallBoundary(nwg_runtime *rt, const std::uint32_t *slots, const float *fitness, const std::uint32_t *eval,
+                    const std::uint8_t *has, std::size_t count, std::size_t generation_index,
+                    const std::uint32_t *pairs, std::size_t child_count, std::uint32_t seed,
+                    const nwg_generation_assembly_config &config, const nwg_pending_injection &injection,
+                    std::size_t next_action_count);
 
 }  // namespace nwg

@@ -5,8 +5,9 @@ Outputs:
   oracle/_lib/libnwg_tape.so    -- GPU draw tapes for the oracle (nwg_tape.cu), nvcc sm_100a
   oracle/_ref/libref_host.so    -- the reference's host-callable code + episode loop harness
   oracle/_ref/libref_dev.so     -- the reference's device functions + harness kernels, sm_100a
+  oracle/_ref/libref_ckpt.so    -- the reference's runtime (checkpoint format, capture, restore, resume), sm_100a
 
-The two oracle/_ref libraries are compiled from the reference's own headers where they
+The oracle/_ref libraries are compiled from the reference's own headers where they
 lie (REFERENCE_ROOT/src); nothing is copied. They are only rebuilt when the reference
 tree is present; elsewhere the prebuilt files are used as they are.
 """
@@ -75,7 +76,12 @@ def build_reference(force: bool = False) -> list[Path]:
         _run([NVCC, *ARCH, "-O3", "-std=c++20", *inc, "-Xcompiler", "-fPIC", "-shared",
               "-DNEUROEVOLUTION_PROJECT_SOURCE_DIR=\"/nonexistent\"",
               str(HERE / "ref_dev_harness.cu"), "-o", str(dev_out)])
-    return [host_out, dev_out]
+    ckpt_out = REF_DIR / "libref_ckpt.so"
+    if force or _stale(ckpt_out, [HERE / "ref_ckpt_harness.cu"]):
+        _run([NVCC, *ARCH, "-O3", "-std=c++20", *inc, "-Xcompiler", "-fPIC", "-shared",
+              "-DNEUROEVOLUTION_PROJECT_SOURCE_DIR=\"/nonexistent\"",
+              str(HERE / "ref_ckpt_harness.cu"), "-o", str(ckpt_out)])
+    return [host_out, dev_out, ckpt_out]
 
 
 def build_all(force: bool = False) -> None:

@@ -277,6 +277,25 @@ def ref_host() -> C.CDLL | None:
     return L
 
 
+@lru_cache(None)
+def ref_ckpt() -> C.CDLL | None:
+    """The reference's runtime-checkpoint code (oracle/ref_ckpt_harness.cu), or None when not built."""
+    path = HERE / "_ref" / "libref_ckpt.so"
+    if not path.exists():
+        return None
+    L = C.CDLL(str(path))
+    L.refckpt_roundtrip.argtypes = [C.c_char_p, C.c_char_p]
+    L.refckpt_write_synthetic.argtypes = [C.c_char_p, C.c_uint32, _sz, _sz, _sz, _sz, C.c_int]
+    L.refckpt_identity_hash.restype = C.c_uint64
+    L.refckpt_identity_hash.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, _sz]
+    L.refckpt_layouts.argtypes = [C.POINTER(_sz)]
+    L.refckpt_runtime_capture.argtypes = [C.c_void_p, C.c_void_p, _sz, _sz, C.c_uint32, C.c_uint32, C.c_void_p,
+                                          C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_char_p]
+    L.refckpt_runtime_resume.argtypes = [C.c_char_p, C.c_void_p, _sz, C.c_void_p, _sz, C.POINTER(_sz),
+                                         C.POINTER(_sz)]
+    return L
+
+
 def ref_host_policy_forward(genome: np.ndarray, solution: np.ndarray, guesses: np.ndarray) -> np.ndarray | None:
     guesses = np.ascontiguousarray(np.asarray(guesses, np.uint8).reshape(-1, 5))
     out = np.zeros(64, np.float32)

@@ -1,0 +1,231 @@
+// Test infrastructure only: the reference's runtime-checkpoint code (genetic_algorithm/device/slab_runtime.cu)
+// and its device runtime, compiled from the reference's own sources where they lie, behind a small C ABI for the
+// parity tests. Built by oracle/build.py into oracle/_ref/libref_ckpt.so; nothing from the reference is copied.
+//
+// Host-only entry points (no GPU needed):
+//   refckpt_roundtrip      TryReadRuntimeCheckpoint then TryWriteRuntimeCheckpointAtomically
+//   refckpt_write_synthetic a RuntimeCheckpoint of seeded content (padding bytes of the padded records set to 0xA5)
+//                          sealed with ComputeRuntimeCheckpointChecksum and written by the reference writer
+//   refckpt_identity_hash  the training-data identity hash, mixed by the reference's helpers in the order
+//                          TryDownloadBoundaryCheckpointPayload uses (slab_runtime.cu:1283-1297)
+// Device entry points (drive the reference's whole runtime on the GPU):
+//   refckpt_runtime_capture create, bootstrap, TryCreatePrebreedingCheckpointOnDevice, write
+//   refckpt_runtime_resume  read, TryRestorePrebreedingCheckpointToDevice, TryResumeGenerationFromCheckpointOnDevice,
+//                          then the new generation's genomes in individual order
+#include "genetic_algorithm/device/slab_runtime.cu"
+#include "genetic_algorithm/genotype_slab/device_runtime.cu"
+#include "genetic_algorithm/genotype_slab/slab_allocator.cpp"
+#include "training_folder/training_data.cu"
+
+#include <cstring>
+#include <random>
+
+namespace {
+
+namespace sd = neuroevolution::genetic_algorithm::slab_device;
+namespace ga = neuroevolution::genetic_algorithm;
+namespace tf = neuroevolution::training_folder;
+namespace gs = neuroevolution::genetic_algorithm::genotype_slab;
+
+bool MakeCatalog(const std::uint8_t *letters, std::size_t count, tf::TrainingWordCatalog &catalog) {
+    catalog = {};
+    if (letters == nullptr || count == 0 || count > tf::kTrainingWordCatalogCapacity) {
+        return false;
+    }
+    for (std::size_t w = 0; w < count; ++w) {
+        for (std::size_t p = 0; p < 5; ++p) {
+            catalog.words[w].letter_indices[p] = letters[w * 5 + p];
+        }
+    }
+    catalog.word_count = count;
+    return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+// The reference's reader keeps reading after a failed check and can then size an allocation from misaligned
+// bytes, which throws; a throw counts as a rejection here.
+int refckpt_roundtrip(const char *in, const char *out) {
+    try {
+        sd::RuntimeCheckpoint c{};
+        if (!sd::TryReadRuntimeCheckpoint(in, c)) {
+            return 0;
+        }
+        return sd::TryWriteRuntimeCheckpointAtomically(c, out) ? 1 : 0;
+    } catch (...) {
+        return 0;
+    }
+}
+
+int refckpt_write_synthetic(const char *path, std::uint32_t seed, std::size_t individuals, std::size_t children,
+                            std::size_t action_count, std::size_t releases, int injection) {
+    std::mt19937_64 rng(seed);
+    const auto u = [&](std::uint64_t bound) { return static_cast<std::size_t>(rng() % bound); };
+    sd::RuntimeCheckpoint c{};
+    c.training_data_identity_hash = rng();
+    c.generation_seed = static_cast<std::uint32_t>(rng());
+    c.runtime_word_counts.training_word_count = u(5000);
+    c.runtime_word_counts.action_space_word_count = u(5000);
+    c.runtime_word_counts.training_word_schedule.initial_word_count = u(100);
+    c.runtime_word_counts.training_word_schedule.word_count_step = u(100);
+    c.runtime_word_counts.training_word_schedule.word_count_step_period_generations = u(100);
+    c.runtime_word_counts.shard_initial_radius = u(10);
+    c.runtime_word_counts.shard_radius_growth_period_generations = u(10);
+    c.training_shard_release_history.release_count = releases;
+    for (std::size_t i = 0; i < releases; ++i) {
+        c.training_shard_release_history.release_generations[i] = u(1000);
+        c.training_shard_release_history.release_fitness_p99[i] = static_cast<float>(u(1000)) / 1000.0f;
+    }
+    // padded records: non-zero padding, which the format carries as stored
+    std::memset(static_cast<void *>(&c.assembly_config), 0xA5, sizeof(c.assembly_config));
+    c.assembly_config.parent_selection.cellular_breeding_radius = 1 + u(3);
+    c.assembly_config.parent_selection.rank_exponent = 0.5f;
+    c.assembly_config.breeding.crossover_temperature_level1 = 0.02f;
+    c.assembly_config.breeding.crossover_temperature_level2 = 0.01f;
+    c.assembly_config.breeding.crossover_temperature_level3 = 0.005f;
+    c.assembly_config.mutation.mutation_probability = 0.001f;
+    c.assembly_config.mutation.mutation_sigma = 0.02f;
+    c.assembly_config.mutation.output_tail_row_scale_mutation_probability = 0.0f;
+    std::memset(static_cast<void *>(&c.pending_output_embedding_injection), 0xA5,
+                sizeof(c.pending_output_embedding_injection));
+    c.pending_output_embedding_injection.enabled = injection != 0;
+    c.pending_output_embedding_injection.first_catalog_word_index = injection != 0 ? action_count - 3 : 0;
+    c.pending_output_embedding_injection.injection_count = injection != 0 ? 3 : 0;
+    const std::size_t stride = gs::ComputeSlabSlotStrideBytes(action_count);
+    c.slab_layout.action_count = action_count;
+    c.slab_layout.slot_stride_bytes = stride;
+    c.slab_layout.slot_count = 2 * individuals;
+    c.slab_layout.slab_bytes = 2 * individuals * stride;
+    c.runtime_config.genotype_slab_byte_budget_bytes = c.slab_layout.slab_bytes;
+    c.runtime_config.generation_byte_budget_bytes = individuals * stride;
+    c.runtime_config.action_count = action_count;
+    c.runtime_config.population_size_ceiling = individuals;
+    c.runtime_config.grid_column_count = 4;
+    c.current_grid_shape = {individuals / 4, 4, individuals};
+    c.next_grid_shape = {children / 4, 4, children};
+    c.epicenter_grid_shape = {individuals / 4, 4, individuals};
+    if (!gs::TryCreateSlabGeneration(c.current_generation, individuals, u(50)) ||
+        !gs::TryCreateSlabAssemblyPlan(c.assembly_plan, children)) {
+        return 0;
+    }
+    for (std::size_t i = 0; i < individuals; ++i) {
+        const bool live = u(4) != 0;
+        c.current_generation.slot_indices[i] = live ? static_cast<std::uint32_t>(i) : gs::kInvalidSlabSlotIndex;
+        c.current_generation.fitness[i] = static_cast<float>(u(100000)) / 100000.0f;
+        c.current_generation.evaluation_counts[i] = static_cast<std::uint32_t>(u(40));
+        c.current_generation.has_fitness[i] = static_cast<std::uint8_t>(u(2));
+        if (live) {
+            sd::RuntimeCheckpointGenotypeRecord record{};
+            record.organism_index = static_cast<std::uint32_t>(i);
+            record.genome_bytes.resize(stride);
+            for (std::size_t b = 0; b < stride; ++b) {
+                record.genome_bytes[b] = static_cast<std::uint8_t>(rng());
+            }
+            c.live_genotypes.push_back(std::move(record));
+        }
+    }
+    for (std::size_t k = 0; k < children; ++k) {
+        c.assembly_plan.parent_pairs[k].first_parent_index = static_cast<std::uint32_t>(u(individuals));
+        c.assembly_plan.parent_pairs[k].second_parent_index = static_cast<std::uint32_t>(u(individuals));
+    }
+    c.checksum = sd::ComputeRuntimeCheckpointChecksum(c);
+    return sd::TryWriteRuntimeCheckpointAtomically(c, path) ? 1 : 0;
+}
+
+std::uint64_t refckpt_identity_hash(const void *counts, const void *history, const std::uint8_t *letters,
+                                    std::size_t count) {
+    std::uint64_t hash = 1469598103934665603ULL;
+    sd::MixCheckpointBytes(hash, counts, sizeof(sd::RuntimeWordCounts));
+    if (history != nullptr) {
+        sd::MixTrainingShardReleaseHistory(hash, *static_cast<const tf::TrainingDataShardReleaseHistory *>(history));
+    }
+    if (letters != nullptr) {
+        static tf::TrainingWordCatalog catalog{};
+        if (!MakeCatalog(letters, count, catalog)) {
+            return 0;
+        }
+        sd::MixCheckpointValue(hash, catalog.word_count);
+        for (std::size_t w = 0; w < catalog.word_count; ++w) {
+            sd::MixCheckpointBytes(hash, &catalog.words[w], sizeof(catalog.words[w]));
+        }
+    }
+    return hash;
+}
+
+// Records the POD layouts the C ABI relies on.
+int refckpt_layouts(std::size_t *out) {
+    out[0] = sizeof(sd::RuntimeWordCounts);
+    out[1] = sizeof(tf::TrainingDataShardReleaseHistory);
+    out[2] = sizeof(ga::GenerationAssemblyConfig);
+    out[3] = sizeof(sd::PendingOutputEmbeddingInjection);
+    out[4] = sizeof(sd::DeviceSlabGARuntimeConfig);
+    out[5] = sizeof(gs::GenotypeSlabLayout);
+    out[6] = sizeof(neuroevolution::spatial::CellularGridShape);
+    out[7] = sizeof(neuroevolution::wordle::Word);
+    return 8;
+}
+
+int refckpt_runtime_capture(const void *config, const std::uint8_t *letters, std::size_t catalog_count,
+                            std::size_t generation_size, std::uint32_t bootstrap_seed, std::uint32_t generation_seed,
+                            const void *counts, const void *assembly, const void *pending, const void *history,
+                            int hash_catalog, const char *path) {
+    tf::TrainingWordCatalog *catalog = new tf::TrainingWordCatalog{};
+    if (!MakeCatalog(letters, catalog_count, *catalog) || !tf::UploadTrainingWordCatalogToDeviceConstantMemory(*catalog)) {
+        delete catalog;
+        return 0;
+    }
+    sd::DeviceSlabGARuntimeBuffers buffers{};
+    sd::RuntimeCheckpoint checkpoint{};
+    const auto *h = static_cast<const tf::TrainingDataShardReleaseHistory *>(history);
+    bool ok = sd::TryCreateDeviceSlabGARuntimeBuffers(buffers, *static_cast<const sd::DeviceSlabGARuntimeConfig *>(config)) &&
+              sd::TryBootstrapRandomCurrentGenerationOnDevice(buffers, generation_size, bootstrap_seed, 0) &&
+              sd::TryCreatePrebreedingCheckpointOnDevice(
+                  buffers, generation_seed, *static_cast<const sd::RuntimeWordCounts *>(counts),
+                  *static_cast<const ga::GenerationAssemblyConfig *>(assembly),
+                  *static_cast<const sd::PendingOutputEmbeddingInjection *>(pending), checkpoint,
+                  hash_catalog != 0 ? catalog : nullptr, false, {}, {}, h) &&
+              sd::TryWriteRuntimeCheckpointAtomically(checkpoint, path);
+    sd::DestroyDeviceSlabGARuntimeBuffers(buffers);
+    delete catalog;
+    return ok ? 1 : 0;
+}
+
+int refckpt_runtime_resume(const char *path, const std::uint8_t *letters, std::size_t catalog_count,
+                           std::uint8_t *genomes, std::size_t capacity_bytes, std::size_t *count_out,
+                           std::size_t *stride_out) {
+    tf::TrainingWordCatalog *catalog = new tf::TrainingWordCatalog{};
+    const bool have_catalog =
+        MakeCatalog(letters, catalog_count, *catalog) && tf::UploadTrainingWordCatalogToDeviceConstantMemory(*catalog);
+    delete catalog;
+    if (!have_catalog) {
+        return 0;
+    }
+    sd::RuntimeCheckpoint checkpoint{};
+    sd::DeviceSlabGARuntimeBuffers buffers{};
+    gs::SlabGeneration generation{};
+    bool ok = sd::TryReadRuntimeCheckpoint(path, checkpoint) &&
+              sd::TryRestorePrebreedingCheckpointToDevice(checkpoint, buffers) &&
+              sd::TryResumeGenerationFromCheckpointOnDevice(buffers, checkpoint, false) &&
+              sd::TryDownloadCurrentGenerationFromDevice(buffers, generation);
+    std::size_t stride = 0;
+    if (ok) {
+        stride = buffers.genotype_slab.slab_layout.slot_stride_bytes;
+        ok = generation.active_individual_count * stride <= capacity_bytes;
+    }
+    for (std::size_t i = 0; ok && i < generation.active_individual_count; ++i) {
+        std::unique_ptr<std::uint8_t[]> bytes;
+        std::size_t n = 0;
+        ok = sd::TryDownloadSlabSlotBytesFromDevice(buffers, generation.slot_indices[i], bytes, n) && n == stride;
+        if (ok) {
+            std::memcpy(genomes + i * stride, bytes.get(), stride);
+        }
+    }
+    *count_out = ok ? generation.active_individual_count : 0;
+    *stride_out = stride;
+    sd::DestroyDeviceSlabGARuntimeBuffers(buffers);
+    return ok ? 1 : 0;
+}
+
+}  // extern "C"
