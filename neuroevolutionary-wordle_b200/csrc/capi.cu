@@ -459,7 +459,8 @@ int EvaluateImpl(nwg_runtime *rt, const nwg_runtime_word_counts *counts, const n
     p.trace_turns = static_cast<std::int32_t *>(turns);
     p.trace_scores = static_cast<float *>(scores);
     p.trace_policy = static_cast<float *>(policy);
-    if (rt->form == NWG_FORM_FP32) {
+    // at <= 128 selectable actions every form scores on the reference's tensor-tile path, in the plain kernel
+    if (rt->form == NWG_FORM_FP32 || selectable <= 128) {
         NWG_TRY(cudaEventRecord(rt->eval_begin, rt->stream));
         NWG_TRY(LaunchEvalFp32(p, rt->scratch_ctas, rt->stream));
         NWG_TRY(cudaEventRecord(rt->eval_end, rt->stream));

@@ -9,6 +9,7 @@
 //   trunk layer 1            cached accumulator per game, extended by the new turn's 64 inputs
 //   trunk layers 2, 3        256 -> 128 ReLU -> 64
 //   scoring + argmax         policy (128 x 64) x catalog embeddings (64 x A), fused masked argmax
+//                            (at <= 128 selectable actions: the reference's FP16 tensor-tile scoring instead)
 //
 // Bit-exactness with the reference's device arithmetic: each output is the same chain of fused
 // multiply-adds in the same input order as the reference's `sum += w * x` loops (bias first, inputs
@@ -18,6 +19,9 @@
 // its 64 inputs to the end of the chain). Ties in the argmax go to the lowest action index, and
 // guessed words are masked by word equality, as in the reference.
 #include <cuda_fp16.h>
+#include <mma.h>
+
+#include <cstdint>
 
 #include "eval_common.cuh"
 
@@ -155,6 +159,92 @@ __device__ __forceinline__ void ScoreFp32(const EvalParams &p, ChunkState &st, c
 
 }
 
+// Action spaces of at most kSmallActionSpace selectable actions, where the reference scores with its tensor-tile
+// path (slab_runtime.cu:70 and :1126-1140; evaluation_ops.cuh:286-388): the policy vector rounded to FP16, the
+// fixed features rounded to FP16 (small integers, exact) and the FP16 tail form a 64-deep product, accumulated in
+// FP32 by a 16x16x16 FP16 tensor-core MMA over the depth chunks [0,16), [16,32), [32,48), [48,64) in that order,
+// from a zero accumulator. Each score depends only on its own policy row and action column, so the same MMA over
+// this chunk's 128 games x 128 actions gives the reference's scores bit for bit; the argmax walks the actions in
+// ascending order with ties to the lowest index, as the reference's lane-0 scan does.
+constexpr int kSmallActionSpace = 128;
+constexpr int kSmallALd = 72;   // halfs per policy row (64 + 8)
+constexpr int kSmallBLd = 136;  // halfs per feature row of the action tile (128 + 8)
+constexpr int kSmallCLd = 20;   // floats per row of a warp's 16 x 16 score tile
+
+__device__ __forceinline__ void ScoreSmallActionSpace(const EvalParams &p, ChunkState &st, const __half *gh,
+                                                      float *arena, int t) {
+    namespace wmma = nvcuda::wmma;
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5;
+    const int lane = tid & 31;
+    const int actions = static_cast<int>(p.action_count);
+    const float *pv = arena;  // [64][kLd] policy vectors, feature-major
+    // MMA operands must start on 32-byte boundaries: align the base up to 128 bytes (the buffers below end
+    // 21,504 bytes before the arena does)
+    const std::uintptr_t free_base = reinterpret_cast<std::uintptr_t>(arena + kTile);
+    __half *ah = reinterpret_cast<__half *>((free_base + 127u) & ~static_cast<std::uintptr_t>(127u));  // [128][72]
+    __half *bh = ah + kChunkGames * kSmallALd;               // [64 features][kSmallBLd]
+    float *cw = reinterpret_cast<float *>(bh + 64 * kSmallBLd) + warp * 16 * kSmallCLd;
+    const __half *tail = reinterpret_cast<const __half *>(reinterpret_cast<const std::uint8_t *>(gh) +
+                                                          kTailOffsetBytes);
+    for (int idx = tid; idx < kChunkGames * 64; idx += kEvalThreads) {
+        const int g = idx >> 6;
+        const int k = idx & 63;
+        ah[g * kSmallALd + k] = __float2half_rn(pv[k * kLd + g]);
+    }
+    for (int idx = tid; idx < 64 * kSmallActionSpace; idx += kEvalThreads) {
+        const int k = idx >> 7;
+        const int a = idx & 127;
+        __half v = __float2half_rn(0.0f);
+        if (a < actions) {
+            v = k < kFixedDim ? __float2half_rn(p.fixed_t[static_cast<std::size_t>(k) * p.action_pad + a])
+                              : tail[static_cast<std::size_t>(a) * kTailDim + (k - kFixedDim)];
+        }
+        bh[k * kSmallBLd + a] = v;
+    }
+    if (tid < kSmallActionSpace) {
+        st.tile_codes[0][tid] = tid < actions ? p.codes[tid] : 0u;
+    }
+    __syncthreads();
+    // warp w: games 16w .. 16w+15; lanes 0..15 keep one game's running best
+    const int g = warp * 16 + (lane & 15);
+    float best_s = 0.0f;
+    int best_i = -1;
+    wmma::fragment<wmma::matrix_a, 16, 16, 16, __half, wmma::row_major> fa;
+    wmma::fragment<wmma::matrix_b, 16, 16, 16, __half, wmma::row_major> fb;
+    wmma::fragment<wmma::accumulator, 16, 16, 16, float> fc;
+    for (int a0 = 0; a0 < actions; a0 += 16) {
+        wmma::fill_fragment(fc, 0.0f);
+#pragma unroll
+        for (int k0 = 0; k0 < 64; k0 += 16) {
+            wmma::load_matrix_sync(fa, ah + warp * 16 * kSmallALd + k0, kSmallALd);
+            wmma::load_matrix_sync(fb, bh + k0 * kSmallBLd + a0, kSmallBLd);
+            wmma::mma_sync(fc, fa, fb, fc);
+        }
+        wmma::store_matrix_sync(cw, fc, kSmallCLd, wmma::mem_row_major);
+        __syncwarp();
+        if (lane < 16) {
+            for (int c = 0; c < 16 && a0 + c < actions; ++c) {
+                const std::uint32_t code = st.tile_codes[0][a0 + c];
+                bool masked = false;
+                for (int u = 0; u < t; ++u) {
+                    masked |= st.guess[u][g] == code;
+                }
+                const float s = cw[(lane & 15) * kSmallCLd + c];
+                if (!masked && (best_i < 0 || s > best_s)) {
+                    best_s = s;
+                    best_i = a0 + c;
+                }
+            }
+        }
+        __syncwarp();
+    }
+    if (lane < 16) {
+        st.best[g] = best_i;
+    }
+    __syncthreads();
+}
+
 __global__ void __launch_bounds__(kEvalThreads, 2) EvalFp32Kernel(const EvalParams p) {
     extern __shared__ __align__(16) float arena[];
     __shared__ ChunkState st;
@@ -187,7 +277,11 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalFp32Kernel(const EvalPara
                 encoded += tid == 0 ? static_cast<unsigned long long>(st.active) : 0ull;
             }
             TrunkForward(p, st, gh, arena, scratch, t, step, ind);
-            ScoreFp32(p, st, gh, arena, t);
+            if (p.action_count <= static_cast<std::uint32_t>(kSmallActionSpace)) {
+                ScoreSmallActionSpace(p, st, gh, arena, t);
+            } else {
+                ScoreFp32(p, st, gh, arena, t);
+            }
             AppendGuesses(p, st, step, decisions);
         }
         FinishChunk(p, st, ind, episodes);

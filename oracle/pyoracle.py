@@ -289,8 +289,10 @@ def ref_ckpt() -> C.CDLL | None:
     L.refckpt_identity_hash.restype = C.c_uint64
     L.refckpt_identity_hash.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, _sz]
     L.refckpt_layouts.argtypes = [C.POINTER(_sz)]
-    L.refckpt_runtime_capture.argtypes = [C.c_void_p, C.c_void_p, _sz, _sz, C.c_uint32, C.c_uint32, C.c_void_p,
+    L.refckpt_runtime_capture.argtypes = [C.c_void_p, C.c_void_p, _sz, _sz, C.c_uint32, _sz, C.c_uint32, C.c_void_p,
                                           C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_char_p]
+    L.refckpt_runtime_evaluate.argtypes = [C.c_void_p, C.c_void_p, _sz, _sz, C.c_uint32, _sz, C.c_void_p, C.c_void_p,
+                                           C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     L.refckpt_runtime_resume.argtypes = [C.c_char_p, C.c_void_p, _sz, C.c_void_p, _sz, C.POINTER(_sz),
                                          C.POINTER(_sz)]
     return L

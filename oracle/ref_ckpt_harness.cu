@@ -10,6 +10,7 @@
 //                          TryDownloadBoundaryCheckpointPayload uses (slab_runtime.cu:1283-1297)
 // Device entry points (drive the reference's whole runtime on the GPU):
 //   refckpt_runtime_capture create, bootstrap, TryCreatePrebreedingCheckpointOnDevice, write
+//   refckpt_runtime_evaluate create, bootstrap, TryEvaluateCurrentGenerationFitnessOnDevice, fitness arrays
 //   refckpt_runtime_resume  read, TryRestorePrebreedingCheckpointToDevice, TryResumeGenerationFromCheckpointOnDevice,
 //                          then the new generation's genomes in individual order
 #include "genetic_algorithm/device/slab_runtime.cu"
@@ -168,7 +169,8 @@ int refckpt_layouts(std::size_t *out) {
 }
 
 int refckpt_runtime_capture(const void *config, const std::uint8_t *letters, std::size_t catalog_count,
-                            std::size_t generation_size, std::uint32_t bootstrap_seed, std::uint32_t generation_seed,
+                            std::size_t generation_size, std::uint32_t bootstrap_seed, std::size_t generation_index,
+                            std::uint32_t generation_seed,
                             const void *counts, const void *assembly, const void *pending, const void *history,
                             int hash_catalog, const char *path) {
     tf::TrainingWordCatalog *catalog = new tf::TrainingWordCatalog{};
@@ -180,7 +182,7 @@ int refckpt_runtime_capture(const void *config, const std::uint8_t *letters, std
     sd::RuntimeCheckpoint checkpoint{};
     const auto *h = static_cast<const tf::TrainingDataShardReleaseHistory *>(history);
     bool ok = sd::TryCreateDeviceSlabGARuntimeBuffers(buffers, *static_cast<const sd::DeviceSlabGARuntimeConfig *>(config)) &&
-              sd::TryBootstrapRandomCurrentGenerationOnDevice(buffers, generation_size, bootstrap_seed, 0) &&
+              sd::TryBootstrapRandomCurrentGenerationOnDevice(buffers, generation_size, bootstrap_seed, generation_index) &&
               sd::TryCreatePrebreedingCheckpointOnDevice(
                   buffers, generation_seed, *static_cast<const sd::RuntimeWordCounts *>(counts),
                   *static_cast<const ga::GenerationAssemblyConfig *>(assembly),
@@ -189,6 +191,41 @@ int refckpt_runtime_capture(const void *config, const std::uint8_t *letters, std
               sd::TryWriteRuntimeCheckpointAtomically(checkpoint, path);
     sd::DestroyDeviceSlabGARuntimeBuffers(buffers);
     delete catalog;
+    return ok ? 1 : 0;
+}
+
+// TryCreateDeviceSlabGARuntimeBuffers, TryBootstrapRandomCurrentGenerationOnDevice,
+// TryEvaluateCurrentGenerationFitnessOnDevice, then the generation's fitness arrays and the summary.
+int refckpt_runtime_evaluate(const void *config, const std::uint8_t *letters, std::size_t catalog_count,
+                             std::size_t generation_size, std::uint32_t bootstrap_seed, std::size_t generation_index,
+                             const void *counts, const void *history, float *fitness, std::uint32_t *evaluation_counts,
+                             std::uint8_t *has_fitness, void *summary) {
+    tf::TrainingWordCatalog *catalog = new tf::TrainingWordCatalog{};
+    const bool have_catalog =
+        MakeCatalog(letters, catalog_count, *catalog) && tf::UploadTrainingWordCatalogToDeviceConstantMemory(*catalog);
+    delete catalog;
+    if (!have_catalog) {
+        return 0;
+    }
+    sd::DeviceSlabGARuntimeBuffers buffers{};
+    gs::SlabGeneration generation{};
+    sd::PopulationFitnessSummary s{};
+    bool ok = sd::TryCreateDeviceSlabGARuntimeBuffers(buffers, *static_cast<const sd::DeviceSlabGARuntimeConfig *>(config)) &&
+              sd::TryBootstrapRandomCurrentGenerationOnDevice(buffers, generation_size, bootstrap_seed, generation_index) &&
+              sd::TryEvaluateCurrentGenerationFitnessOnDevice(
+                  buffers, *static_cast<const sd::RuntimeWordCounts *>(counts),
+                  static_cast<const tf::TrainingDataShardReleaseHistory *>(history)) &&
+              sd::TryDownloadCurrentGenerationFromDevice(buffers, generation) &&
+              sd::TryReadPopulationFitnessSummaryFromDevice(buffers, s);
+    for (std::size_t i = 0; ok && i < generation.active_individual_count; ++i) {
+        fitness[i] = generation.fitness[i];
+        evaluation_counts[i] = generation.evaluation_counts[i];
+        has_fitness[i] = generation.has_fitness[i];
+    }
+    if (ok) {
+        std::memcpy(summary, &s, sizeof(s));
+    }
+    sd::DestroyDeviceSlabGARuntimeBuffers(buffers);
     return ok ? 1 : 0;
 }
 

@@ -83,7 +83,8 @@ def test_checkpoint_matches_reference_and_every_resume_agrees(tmp_path, name):
     rc.generation_byte_budget_bytes = pop * stride
     rc.action_count, rc.population_size_ceiling, rc.grid_column_count = a, pop, cols
     assert O.ref_ckpt().refckpt_runtime_capture(C.addressof(rc), catalog.ctypes.data, len(catalog), pop,
-                                                k["boot_seed"], k["seed"], C.addressof(counts), C.addressof(cfg),
+                                                k["boot_seed"], k["boot_index"], k["seed"], C.addressof(counts),
+                                                C.addressof(cfg),
                                                 C.addressof(pending), None, 1, str(ref_path).encode()) == 1
     ref = capi.Checkpoint.read(ref_path)
 

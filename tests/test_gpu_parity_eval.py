@@ -148,26 +148,49 @@ def test_csr_lists_match_cpu_oracle():
                               lists[i])["steps"] for i in range(population))
 
 
-def test_small_action_space_matches_oracle():
-    """At <= 128 actions the reference switches to an FP16 WMMA scorer; the FP32 form follows the FP32 oracle."""
-    action_count, columns, population = 40, 2, 2
-    rng = np.random.default_rng(11)
+@pytest.mark.skipif(O.ref_ckpt() is None, reason="reference runtime library not built")
+@pytest.mark.parametrize("action_count,training,population,columns,forms", [
+    (20, 20, 9, 3, (0, 1, 2, 3, 4)), (60, 60, 16, 4, (0, 2, 4)), (100, 40, 16, 4, (0, 3)),
+    (127, 127, 9, 3, (0,)), (128, 64, 16, 4, (0, 1, 4)), (129, 129, 9, 3, (0, 1, 2)), (300, 30, 16, 4, (0, 2))])
+def test_runtime_evaluation_matches_reference_runtime(action_count, training, population, columns, forms):
+    """The reference's whole evaluation (TryEvaluateCurrentGenerationFitnessOnDevice) against ours, on both sides of
+    its switch at 128 selectable actions (slab_runtime.cu:70, :1126-1140): FP16 tensor-tile scoring at or below it,
+    FP32 warp scoring above it. Fitness bits, evaluation counts and the summary agree; at or below 128 actions every
+    evaluation form takes the tensor-tile path."""
+    import ctypes as C
+
+    rng = np.random.default_rng(action_count * 7 + training)
     catalog = H.synthetic_words(rng, action_count)
     G.upload_catalog_everywhere(catalog)
+    capi = G.nwg.capi
+    counts = capi.word_counts(training=training, action_space=action_count)
+    stride = capi.genome_stride_bytes(action_count)
+    rc = capi.RuntimeConfig()
+    rc.genotype_slab_byte_budget_bytes = 2 * population * stride
+    rc.generation_byte_budget_bytes = population * stride
+    rc.action_count, rc.population_size_ceiling, rc.grid_column_count = action_count, population, columns
+    fit = np.zeros(population, np.float32)
+    evals = np.zeros(population, np.uint32)
+    has = np.zeros(population, np.uint8)
+    summary = capi.FitnessSummary()
+    assert O.ref_ckpt().refckpt_runtime_evaluate(C.addressof(rc), catalog.ctypes.data, len(catalog), population,
+                                                 31 + action_count, 3, C.addressof(counts), None, fit.ctypes.data,
+                                                 evals.ctypes.data, has.ctypes.data, C.addressof(summary)) == 1
     rt = G.nwg.Runtime(action_count, population, columns)
-    rt.bootstrap(population, seed=99)
-    lists = [np.arange(0, 8, dtype=np.uint32), np.arange(8, 20, dtype=np.uint32)]
-    offsets = np.array([0, 8, 20], np.uint32)
-    rt.set_cell_words(offsets, np.concatenate(lists))
-    counts = G.nwg.capi.word_counts(training=20, action_space=action_count)
-    oc, ot, os_, op = _run_ours(rt, counts, 36)
-    gen = rt.current_generation()
-    for i in range(population):
-        genome = rt.download_slot(int(gen["slots"][i])).view(np.uint16)
-        res = O.evaluate_individual(genome, action_count, catalog, lists[i])
-        w3 = 3 * len(lists[i])
-        assert np.array_equal(ot[i, :w3], res["turns"])
-        assert np.array_equal(os_[i, :w3], res["scores"])
+    rt.bootstrap(population, seed=31 + action_count, generation_index=3)
+    for form in forms:
+        rt.set_form(form)
+        if form >= 3:
+            rt.set_margin_guard(1.0e30)
+        rt.evaluate(counts)
+        gen = rt.current_generation()
+        assert np.array_equal(gen["fitness"].view(np.uint32), fit.view(np.uint32)), f"form {form}"
+        assert np.array_equal(gen["evaluation_counts"], evals) and np.array_equal(gen["has_fitness"], has)
+        s = rt.summary()
+        assert (s.best_fitness, s.average_fitness, s.best_index, s.generation_index, s.population_size) == (
+            summary.best_fitness, summary.average_fitness, summary.best_index, summary.generation_index,
+            summary.population_size)
+    rt.close()
 
 
 def test_evaluation_error_statuses():

@@ -59,7 +59,10 @@ def test_tensor_core_form_equals_plain_form(form, action_count, population, colu
         assert np.array_equal(tc[3][i, :w3], plain[3][i, :w3])
     assert np.array_equal(tc[4], plain[4])
     assert tc[5].game_steps == plain[5].game_steps
-    assert tc[5].rescored_chunks > 0
+    if action_count > 128:
+        assert tc[5].rescored_chunks > 0
+    else:  # at <= 128 actions every form scores on the reference's tensor-tile path, in the plain kernel
+        assert tc[5].rescored_chunks == 0
     rt.close()
 
 

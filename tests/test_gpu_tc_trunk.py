@@ -84,7 +84,8 @@ def test_exact_path_equals_plain_form(form, action_count, population, columns, s
         assert np.array_equal(tc[3][i, :w3].view(np.uint32), plain[3][i, :w3].view(np.uint32))
     assert np.array_equal(tc[4], plain[4])
     assert tc[5].game_steps == plain[5].game_steps
-    assert tc[5].fallback_steps == tc[5].game_steps
+    # at <= 128 actions every form scores on the reference's tensor-tile path, in the plain kernel
+    assert tc[5].fallback_steps == (tc[5].game_steps if action_count > 128 else 0)
     rt.close()
 
 
