@@ -328,6 +328,38 @@ uint64_t nwg_checkpoint_checksum(const nwg_checkpoint *checkpoint);
 uint64_t nwg_checkpoint_identity_hash(const nwg_runtime_word_counts *counts, const nwg_shard_release_history *history,
                                       const uint8_t *catalog_letters, size_t catalog_count);
 
+/* WinnerArtifactMetadata (model_artifact/winner_artifact.hpp:12-21) without its path member, which the artefact
+ * calls take as a string. */
+typedef struct {
+    float best_fitness;
+    size_t generation_index;
+    size_t best_index;
+    uint32_t best_slot_index;
+    size_t action_count;
+    size_t genome_byte_count;
+    uint32_t seed;
+} nwg_winner_metadata;
+
+/* TryWriteWinnerArtifactToPaths (model_artifact/winner_artifact.hpp:33-36): genome_byte_count bytes of the genome
+ * image to binary_path and the reference's JSON metadata (format_version 2, the first action_count catalog words)
+ * to metadata_path, each through path.tmp and a rename. timestamp_local NULL = now, local time. */
+int nwg_winner_artifact_write(const char *binary_path, const char *metadata_path, const uint8_t *genome_bytes,
+                              const nwg_winner_metadata *metadata, const uint8_t *catalog_letters,
+                              size_t catalog_count, const char *action_space_path, const char *timestamp_local);
+
+/* TryPersistWinningGenome (cli/run_genetic_algorithm.cu:1519-1532): the last evaluation's best individual (its
+ * summary and slot image) written as a winner artefact. */
+int nwg_winner_artifact_persist(const nwg_runtime *runtime, uint32_t seed, const uint8_t *catalog_letters,
+                                size_t catalog_count, const char *action_space_path, const char *binary_path,
+                                const char *metadata_path, const char *timestamp_local);
+
+/* TryReadWinnerArtifact (model_artifact/winner_artifact_reader.hpp:20-21). Any output but metadata may be NULL;
+ * catalog_letters holds up to NWG_CATALOG_CAPACITY rows of 5 letter indices. */
+int nwg_winner_artifact_read(const char *binary_path, const char *metadata_path, nwg_winner_metadata *metadata,
+                             uint8_t *genome_bytes, size_t genome_capacity, uint8_t *catalog_letters,
+                             size_t *catalog_count, char *action_space_path, size_t path_capacity,
+                             char *timestamp_local, size_t timestamp_capacity);
+
 /* SwapDeviceSlabGenerationBuffers (slab_runtime.hpp:181). */
 int nwg_swap_generations(nwg_runtime *runtime);
 

@@ -112,6 +112,13 @@ class CheckpointRecord(C.Structure):
                 ("live_genomes", _vp)]
 
 
+class WinnerMetadata(C.Structure):
+    """nwg_winner_metadata: WinnerArtifactMetadata (model_artifact/winner_artifact.hpp:12-21) minus its path."""
+    _fields_ = [("best_fitness", C.c_float), ("generation_index", _sz), ("best_index", _sz),
+                ("best_slot_index", C.c_uint32), ("action_count", _sz), ("genome_byte_count", _sz),
+                ("seed", C.c_uint32)]
+
+
 POST_FITNESS_FN = C.CFUNCTYPE(C.c_bool, _vp, C.POINTER(RuntimeWordCounts), _vp)
 SHARD_RELEASE_FN = C.CFUNCTYPE(C.c_bool, _vp, C.POINTER(RuntimeWordCounts), C.POINTER(PendingInjection), _vp)
 
@@ -124,7 +131,8 @@ EXPORTS = [
     "nwg_breed_device", "nwg_bootstrap_device", "nwg_evaluate_noalloc", "nwg_prepare_generation",
     "nwg_assemble_prepared", "nwg_checkpoint_capture", "nwg_checkpoint_restore", "nwg_checkpoint_resume",
     "nwg_checkpoint_write", "nwg_checkpoint_read", "nwg_checkpoint_free", "nwg_checkpoint_checksum",
-    "nwg_checkpoint_identity_hash",
+    "nwg_checkpoint_identity_hash", "nwg_winner_artifact_write", "nwg_winner_artifact_persist",
+    "nwg_winner_artifact_read",
 ]
 
 
@@ -165,6 +173,12 @@ def lib() -> C.CDLL:
     L.nwg_checkpoint_identity_hash.argtypes = [C.POINTER(RuntimeWordCounts), C.POINTER(ShardReleaseHistory), _vp,
                                                _sz]
     L.nwg_checkpoint_identity_hash.restype = C.c_uint64
+    L.nwg_winner_artifact_write.argtypes = [C.c_char_p, C.c_char_p, _vp, C.POINTER(WinnerMetadata), _vp, _sz,
+                                            C.c_char_p, C.c_char_p]
+    L.nwg_winner_artifact_persist.argtypes = [_vp, C.c_uint32, _vp, _sz, C.c_char_p, C.c_char_p, C.c_char_p,
+                                              C.c_char_p]
+    L.nwg_winner_artifact_read.argtypes = [C.c_char_p, C.c_char_p, C.POINTER(WinnerMetadata), _vp, _sz, _vp,
+                                           C.POINTER(_sz), C.c_char_p, _sz, C.c_char_p, _sz]
     L.nwg_swap_generations.argtypes = [_vp]
     L.nwg_read_status.argtypes = [_vp, C.POINTER(C.c_int)]
     L.nwg_download_current_generation.argtypes = [_vp, _vp, _vp, _vp, _vp, _sz, C.POINTER(_sz), C.POINTER(_sz)]
@@ -348,6 +362,15 @@ class Runtime:
         check(lib().nwg_prepare_generation(*self._boundary_args(seed, counts, config, pending, post_fitness,
                                                                 shard_release, history)), "nwg_prepare_generation")
 
+    def persist_winner(self, binary_path, metadata_path, seed: int, catalog: np.ndarray, action_space_path="",
+                       timestamp: str | None = None) -> None:
+        """TryPersistWinningGenome: the last evaluation's best individual as a winner artefact."""
+        cat = np.ascontiguousarray(catalog, np.uint8)
+        check(lib().nwg_winner_artifact_persist(self.handle, seed, _np_ptr(cat), len(cat), str(action_space_path).encode(),
+                                                str(binary_path).encode(), str(metadata_path).encode(),
+                                                timestamp.encode() if timestamp is not None else None),
+              "nwg_winner_artifact_persist")
+
     def resume(self) -> None:
         """TryResumeGenerationFromCheckpointOnDevice: assemble a restored boundary."""
         check(lib().nwg_checkpoint_resume(self.handle), "nwg_checkpoint_resume")
@@ -495,4 +518,31 @@ def identity_hash(counts: RuntimeWordCounts, history: ShardReleaseHistory | None
     cat = None if catalog is None else np.ascontiguousarray(catalog, np.uint8)
     return lib().nwg_checkpoint_identity_hash(C.byref(counts), C.byref(history) if history else None, _np_ptr(cat),
                                               0 if cat is None else len(cat))
+
+
+def write_winner_artifact(binary_path, metadata_path, genome: np.ndarray, metadata: WinnerMetadata,
+                          catalog: np.ndarray, action_space_path="", timestamp: str | None = None) -> None:
+    g = np.ascontiguousarray(genome).view(np.uint8)
+    cat = np.ascontiguousarray(catalog, np.uint8)
+    check(lib().nwg_winner_artifact_write(str(binary_path).encode(), str(metadata_path).encode(), _np_ptr(g),
+                                          C.byref(metadata), _np_ptr(cat), len(cat), str(action_space_path).encode(),
+                                          timestamp.encode() if timestamp is not None else None),
+          "nwg_winner_artifact_write")
+
+
+def read_winner_artifact(binary_path, metadata_path) -> dict:
+    """TryReadWinnerArtifact: metadata, genome image, action-space words, path and timestamp."""
+    m = WinnerMetadata()
+    check(lib().nwg_winner_artifact_read(str(binary_path).encode(), str(metadata_path).encode(), C.byref(m), None, 0,
+                                         None, None, None, 0, None, 0), "nwg_winner_artifact_read")
+    genome = np.zeros(m.genome_byte_count, np.uint8)
+    letters = np.zeros((CATALOG_CAPACITY, 5), np.uint8)
+    count = _sz()
+    path = C.create_string_buffer(4096)
+    stamp = C.create_string_buffer(64)
+    check(lib().nwg_winner_artifact_read(str(binary_path).encode(), str(metadata_path).encode(), C.byref(m),
+                                         _np_ptr(genome), genome.nbytes, _np_ptr(letters), C.byref(count), path,
+                                         len(path), stamp, len(stamp)), "nwg_winner_artifact_read")
+    return dict(metadata=m, genome=genome, words=letters[:count.value].copy(), action_space_path=path.value.decode(),
+                timestamp=stamp.value.decode())
 

@@ -293,6 +293,9 @@ def ref_ckpt() -> C.CDLL | None:
                                           C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_char_p]
     L.refckpt_runtime_evaluate.argtypes = [C.c_void_p, C.c_void_p, _sz, _sz, C.c_uint32, _sz, C.c_void_p, C.c_void_p,
                                            C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.refart_write.argtypes = [C.c_char_p, C.c_char_p, C.c_void_p, C.c_void_p, _sz, C.c_void_p, C.c_char_p]
+    L.refart_read.argtypes = [C.c_char_p, C.c_char_p, C.c_void_p, C.c_void_p, _sz, C.c_void_p, C.POINTER(_sz),
+                              C.c_char_p, _sz]
     L.refckpt_runtime_resume.argtypes = [C.c_char_p, C.c_void_p, _sz, C.c_void_p, _sz, C.POINTER(_sz),
                                          C.POINTER(_sz)]
     return L

@@ -8,6 +8,7 @@
 //                          sealed with ComputeRuntimeCheckpointChecksum and written by the reference writer
 //   refckpt_identity_hash  the training-data identity hash, mixed by the reference's helpers in the order
 //                          TryDownloadBoundaryCheckpointPayload uses (slab_runtime.cu:1283-1297)
+//   refart_write / refart_read TryWriteWinnerArtifactToPaths / TryReadWinnerArtifact (model_artifact/)
 // Device entry points (drive the reference's whole runtime on the GPU):
 //   refckpt_runtime_capture create, bootstrap, TryCreatePrebreedingCheckpointOnDevice, write
 //   refckpt_runtime_evaluate create, bootstrap, TryEvaluateCurrentGenerationFitnessOnDevice, fitness arrays
@@ -17,6 +18,8 @@
 #include "genetic_algorithm/genotype_slab/device_runtime.cu"
 #include "genetic_algorithm/genotype_slab/slab_allocator.cpp"
 #include "training_folder/training_data.cu"
+#include "model_artifact/winner_artifact.cpp"
+#include "model_artifact/winner_artifact_reader.cpp"
 
 #include <cstring>
 #include <random>
@@ -153,6 +156,72 @@ std::uint64_t refckpt_identity_hash(const void *counts, const void *history, con
         }
     }
     return hash;
+}
+
+// meta: best_fitness (float bits in u64), generation_index, best_index, best_slot_index, action_count,
+// genome_byte_count, seed
+int refart_write(const char *binary_path, const char *metadata_path, const std::uint8_t *genome,
+                 const std::uint8_t *letters, std::size_t catalog_count, const std::uint64_t *meta,
+                 const char *action_space_path) {
+    try {
+        static tf::TrainingWordCatalog catalog{};
+        if (!MakeCatalog(letters, catalog_count, catalog)) {
+            return 0;
+        }
+        neuroevolution::model_artifact::WinnerArtifactMetadata m{};
+        std::uint32_t bits = static_cast<std::uint32_t>(meta[0]);
+        std::memcpy(&m.best_fitness, &bits, 4);
+        m.generation_index = meta[1];
+        m.best_index = meta[2];
+        m.best_slot_index = static_cast<std::uint32_t>(meta[3]);
+        m.action_count = meta[4];
+        m.genome_byte_count = meta[5];
+        m.seed = static_cast<std::uint32_t>(meta[6]);
+        m.action_space_path = action_space_path;
+        neuroevolution::model_artifact::WinnerArtifactPaths paths{};
+        return neuroevolution::model_artifact::TryWriteWinnerArtifactToPaths(binary_path, metadata_path, genome,
+                                                                             catalog, m, paths)
+                   ? 1
+                   : 0;
+    } catch (...) {
+        return 0;
+    }
+}
+
+int refart_read(const char *binary_path, const char *metadata_path, std::uint64_t *meta, std::uint8_t *genome,
+                std::size_t capacity, std::uint8_t *letters, std::size_t *catalog_count, char *path_out,
+                std::size_t path_capacity) {
+    try {
+        neuroevolution::model_artifact::LoadedWinnerArtifact a{};
+        if (!neuroevolution::model_artifact::TryReadWinnerArtifact(binary_path, metadata_path, a) ||
+            a.metadata.genome_byte_count > capacity) {
+            return 0;
+        }
+        std::uint32_t bits = 0;
+        std::memcpy(&bits, &a.metadata.best_fitness, 4);
+        meta[0] = bits;
+        meta[1] = a.metadata.generation_index;
+        meta[2] = a.metadata.best_index;
+        meta[3] = a.metadata.best_slot_index;
+        meta[4] = a.metadata.action_count;
+        meta[5] = a.metadata.genome_byte_count;
+        meta[6] = a.metadata.seed;
+        std::memcpy(genome, a.genome_bytes.get(), a.metadata.genome_byte_count);
+        for (std::size_t w = 0; w < a.action_space_words.word_count; ++w) {
+            for (std::size_t k = 0; k < 5; ++k) {
+                letters[w * 5 + k] = a.action_space_words.words[w].letter_indices[k];
+            }
+        }
+        *catalog_count = a.action_space_words.word_count;
+        const std::string path = a.metadata.action_space_path.string();
+        if (path.size() + 1 > path_capacity) {
+            return 0;
+        }
+        std::memcpy(path_out, path.c_str(), path.size() + 1);
+        return 1;
+    } catch (...) {
+        return 0;
+    }
 }
 
 // Records the POD layouts the C ABI relies on.

@@ -164,3 +164,32 @@ def test_restore_rejects_bad_checkpoints(tmp_path):
         good.resume()
     assert e.value.status == 12
     good.close()
+
+
+def test_persist_winner_writes_the_best_individual(tmp_path):
+    """TryPersistWinningGenome (cli/run_genetic_algorithm.cu:1519-1532): the summary's best slot image and metadata."""
+    rng = np.random.default_rng(8)
+    catalog = _catalog(rng, 200)
+    G.upload_catalog_everywhere(catalog)
+    rt = G.nwg.Runtime(200, 8, 4)
+    rt.bootstrap(8, seed=21, generation_index=5)
+    rt.evaluate(capi.word_counts(training=50, action_space=200))
+    s = rt.summary()
+    b, j = tmp_path / "win.bin", tmp_path / "win.json"
+    rt.persist_winner(b, j, seed=77, catalog=catalog, action_space_path="words.txt")
+    got = capi.read_winner_artifact(b, j)
+    m = got["metadata"]
+    assert np.array_equal(got["genome"], rt.download_slot(s.best_slot_index))
+    assert (m.generation_index, m.best_index, m.best_slot_index, m.action_count, m.seed) == (
+        5, s.best_index, s.best_slot_index, 200, 77)
+    assert abs(m.best_fitness - s.best_fitness) <= 1e-6 and np.array_equal(got["words"], catalog)
+    if O.ref_ckpt() is not None:
+        meta = np.zeros(7, np.uint64)
+        genome = np.zeros(m.genome_byte_count, np.uint8)
+        letters = np.zeros((capi.CATALOG_CAPACITY, 5), np.uint8)
+        count = C.c_size_t()
+        path = C.create_string_buffer(256)
+        assert O.ref_ckpt().refart_read(str(b).encode(), str(j).encode(), meta.ctypes.data, genome.ctypes.data,
+                                        genome.nbytes, letters.ctypes.data, C.byref(count), path, len(path)) == 1
+        assert np.array_equal(genome, got["genome"]) and count.value == 200
+    rt.close()
