@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define NWG_ABI_VERSION 3
+#define NWG_ABI_VERSION 4
 #define NWG_CATALOG_CAPACITY 4739
 
 enum {
@@ -165,6 +165,14 @@ typedef struct {
     size_t grid_column_count;
     size_t current_generation_index;
     size_t current_generation_size;
+    size_t next_generation_index;       /* the generation being assembled (reference DeviceSlabRuntimeBuffers) */
+    size_t next_generation_size;
+    size_t planned_child_count;         /* children of the last plan */
+    size_t slab_bytes;                  /* GenotypeSlabLayout::slab_bytes (slot_count x stride at creation) */
+    size_t generation_byte_budget_bytes;
+    size_t host_spillover_byte_budget_bytes;
+    size_t epicenter_row_count;         /* rows of the epicenter grid (generation capacity / columns) */
+    uint32_t prepared;                  /* 1 between nwg_prepare_generation (or a restore) and assembly */
 } nwg_runtime_info;
 
 /* Callbacks of TryAdvanceGenerationOnDevice (slab_runtime.hpp:81-84); return true to continue. */
@@ -370,6 +378,12 @@ int nwg_read_status(const nwg_runtime *runtime, int *status);
 int nwg_download_current_generation(const nwg_runtime *runtime, uint32_t *slot_indices, float *fitness,
                                     uint32_t *evaluation_counts, uint8_t *has_fitness, size_t capacity,
                                     size_t *count_out, size_t *generation_index_out);
+
+/* TryDownloadNextGenerationFromDevice (slab_runtime.hpp:134-135): the other generation buffer (after an advance,
+ * the parents). */
+int nwg_download_next_generation(const nwg_runtime *runtime, uint32_t *slot_indices, float *fitness,
+                                 uint32_t *evaluation_counts, uint8_t *has_fitness, size_t capacity,
+                                 size_t *count_out, size_t *generation_index_out);
 
 /* TryDownloadSlabSlotBytesFromDevice (slab_runtime.hpp:128-129): the slot's genome image,
  * slot_stride_bytes long, byte-identical to the reference layout. */

@@ -87,7 +87,10 @@ FORM_FP32, FORM_TC_BF16, FORM_TC_FP16, FORM_TC_TRUNK_BF16, FORM_TC_TRUNK_FP16 = 
 class RuntimeInfo(C.Structure):
     _fields_ = [(n, _sz) for n in ("action_count", "slot_stride_bytes", "slot_pitch_bytes", "slot_count",
                                    "max_generation_size", "grid_column_count", "current_generation_index",
-                                   "current_generation_size")]
+                                   "current_generation_size", "next_generation_index", "next_generation_size",
+                                   "planned_child_count", "slab_bytes", "generation_byte_budget_bytes",
+                                   "host_spillover_byte_budget_bytes", "epicenter_row_count")] + [
+        ("prepared", C.c_uint32)]
 
 
 class SlabLayout(C.Structure):
@@ -132,7 +135,7 @@ EXPORTS = [
     "nwg_assemble_prepared", "nwg_checkpoint_capture", "nwg_checkpoint_restore", "nwg_checkpoint_resume",
     "nwg_checkpoint_write", "nwg_checkpoint_read", "nwg_checkpoint_free", "nwg_checkpoint_checksum",
     "nwg_checkpoint_identity_hash", "nwg_winner_artifact_write", "nwg_winner_artifact_persist",
-    "nwg_winner_artifact_read",
+    "nwg_winner_artifact_read", "nwg_download_next_generation",
 ]
 
 

@@ -918,6 +918,14 @@ int nwg_get_info(const nwg_runtime *rt, nwg_runtime_info *info) {
     info->grid_column_count = rt->grid_column_count;
     info->current_generation_index = rt->cur_gen_index;
     info->current_generation_size = rt->cur_gen_size;
+    info->next_generation_index = rt->next_gen_index;
+    info->next_generation_size = rt->next_gen_size;
+    info->planned_child_count = rt->planned_children;
+    info->slab_bytes = rt->slab_byte_budget;
+    info->generation_byte_budget_bytes = rt->generation_byte_budget;
+    info->host_spillover_byte_budget_bytes = rt->host_spill_budget;
+    info->epicenter_row_count = rt->epicenter_rows;
+    info->prepared = rt->prepared ? 1u : 0u;
     return kOk;
 }
 
@@ -1276,27 +1284,55 @@ int nwg_read_status(const nwg_runtime *rt, int *status) {
     return kOk;
 }
 
-int nwg_download_current_generation(const nwg_runtime *rt, uint32_t *slot_indices, float *fitness,
-                                    uint32_t *evaluation_counts, uint8_t *has_fitness, size_t capacity,
-                                    size_t *count_out, size_t *generation_index_out) {
-    if (rt == nullptr || rt->cur_gen_size == 0 || capacity < rt->cur_gen_size) {
+namespace {
+
+int DownloadGeneration(const nwg_runtime *rt, bool current, uint32_t *slot_indices, float *fitness,
+                       uint32_t *evaluation_counts, uint8_t *has_fitness, size_t capacity, size_t *count_out,
+                       size_t *generation_index_out) {
+    const std::size_t n = current ? rt->cur_gen_size : rt->next_gen_size;
+    if (n == 0 || capacity < n) {
         return kInvalidGeneration;
     }
+    const std::uint32_t *slots = current ? rt->cur_slots : rt->next_slots;
+    const float *fit = current ? rt->cur_fitness : rt->next_fitness;
+    const std::uint32_t *evals = current ? rt->cur_eval : rt->next_eval;
+    const std::uint8_t *has = current ? rt->cur_has : rt->next_has;
     cudaStreamSynchronize(rt->stream);
-    const std::size_t n = rt->cur_gen_size;
-    if ((slot_indices && cudaMemcpy(slot_indices, rt->cur_slots, n * 4, cudaMemcpyDeviceToHost) != cudaSuccess) ||
-        (fitness && cudaMemcpy(fitness, rt->cur_fitness, n * 4, cudaMemcpyDeviceToHost) != cudaSuccess) ||
-        (evaluation_counts && cudaMemcpy(evaluation_counts, rt->cur_eval, n * 4, cudaMemcpyDeviceToHost) != cudaSuccess) ||
-        (has_fitness && cudaMemcpy(has_fitness, rt->cur_has, n, cudaMemcpyDeviceToHost) != cudaSuccess)) {
+    if ((slot_indices && cudaMemcpy(slot_indices, slots, n * 4, cudaMemcpyDeviceToHost) != cudaSuccess) ||
+        (fitness && cudaMemcpy(fitness, fit, n * 4, cudaMemcpyDeviceToHost) != cudaSuccess) ||
+        (evaluation_counts && cudaMemcpy(evaluation_counts, evals, n * 4, cudaMemcpyDeviceToHost) != cudaSuccess) ||
+        (has_fitness && cudaMemcpy(has_fitness, has, n, cudaMemcpyDeviceToHost) != cudaSuccess)) {
         return kCudaFailure;
     }
     if (count_out) {
         *count_out = n;
     }
     if (generation_index_out) {
-        *generation_index_out = rt->cur_gen_index;
+        *generation_index_out = current ? rt->cur_gen_index : rt->next_gen_index;
     }
     return kOk;
+}
+
+}  // namespace
+
+int nwg_download_current_generation(const nwg_runtime *rt, uint32_t *slot_indices, float *fitness,
+                                    uint32_t *evaluation_counts, uint8_t *has_fitness, size_t capacity,
+                                    size_t *count_out, size_t *generation_index_out) {
+    if (rt == nullptr) {
+        return kInvalidGeneration;
+    }
+    return DownloadGeneration(rt, true, slot_indices, fitness, evaluation_counts, has_fitness, capacity, count_out,
+                              generation_index_out);
+}
+
+int nwg_download_next_generation(const nwg_runtime *rt, uint32_t *slot_indices, float *fitness,
+                                 uint32_t *evaluation_counts, uint8_t *has_fitness, size_t capacity,
+                                 size_t *count_out, size_t *generation_index_out) {
+    if (rt == nullptr) {
+        return kInvalidGeneration;
+    }
+    return DownloadGeneration(rt, false, slot_indices, fitness, evaluation_counts, has_fitness, capacity, count_out,
+                              generation_index_out);
 }
 
 int nwg_download_slot(const nwg_runtime *rt, uint32_t slot_index, uint8_t *bytes, size_t capacity,

@@ -6,6 +6,8 @@ Outputs:
   oracle/_ref/libref_host.so    -- the reference's host-callable code + episode loop harness
   oracle/_ref/libref_dev.so     -- the reference's device functions + harness kernels, sm_100a
   oracle/_ref/libref_ckpt.so    -- the reference's runtime (checkpoint format, capture, restore, resume), sm_100a
+  oracle/_ref/shim_driver       -- tests/shim_driver.cu: a caller of the reference's slab_device API, linked
+                                   against libnwg.so through include/nwg_slab_device_shim.hpp
 
 The oracle/_ref libraries are compiled from the reference's own headers where they
 lie (REFERENCE_ROOT/src); nothing is copied. They are only rebuilt when the reference
@@ -84,10 +86,30 @@ def build_reference(force: bool = False) -> list[Path]:
     return [host_out, dev_out, ckpt_out]
 
 
+def build_shim_driver(force: bool = False) -> Path | None:
+    """The compat-layer test program: the reference's API headers where they lie, the shim, libnwg.so."""
+    if not reference_present():
+        return None
+    root = HERE.parent
+    lib_dir = root / "neuroevolutionary-wordle_b200"
+    out = REF_DIR / "shim_driver"
+    srcs = [root / "tests" / "shim_driver.cu", root / "include" / "nwg_slab_device_shim.hpp",
+            root / "include" / "nwg_capi.h"]
+    if force or _stale(out, srcs):
+        REF_DIR.mkdir(exist_ok=True)
+        _run([NVCC, *ARCH, "-O2", "-std=c++20", "-I", str(REFERENCE_ROOT / "src"), "-I", str(root / "include"),
+              str(root / "tests" / "shim_driver.cu"),
+              str(REFERENCE_ROOT / "src" / "genetic_algorithm" / "genotype_slab" / "slab_allocator.cpp"),
+              "-L", str(lib_dir), "-lnwg", "-Xlinker", "-rpath,$ORIGIN/../../neuroevolutionary-wordle_b200",
+              "-o", str(out)])
+    return out
+
+
 def build_all(force: bool = False) -> None:
     build_oracle(force)
     build_tape(force)
     build_reference(force)
+    build_shim_driver(force)
 
 
 if __name__ == "__main__":

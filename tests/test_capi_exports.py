@@ -47,7 +47,7 @@ def test_status_strings_match_reference_codes():
 
 def test_abi_version():
     pkg = importlib.import_module("neuroevolutionary-wordle_b200")
-    assert pkg.capi.lib().nwg_abi_version() == 3
+    assert pkg.capi.lib().nwg_abi_version() == 4
 
 
 def test_workload_generator_is_seeded_and_distinct():
