@@ -368,6 +368,80 @@ int nwg_winner_artifact_read(const char *binary_path, const char *metadata_path,
                              size_t *catalog_count, char *action_space_path, size_t path_capacity,
                              char *timestamp_local, size_t timestamp_capacity);
 
+/* GenerationFitnessTelemetryRow (cli/run_genetic_algorithm.cu:594-610). */
+typedef struct {
+    size_t generation;
+    size_t population_size;
+    size_t training_word_count;
+    float fitness_min;
+    float fitness_mean;
+    float fitness_median;
+    float fitness_p90;
+    float fitness_p99;
+    float fitness_max;
+    float fitness_stddev;
+    size_t distinct_fitness_count;
+    bool has_breeding_metrics;
+    size_t parent_childless_count;
+    size_t parent_one_child_count;
+    size_t parent_multiple_children_count;
+} nwg_fitness_telemetry;
+
+/* GeneticConvergenceTelemetryRow (cli/run_genetic_algorithm.cu:612-624); elapsed_ms is device time here. */
+typedef struct {
+    size_t generation;
+    size_t sample_organisms;
+    size_t sample_weights;
+    size_t pair_count;
+    float centroid_distance_mean;
+    float centroid_distance_min;
+    float centroid_distance_max;
+    float pairwise_distance_mean;
+    float pairwise_distance_min;
+    float pairwise_distance_max;
+    float elapsed_ms;
+} nwg_convergence_telemetry;
+
+/* The adaptive release thresholds of the reference CLI (run_genetic_algorithm.cu:94-101); its defaults
+ * (training_folder/training_data.hpp:17-20) are 3, 10, 6.0 and 0.20. */
+typedef struct {
+    size_t min_gap_generations;
+    size_t first_new_release_generation;
+    float centroid_distance_threshold;
+    float fitness_p99_threshold;
+} nwg_shard_release_policy;
+
+/* TryCollectGenerationFitnessTelemetry (cli/run_genetic_algorithm.cu:1080-1186) on the GPU: the current
+ * generation's fitness min, mean, median, p90 and p99 (nearest rank), max, population standard deviation and
+ * distinct-value count, bit-identical to the reference's host sort and sequential double sums; with
+ * with_breeding, the last plan's childless / one-child / several-children parent counts. counts may be NULL
+ * (training_word_count 0). Populations up to 32,768 (NWG_UNSUPPORTED beyond); NWG_POPULATION_NOT_EVALUATED when an
+ * individual has no fitness. */
+int nwg_fitness_telemetry_collect(const nwg_runtime *runtime, const nwg_runtime_word_counts *counts,
+                                  bool with_breeding, nwg_fitness_telemetry *row);
+
+/* TryCollectGeneticConvergenceTelemetry (cli/run_genetic_algorithm.cu:941-1054) on the GPU: the sample plan
+ * (genetic_convergence.hpp:86-119: 256 organisms, 8,192 trainable scalars, 512 pairs, seeded by run seed and
+ * generation) gathered from the slab and reduced to centroid and pairwise distances, bit-identical to the
+ * reference's TryComputeMetrics. */
+int nwg_convergence_telemetry_collect(const nwg_runtime *runtime, uint32_t run_seed, nwg_convergence_telemetry *row);
+
+/* MakeSamplePlan (genetic_convergence.hpp:86-119): organisms[<=256], weights[<=8192], pairs[512][2]. */
+int nwg_convergence_sample_plan(size_t organism_count, size_t trainable_count, uint32_t run_seed, size_t generation,
+                                uint32_t *organisms, size_t *organism_count_out, uint32_t *weights,
+                                size_t *weight_count_out, uint32_t *pairs, size_t *pair_count_out);
+
+/* TryMaybeReleaseTrainingDataShard (cli/run_genetic_algorithm.cu:1199-1282): after the foundation release and the
+ * gap rules, releases the next word_count_step catalog words when the centroid distance mean is at most its
+ * threshold and the fitness p99 exceeds its threshold: records the release in history and fills pending (for
+ * nwg_advance) and next_word_count. Meant for the shard-release callback. The telemetry rows it computed are
+ * returned when the pointers are not NULL (left zero when a gap rule decided). */
+int nwg_maybe_release_training_shard(const nwg_runtime *runtime, const nwg_runtime_word_counts *counts,
+                                     const nwg_shard_release_policy *policy, size_t catalog_word_count,
+                                     uint32_t run_seed, nwg_shard_release_history *history,
+                                     nwg_pending_injection *pending, size_t *next_word_count,
+                                     nwg_fitness_telemetry *fitness_row, nwg_convergence_telemetry *convergence_row);
+
 /* SwapDeviceSlabGenerationBuffers (slab_runtime.hpp:181). */
 int nwg_swap_generations(nwg_runtime *runtime);
 

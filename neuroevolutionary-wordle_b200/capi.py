@@ -122,6 +122,34 @@ class WinnerMetadata(C.Structure):
                 ("seed", C.c_uint32)]
 
 
+class FitnessTelemetry(C.Structure):
+    """nwg_fitness_telemetry: GenerationFitnessTelemetryRow (cli/run_genetic_algorithm.cu:594-610)."""
+    _fields_ = [("generation", _sz), ("population_size", _sz), ("training_word_count", _sz)] + [
+        (n, C.c_float) for n in ("fitness_min", "fitness_mean", "fitness_median", "fitness_p90", "fitness_p99",
+                                 "fitness_max", "fitness_stddev")] + [
+        ("distinct_fitness_count", _sz), ("has_breeding_metrics", C.c_bool), ("parent_childless_count", _sz),
+        ("parent_one_child_count", _sz), ("parent_multiple_children_count", _sz)]
+
+
+class ConvergenceTelemetry(C.Structure):
+    """nwg_convergence_telemetry: GeneticConvergenceTelemetryRow (cli/run_genetic_algorithm.cu:612-624)."""
+    _fields_ = [(n, _sz) for n in ("generation", "sample_organisms", "sample_weights", "pair_count")] + [
+        (n, C.c_float) for n in ("centroid_distance_mean", "centroid_distance_min", "centroid_distance_max",
+                                 "pairwise_distance_mean", "pairwise_distance_min", "pairwise_distance_max",
+                                 "elapsed_ms")]
+
+
+class ShardReleasePolicy(C.Structure):
+    """nwg_shard_release_policy; defaults of training_folder/training_data.hpp:17-20."""
+    _fields_ = [("min_gap_generations", _sz), ("first_new_release_generation", _sz),
+                ("centroid_distance_threshold", C.c_float), ("fitness_p99_threshold", C.c_float)]
+
+    def __init__(self, min_gap_generations=3, first_new_release_generation=10, centroid_distance_threshold=6.0,
+                 fitness_p99_threshold=0.20):
+        super().__init__(min_gap_generations, first_new_release_generation, centroid_distance_threshold,
+                         fitness_p99_threshold)
+
+
 POST_FITNESS_FN = C.CFUNCTYPE(C.c_bool, _vp, C.POINTER(RuntimeWordCounts), _vp)
 SHARD_RELEASE_FN = C.CFUNCTYPE(C.c_bool, _vp, C.POINTER(RuntimeWordCounts), C.POINTER(PendingInjection), _vp)
 
@@ -135,7 +163,8 @@ EXPORTS = [
     "nwg_assemble_prepared", "nwg_checkpoint_capture", "nwg_checkpoint_restore", "nwg_checkpoint_resume",
     "nwg_checkpoint_write", "nwg_checkpoint_read", "nwg_checkpoint_free", "nwg_checkpoint_checksum",
     "nwg_checkpoint_identity_hash", "nwg_winner_artifact_write", "nwg_winner_artifact_persist",
-    "nwg_winner_artifact_read", "nwg_download_next_generation",
+    "nwg_winner_artifact_read", "nwg_download_next_generation", "nwg_fitness_telemetry_collect",
+    "nwg_convergence_telemetry_collect", "nwg_convergence_sample_plan", "nwg_maybe_release_training_shard",
 ]
 
 
@@ -182,6 +211,15 @@ def lib() -> C.CDLL:
                                               C.c_char_p]
     L.nwg_winner_artifact_read.argtypes = [C.c_char_p, C.c_char_p, C.POINTER(WinnerMetadata), _vp, _sz, _vp,
                                            C.POINTER(_sz), C.c_char_p, _sz, C.c_char_p, _sz]
+    L.nwg_fitness_telemetry_collect.argtypes = [_vp, C.POINTER(RuntimeWordCounts), C.c_bool,
+                                                C.POINTER(FitnessTelemetry)]
+    L.nwg_convergence_telemetry_collect.argtypes = [_vp, C.c_uint32, C.POINTER(ConvergenceTelemetry)]
+    L.nwg_convergence_sample_plan.argtypes = [_sz, _sz, C.c_uint32, _sz, _vp, C.POINTER(_sz), _vp, C.POINTER(_sz),
+                                              _vp, C.POINTER(_sz)]
+    L.nwg_maybe_release_training_shard.argtypes = [_vp, C.POINTER(RuntimeWordCounts), C.POINTER(ShardReleasePolicy),
+                                                   _sz, C.c_uint32, C.POINTER(ShardReleaseHistory),
+                                                   C.POINTER(PendingInjection), C.POINTER(_sz),
+                                                   C.POINTER(FitnessTelemetry), C.POINTER(ConvergenceTelemetry)]
     L.nwg_swap_generations.argtypes = [_vp]
     L.nwg_read_status.argtypes = [_vp, C.POINTER(C.c_int)]
     L.nwg_download_current_generation.argtypes = [_vp, _vp, _vp, _vp, _vp, _sz, C.POINTER(_sz), C.POINTER(_sz)]
@@ -374,6 +412,31 @@ class Runtime:
                                                 timestamp.encode() if timestamp is not None else None),
               "nwg_winner_artifact_persist")
 
+    def fitness_telemetry(self, counts: RuntimeWordCounts | None = None, with_breeding: bool = False):
+        row = FitnessTelemetry()
+        check(lib().nwg_fitness_telemetry_collect(self.handle, C.byref(counts) if counts else None, with_breeding,
+                                                  C.byref(row)), "nwg_fitness_telemetry_collect")
+        return row
+
+    def convergence_telemetry(self, run_seed: int):
+        row = ConvergenceTelemetry()
+        check(lib().nwg_convergence_telemetry_collect(self.handle, run_seed, C.byref(row)),
+              "nwg_convergence_telemetry_collect")
+        return row
+
+    def maybe_release_training_shard(self, counts: RuntimeWordCounts, policy: ShardReleasePolicy,
+                                     catalog_word_count: int, run_seed: int, history: ShardReleaseHistory):
+        """TryMaybeReleaseTrainingDataShard: (pending injection, next word count, fitness row, convergence row)."""
+        pending = PendingInjection()
+        nxt = _sz()
+        f = FitnessTelemetry()
+        c = ConvergenceTelemetry()
+        check(lib().nwg_maybe_release_training_shard(self.handle, C.byref(counts), C.byref(policy),
+                                                     catalog_word_count, run_seed, C.byref(history), C.byref(pending),
+                                                     C.byref(nxt), C.byref(f), C.byref(c)),
+              "nwg_maybe_release_training_shard")
+        return pending, nxt.value, f, c
+
     def resume(self) -> None:
         """TryResumeGenerationFromCheckpointOnDevice: assemble a restored boundary."""
         check(lib().nwg_checkpoint_resume(self.handle), "nwg_checkpoint_resume")
@@ -548,4 +611,16 @@ def read_winner_artifact(binary_path, metadata_path) -> dict:
                                          len(path), stamp, len(stamp)), "nwg_winner_artifact_read")
     return dict(metadata=m, genome=genome, words=letters[:count.value].copy(), action_space_path=path.value.decode(),
                 timestamp=stamp.value.decode())
+
+
+def convergence_sample_plan(organism_count: int, trainable_count: int, run_seed: int, generation: int):
+    """MakeSamplePlan (genetic_convergence.hpp:86-119): organism indices, weight indices, (first, second) pairs."""
+    org = np.zeros(256, np.uint32)
+    w = np.zeros(8192, np.uint32)
+    pairs = np.zeros((512, 2), np.uint32)
+    n_o, n_w, n_p = _sz(), _sz(), _sz()
+    check(lib().nwg_convergence_sample_plan(organism_count, trainable_count, run_seed, generation, _np_ptr(org),
+                                            C.byref(n_o), _np_ptr(w), C.byref(n_w), _np_ptr(pairs), C.byref(n_p)),
+          "nwg_convergence_sample_plan")
+    return org[:n_o.value].copy(), w[:n_w.value].copy(), pairs[:n_p.value].copy()
 

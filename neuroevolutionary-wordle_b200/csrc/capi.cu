@@ -742,6 +742,24 @@ int ReadBoundary(const nwg_runtime *rt, BoundaryState *out) {
     return kOk;
 }
 
+int ReadGenerationView(const nwg_runtime *rt, GenerationView *out) {
+    if (rt == nullptr || out == nullptr) {
+        return kInvalidRuntimeConfig;
+    }
+    out->stream = rt->stream;
+    out->slab = rt->slab;
+    out->pitch = rt->pitch;
+    out->action_count = rt->action_count;
+    out->slots = rt->cur_slots;
+    out->fitness = rt->cur_fitness;
+    out->has_fitness = rt->cur_has;
+    out->pairs = rt->pairs;
+    out->generation_index = rt->cur_gen_index;
+    out->generation_size = rt->cur_gen_size;
+    out->planned_children = rt->planned_children;
+    return kOk;
+}
+
 int InstallBoundary(nwg_runtime *rt, const std::uint32_t *slots, const float *fitness, const std::uint32_t *eval,
                     const std::uint8_t *has, std::size_t count, std::size_t generation_index,
                     const std::uint32_t *pairs, std::size_t child_count, std::uint32_t seed,

@@ -181,6 +181,19 @@ struct BoundaryState {
 // kInvalidAssemblyPlan when the runtime is not prepared.
 int ReadBoundary(const nwg_runtime *rt, BoundaryState *out);
 
+// Device buffers of the current generation, for read-only consumers (telemetry.cu). Pointers are the runtime's.
+struct GenerationView {
+    cudaStream_t stream;
+    const std::uint8_t *slab;
+    std::size_t pitch, action_count;
+    const std::uint32_t *slots;
+    const float *fitness;
+    const std::uint8_t *has_fitness;
+    const std::uint32_t *pairs;  // the last plan's (first, second) parent indices
+    std::size_t generation_index, generation_size, planned_children;
+};
+int ReadGenerationView(const nwg_runtime *rt, GenerationView *out);
+
 // A runtime with explicit sizes (a restored checkpoint's, slab_runtime.cu:1746-1765).
 struct RuntimeShape {
     std::size_t action_count, slot_count, slab_bytes, max_generation_size, grid_column_count;

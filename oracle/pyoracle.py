@@ -296,6 +296,9 @@ def ref_ckpt() -> C.CDLL | None:
     L.refart_write.argtypes = [C.c_char_p, C.c_char_p, C.c_void_p, C.c_void_p, _sz, C.c_void_p, C.c_char_p]
     L.refart_read.argtypes = [C.c_char_p, C.c_char_p, C.c_void_p, C.c_void_p, _sz, C.c_void_p, C.POINTER(_sz),
                               C.c_char_p, _sz]
+    L.refconv_plan.argtypes = [_sz, _sz, C.c_uint32, _sz, C.c_void_p, C.POINTER(_sz), C.c_void_p, C.POINTER(_sz),
+                               C.c_void_p, C.POINTER(_sz)]
+    L.refconv_metrics.argtypes = [C.c_void_p, _sz, _sz, C.c_void_p, _sz, C.c_void_p]
     L.refckpt_runtime_resume.argtypes = [C.c_char_p, C.c_void_p, _sz, C.c_void_p, _sz, C.POINTER(_sz),
                                          C.POINTER(_sz)]
     return L
@@ -354,3 +357,92 @@ def ref_dev() -> C.CDLL | None:
     L.refdev_bootstrap.argtypes = [C.c_void_p, _sz, _sz, _sz, C.c_uint32, _sz, C.c_void_p]
     L.refdev_inject.argtypes = [C.c_void_p, _sz, _sz, _sz, _sz, _sz, C.c_void_p, C.c_void_p]
     return L
+
+
+# ---- shard-release statistics (test infrastructure: restatements of the reference's host reductions) ----
+
+def fitness_telemetry(fitness: np.ndarray, pairs: np.ndarray | None = None) -> dict:
+    """cli/run_genetic_algorithm.cu:1100-1183: sort, sequential double sums, nearest-rank percentiles, distinct
+    count; with pairs, children per parent classified 0 / 1 / more."""
+    import math
+
+    v = np.sort(np.asarray(fitness, np.float32))
+    n = len(v)
+    total = 0.0
+    for x in v:
+        total += float(x)
+    mean = total / n
+    squares = 0.0
+    for x in v:
+        d = float(x) - mean
+        squares += d * d
+    mid = n // 2
+    median = v[mid] if n % 2 else np.float32(np.float32(v[mid - 1] + v[mid]) * np.float32(0.5))
+
+    def rank(p):
+        r = math.ceil((p / 100.0) * n)
+        i = 0 if r == 0 else r - 1
+        return v[i if i < n else n - 1]
+
+    out = dict(min=v[0], max=v[-1], mean=np.float32(mean), median=np.float32(median), p90=rank(90.0), p99=rank(99.0),
+               stddev=np.float32(math.sqrt(squares / n)), distinct=int(1 + np.count_nonzero(v[1:] != v[:-1])))
+    if pairs is not None:
+        per = np.bincount(np.asarray(pairs, np.int64).reshape(-1), minlength=n)
+        out.update(childless=int(np.sum(per == 0)), one_child=int(np.sum(per == 1)), more=int(np.sum(per > 1)))
+    return out
+
+
+def convergence_metrics(values: np.ndarray, pairs: np.ndarray) -> np.ndarray:
+    """genetic_convergence.hpp:121-194 in its loop order with float32 rounding per operation: centroid mean, min,
+    max, then pairwise mean, min, max."""
+    values = np.asarray(values, np.float32)
+    organisms, weights = values.shape
+    centroid = np.zeros(weights, np.float32)
+    for o in range(organisms):
+        centroid = centroid + values[o]
+    inverse = np.float32(1.0) / np.float32(organisms)
+    centroid = centroid * inverse
+
+    def distances(a, b):
+        squared = np.zeros(a.shape[0], np.float32)
+        for w in range(weights):
+            d = a[:, w] - b[:, w]
+            squared = squared + d * d
+        return np.sqrt(squared)
+
+    def summary(d, mean_of):
+        total = np.float32(0.0)
+        for x in d:
+            total = np.float32(total + x)
+        return [mean_of(total), np.float32(d.min()), np.float32(max(np.float32(0.0), d.max()))]
+
+    out = summary(distances(values, np.broadcast_to(centroid, values.shape)), lambda t: np.float32(t * inverse))
+    pairs = np.asarray(pairs, np.int64).reshape(-1, 2)
+    if len(pairs) == 0:
+        out += [np.float32(0.0), np.float32(0.0), np.float32(0.0)]
+    else:
+        out += summary(distances(values[pairs[:, 0]], values[pairs[:, 1]]),
+                       lambda t: np.float32(t / np.float32(len(pairs))))
+    return np.array(out, np.float32)
+
+
+def ref_convergence_plan(organisms: int, trainable: int, seed: int, generation: int):
+    """MakeSamplePlan of the reference (oracle/_ref/libref_ckpt.so)."""
+    L = ref_ckpt()
+    o = np.zeros(256, np.uint64)
+    w = np.zeros(8192, np.uint64)
+    p = np.zeros((512, 2), np.uint64)
+    n_o, n_w, n_p = _sz(), _sz(), _sz()
+    assert L.refconv_plan(organisms, trainable, seed, generation, o.ctypes.data, C.byref(n_o), w.ctypes.data,
+                          C.byref(n_w), p.ctypes.data, C.byref(n_p)) == 1
+    return o[:n_o.value], w[:n_w.value], p[:n_p.value]
+
+
+def ref_convergence_metrics(values: np.ndarray, pairs: np.ndarray) -> np.ndarray:
+    """TryComputeMetrics of the reference (oracle/_ref/libref_ckpt.so)."""
+    values = np.ascontiguousarray(values, np.float32)
+    p = np.ascontiguousarray(np.asarray(pairs, np.uint64).reshape(-1, 2))
+    out = np.zeros(6, np.float32)
+    assert ref_ckpt().refconv_metrics(values.ctypes.data, values.shape[0], values.shape[1], p.ctypes.data, len(p),
+                                      out.ctypes.data) == 1
+    return out

@@ -9,6 +9,7 @@
 //   refckpt_identity_hash  the training-data identity hash, mixed by the reference's helpers in the order
 //                          TryDownloadBoundaryCheckpointPayload uses (slab_runtime.cu:1283-1297)
 //   refart_write / refart_read TryWriteWinnerArtifactToPaths / TryReadWinnerArtifact (model_artifact/)
+//   refconv_plan / refconv_metrics MakeSamplePlan / TryComputeMetrics (genetic_algorithm/genetic_convergence.hpp)
 // Device entry points (drive the reference's whole runtime on the GPU):
 //   refckpt_runtime_capture create, bootstrap, TryCreatePrebreedingCheckpointOnDevice, write
 //   refckpt_runtime_evaluate create, bootstrap, TryEvaluateCurrentGenerationFitnessOnDevice, fitness arrays
@@ -20,6 +21,7 @@
 #include "training_folder/training_data.cu"
 #include "model_artifact/winner_artifact.cpp"
 #include "model_artifact/winner_artifact_reader.cpp"
+#include "genetic_algorithm/genetic_convergence.hpp"
 
 #include <cstring>
 #include <random>
@@ -222,6 +224,50 @@ int refart_read(const char *binary_path, const char *metadata_path, std::uint64_
     } catch (...) {
         return 0;
     }
+}
+
+int refconv_plan(std::size_t organisms, std::size_t trainable, std::uint32_t seed, std::size_t generation,
+                 std::uint64_t *org_out, std::size_t *n_org, std::uint64_t *w_out, std::size_t *n_w,
+                 std::uint64_t *pairs_out, std::size_t *n_pairs) {
+    namespace gc = neuroevolution::genetic_algorithm::genetic_convergence;
+    const gc::GeneticConvergenceSamplePlan plan = gc::MakeSamplePlan(organisms, trainable, seed, generation);
+    for (std::size_t i = 0; i < plan.organism_indices.size(); ++i) {
+        org_out[i] = plan.organism_indices[i];
+    }
+    for (std::size_t i = 0; i < plan.weight_indices.size(); ++i) {
+        w_out[i] = plan.weight_indices[i];
+    }
+    for (std::size_t i = 0; i < plan.pairs.size(); ++i) {
+        pairs_out[2 * i] = plan.pairs[i].first;
+        pairs_out[2 * i + 1] = plan.pairs[i].second;
+    }
+    *n_org = plan.organism_indices.size();
+    *n_w = plan.weight_indices.size();
+    *n_pairs = plan.pairs.size();
+    return 1;
+}
+
+// out: centroid mean, min, max, pairwise mean, min, max
+int refconv_metrics(const float *values, std::size_t organisms, std::size_t weights, const std::uint64_t *pairs,
+                    std::size_t pair_count, float *out) {
+    namespace gc = neuroevolution::genetic_algorithm::genetic_convergence;
+    std::vector<float> v(values, values + organisms * weights);
+    std::vector<gc::GeneticConvergencePair> p(pair_count);
+    for (std::size_t i = 0; i < pair_count; ++i) {
+        p[i].first = pairs[2 * i];
+        p[i].second = pairs[2 * i + 1];
+    }
+    gc::GeneticConvergenceMetrics m{};
+    if (!gc::TryComputeMetrics(v, organisms, weights, p, m)) {
+        return 0;
+    }
+    out[0] = m.centroid_distance_mean;
+    out[1] = m.centroid_distance_min;
+    out[2] = m.centroid_distance_max;
+    out[3] = m.pairwise_distance_mean;
+    out[4] = m.pairwise_distance_min;
+    out[5] = m.pairwise_distance_max;
+    return 1;
 }
 
 // Records the POD layouts the C ABI relies on.
