@@ -442,6 +442,34 @@ int nwg_maybe_release_training_shard(const nwg_runtime *runtime, const nwg_runti
                                      nwg_pending_injection *pending, size_t *next_word_count,
                                      nwg_fitness_telemetry *fitness_row, nwg_convergence_telemetry *convergence_row);
 
+/* Single-model inference (inference/single_model_device_runtime.hpp:22-47): one genome and its own action-space
+ * catalog on the device. */
+typedef struct nwg_single_model nwg_single_model;
+
+/* SelectedAction (model/output_embedding/output_embedding.hpp:35-39). */
+typedef struct {
+    uint8_t word[5];      /* letter indices */
+    float score;
+    size_t action_index;
+} nwg_selected_action;
+
+/* TryCreateSingleModelDeviceRuntime (single_model_device_runtime.hpp:38-40): genome_byte_count must be the
+ * stride of catalog_count actions (NWG_INVALID_RUNTIME_CONFIG otherwise). */
+int nwg_single_model_create(const uint8_t *genome_bytes, size_t genome_byte_count, const uint8_t *catalog_letters,
+                            size_t catalog_count, nwg_single_model **model_out);
+void nwg_single_model_destroy(nwg_single_model *model);
+int nwg_single_model_set_stream(nwg_single_model *model, void *cuda_stream);
+
+/* TrySelectNextGuessWithSingleModelDeviceRuntime (single_model_device_runtime.hpp:44-47) for grid_count grids in
+ * one call: grid g has turn_counts[g] turns, turn u's guess at guess_letters[(g*6+u)*5 ..] (letter indices) and
+ * its tiles at feedback[(g*6+u)*5 ..] (0 green, 1 yellow, 2 grey). Each selection is the reference's: FP32 scores
+ * over the whole catalog, words already guessed masked, ties to the lowest index. A grid with more than five
+ * turns, a won turn or an invalid letter or tile gives NWG_POLICY_FORWARD_FAILED (the reference's
+ * kPolicyForwardFailed) and no selection; a grid whose every action is guessed gives NWG_ACTION_SELECTION_FAILED
+ * (its action zeroed, the others filled). */
+int nwg_single_model_select(nwg_single_model *model, const uint8_t *guess_letters, const uint8_t *feedback,
+                            const uint8_t *turn_counts, size_t grid_count, nwg_selected_action *actions);
+
 /* SwapDeviceSlabGenerationBuffers (slab_runtime.hpp:181). */
 int nwg_swap_generations(nwg_runtime *runtime);
 

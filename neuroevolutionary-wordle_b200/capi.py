@@ -150,6 +150,11 @@ class ShardReleasePolicy(C.Structure):
                          fitness_p99_threshold)
 
 
+class SelectedAction(C.Structure):
+    """nwg_selected_action: SelectedAction (model/output_embedding/output_embedding.hpp:35-39)."""
+    _fields_ = [("word", C.c_uint8 * 5), ("score", C.c_float), ("action_index", _sz)]
+
+
 POST_FITNESS_FN = C.CFUNCTYPE(C.c_bool, _vp, C.POINTER(RuntimeWordCounts), _vp)
 SHARD_RELEASE_FN = C.CFUNCTYPE(C.c_bool, _vp, C.POINTER(RuntimeWordCounts), C.POINTER(PendingInjection), _vp)
 
@@ -165,6 +170,7 @@ EXPORTS = [
     "nwg_checkpoint_identity_hash", "nwg_winner_artifact_write", "nwg_winner_artifact_persist",
     "nwg_winner_artifact_read", "nwg_download_next_generation", "nwg_fitness_telemetry_collect",
     "nwg_convergence_telemetry_collect", "nwg_convergence_sample_plan", "nwg_maybe_release_training_shard",
+    "nwg_single_model_create", "nwg_single_model_destroy", "nwg_single_model_set_stream", "nwg_single_model_select",
 ]
 
 
@@ -220,6 +226,11 @@ def lib() -> C.CDLL:
                                                    _sz, C.c_uint32, C.POINTER(ShardReleaseHistory),
                                                    C.POINTER(PendingInjection), C.POINTER(_sz),
                                                    C.POINTER(FitnessTelemetry), C.POINTER(ConvergenceTelemetry)]
+    L.nwg_single_model_create.argtypes = [_vp, _sz, _vp, _sz, C.POINTER(_vp)]
+    L.nwg_single_model_destroy.argtypes = [_vp]
+    L.nwg_single_model_destroy.restype = None
+    L.nwg_single_model_set_stream.argtypes = [_vp, _vp]
+    L.nwg_single_model_select.argtypes = [_vp, _vp, _vp, _vp, _sz, C.POINTER(SelectedAction)]
     L.nwg_swap_generations.argtypes = [_vp]
     L.nwg_read_status.argtypes = [_vp, C.POINTER(C.c_int)]
     L.nwg_download_current_generation.argtypes = [_vp, _vp, _vp, _vp, _vp, _sz, C.POINTER(_sz), C.POINTER(_sz)]
@@ -623,4 +634,43 @@ def convergence_sample_plan(organism_count: int, trainable_count: int, run_seed:
                                             C.byref(n_o), _np_ptr(w), C.byref(n_w), _np_ptr(pairs), C.byref(n_p)),
           "nwg_convergence_sample_plan")
     return org[:n_o.value].copy(), w[:n_w.value].copy(), pairs[:n_p.value].copy()
+
+
+class SingleModel:
+    """A single-model inference runtime (inference/single_model_device_runtime.hpp:22-47): one genome image and its
+    own catalog on the device; select() answers a batch of grids in one call."""
+
+    def __init__(self, genome: np.ndarray, catalog: np.ndarray):
+        g = np.ascontiguousarray(genome).view(np.uint8)
+        cat = np.ascontiguousarray(catalog, np.uint8)
+        handle = _vp()
+        check(lib().nwg_single_model_create(_np_ptr(g), g.nbytes, _np_ptr(cat), len(cat), C.byref(handle)),
+              "nwg_single_model_create")
+        self.handle = handle
+        self.catalog = cat
+
+    def close(self):
+        if self.handle:
+            lib().nwg_single_model_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def select(self, guesses: np.ndarray, feedback: np.ndarray, turns: np.ndarray):
+        """guesses, feedback: (n, 6, 5) letter indices / tiles (0 green, 1 yellow, 2 grey); turns: (n,).
+        Returns (action indices, scores) as arrays; raises NwgError on a failed grid."""
+        guesses = np.ascontiguousarray(guesses, np.uint8).reshape(-1, 6, 5)
+        feedback = np.ascontiguousarray(feedback, np.uint8).reshape(-1, 6, 5)
+        turns = np.ascontiguousarray(turns, np.uint8)
+        n = len(turns)
+        out = (SelectedAction * max(n, 1))()
+        check(lib().nwg_single_model_select(self.handle, _np_ptr(guesses), _np_ptr(feedback), _np_ptr(turns), n, out),
+              "nwg_single_model_select")
+        index = np.array([out[i].action_index for i in range(n)], np.int64)
+        score = np.array([out[i].score for i in range(n)], np.float32)
+        return index, score
 

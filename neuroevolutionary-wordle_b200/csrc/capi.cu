@@ -742,6 +742,41 @@ int ReadBoundary(const nwg_runtime *rt, BoundaryState *out) {
     return kOk;
 }
 
+int BuildCatalogTables(const std::uint8_t *letters, std::size_t word_count, std::uint32_t **codes_out,
+                       float **fixed_out, std::size_t *pad_out, std::vector<std::uint32_t> *host_codes) {
+    *codes_out = nullptr;
+    *fixed_out = nullptr;
+    const std::size_t pad = ((word_count + 127) / 128) * 128;
+    std::vector<std::uint32_t> codes(pad, 0);
+    std::vector<float> fixed(static_cast<std::size_t>(kFixedDim) * pad, 0.0f);
+    for (std::size_t w = 0; w < word_count; ++w) {
+        codes[w] = PackWord(letters + kWordLength * w);
+        int counts[kAlphabet] = {0};
+        for (int p = 0; p < kWordLength; ++p) {
+            ++counts[letters[kWordLength * w + p]];
+        }
+        // output_embedding.hpp:59-73: letter count, or -1 when the letter is absent
+        for (int l = 0; l < kFixedDim; ++l) {
+            fixed[static_cast<std::size_t>(l) * pad + w] = counts[l] == 0 ? -1.0f : static_cast<float>(counts[l]);
+        }
+    }
+    if (cudaMalloc(codes_out, pad * sizeof(std::uint32_t)) != cudaSuccess ||
+        cudaMalloc(fixed_out, fixed.size() * sizeof(float)) != cudaSuccess ||
+        cudaMemcpy(*codes_out, codes.data(), pad * sizeof(std::uint32_t), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(*fixed_out, fixed.data(), fixed.size() * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaFree(*codes_out);
+        cudaFree(*fixed_out);
+        *codes_out = nullptr;
+        *fixed_out = nullptr;
+        return kCudaFailure;
+    }
+    *pad_out = pad;
+    if (host_codes != nullptr) {
+        host_codes->assign(codes.begin(), codes.begin() + static_cast<std::ptrdiff_t>(word_count));
+    }
+    return kOk;
+}
+
 int ReadGenerationView(const nwg_runtime *rt, GenerationView *out) {
     if (rt == nullptr || out == nullptr) {
         return kInvalidRuntimeConfig;
@@ -845,35 +880,20 @@ int nwg_upload_catalog(const uint8_t *letters, size_t word_count) {
         }
     }
     std::lock_guard<std::mutex> lock(g_catalog_mutex);
-    const std::size_t pad = ((word_count + 127) / 128) * 128;
-    std::vector<std::uint32_t> codes(pad, 0);
-    std::vector<float> fixed(static_cast<std::size_t>(kFixedDim) * pad, 0.0f);
-    for (std::size_t w = 0; w < word_count; ++w) {
-        codes[w] = PackWord(letters + kWordLength * w);
-        int counts[kAlphabet] = {0};
-        for (int p = 0; p < kWordLength; ++p) {
-            ++counts[letters[kWordLength * w + p]];
-        }
-        // output_embedding.hpp:59-73: letter count, or -1 when the letter is absent
-        for (int l = 0; l < kFixedDim; ++l) {
-            fixed[static_cast<std::size_t>(l) * pad + w] = counts[l] == 0 ? -1.0f : static_cast<float>(counts[l]);
-        }
-    }
     if (g_catalog.codes != nullptr) {
         cudaFree(g_catalog.codes);
         cudaFree(g_catalog.fixed_t);
         g_catalog = Catalog{};
     }
-    if (cudaMalloc(&g_catalog.codes, pad * sizeof(std::uint32_t)) != cudaSuccess ||
-        cudaMalloc(&g_catalog.fixed_t, fixed.size() * sizeof(float)) != cudaSuccess ||
-        cudaMemcpy(g_catalog.codes, codes.data(), pad * sizeof(std::uint32_t), cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(g_catalog.fixed_t, fixed.data(), fixed.size() * sizeof(float), cudaMemcpyHostToDevice) !=
-            cudaSuccess) {
-        return kCudaFailure;
+    std::vector<std::uint32_t> host_codes;
+    const int st = BuildCatalogTables(letters, word_count, &g_catalog.codes, &g_catalog.fixed_t, &g_catalog.pad,
+                                      &host_codes);
+    if (st != kOk) {
+        g_catalog = Catalog{};
+        return st;
     }
     g_catalog.count = word_count;
-    g_catalog.pad = pad;
-    g_catalog.host_codes.assign(codes.begin(), codes.begin() + static_cast<std::ptrdiff_t>(word_count));
+    g_catalog.host_codes = std::move(host_codes);
     cudaGetDevice(&g_catalog.device);
     return kOk;
 }

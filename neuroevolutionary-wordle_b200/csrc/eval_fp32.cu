@@ -367,7 +367,87 @@ __global__ void SummarizeKernel(const float *fitness, const std::uint8_t *has_fi
     }
 }
 
+// Single-model inference (inference/single_model_device_runtime.cu:53-87, dynamic_policy.hpp:67-151): the next
+// guess of one genome for caller-given grids. The reference runs one grid per warp through its FP32 warp scorer,
+// whatever the action count; here a CTA takes a chunk of up to 128 grids that share a turn count and runs the plain
+// form's encoder, trunk and FP32 scoring (ScoreFp32, never the small-action tensor-tile path), so index and score
+// are the reference's chains bit for bit. The winner's score is its 64-term chain recomputed in the scorer's
+// order (zero start, inputs ascending).
+__global__ void __launch_bounds__(kEvalThreads, 2) SingleModelSelectKernel(const SingleModelParams q) {
+    extern __shared__ __align__(16) float arena[];
+    __shared__ ChunkState st;
+    const int tid = threadIdx.x;
+    EvalParams p{};  // no trace
+    p.action_count = q.action_count;
+    p.codes = q.codes;
+    p.fixed_t = q.fixed_t;
+    p.action_pad = q.action_pad;
+    float *scratch = q.scratch + static_cast<std::size_t>(blockIdx.x) * kScratchFloats;
+    const __half *gh = reinterpret_cast<const __half *>(q.genome);
+    const __half *tail = reinterpret_cast<const __half *>(q.genome + kTailOffsetBytes);
+    for (int ck = blockIdx.x; ck < q.chunk_count; ck += gridDim.x) {
+        const int4 c = q.chunks[ck];
+        const int turns = c.x;
+        const int begin = c.y;
+        const int grids = c.z;
+        if (tid < kChunkGames) {
+            const int g = tid;
+            const std::uint32_t grid = g < grids ? q.order[begin + g] : 0u;
+            for (int u = 0; u < kMaxTurns; ++u) {
+                const bool live = g < grids && u < turns;
+                st.guess[u][g] = live ? q.guess_codes[grid * 5 + u] : 0u;
+                st.tiles[u][g] = live ? q.tiles[grid * 5 + u] : std::uint16_t{0};
+            }
+        }
+        for (int idx = tid; idx < kScratchFloats / 4; idx += kEvalThreads) {
+            const float b = H2F(gh, kTrB1 + (idx * 4) / kChunkGames);
+            reinterpret_cast<float4 *>(scratch)[idx] = make_float4(b, b, b, b);
+        }
+        __syncthreads();
+        for (int u = 0; u < turns; ++u) {
+            EncodeRound(st, gh, arena, scratch, u);
+        }
+        TrunkForward(p, st, gh, arena, scratch, turns, 0, 0);
+        ScoreFp32(p, st, gh, arena, turns);
+        if (tid < grids) {
+            const int g = tid;
+            const int a = st.best[g];
+            float s = 0.0f;
+            if (a >= 0) {
+                for (int k = 0; k < 64; ++k) {
+                    const float e = k < kFixedDim ? p.fixed_t[static_cast<std::size_t>(k) * p.action_pad + a]
+                                                  : __half2float(tail[static_cast<std::size_t>(a) * kTailDim +
+                                                                      (k - kFixedDim)]);
+                    s = __fmaf_rn(arena[k * kLd + g], e, s);
+                }
+            }
+            const std::uint32_t grid = q.order[begin + g];
+            q.best_index[grid] = a;
+            q.best_score[grid] = s;
+        }
+        __syncthreads();
+    }
+}
+
 }  // namespace
+
+cudaError_t LaunchSingleModelSelect(const SingleModelParams &params, int cta_count, cudaStream_t stream) {
+    static bool configured = false;
+    if (!configured) {
+        const cudaError_t e = cudaFuncSetAttribute(SingleModelSelectKernel,
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   kArenaFloats * static_cast<int>(sizeof(float)));
+        if (e != cudaSuccess) {
+            return e;
+        }
+        configured = true;
+    }
+    if (cta_count <= 0 || params.chunk_count <= 0) {
+        return cudaSuccess;
+    }
+    SingleModelSelectKernel<<<cta_count, kEvalThreads, kArenaFloats * sizeof(float), stream>>>(params);
+    return cudaGetLastError();
+}
 
 std::size_t EvalScratchFloatsPerCta() { return kScratchFloats; }
 

@@ -5,6 +5,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <vector>
 
 #include "../../include/nwg_capi.h"
 #include "nwg_layout.cuh"
@@ -193,6 +194,28 @@ struct GenerationView {
     std::size_t generation_index, generation_size, planned_children;
 };
 int ReadGenerationView(const nwg_runtime *rt, GenerationView *out);
+
+// Device catalog tables: packed words [pad] and fixed word features [26][pad], pad = word count rounded up to 128.
+int BuildCatalogTables(const std::uint8_t *letters, std::size_t word_count, std::uint32_t **codes_out,
+                       float **fixed_out, std::size_t *pad_out, std::vector<std::uint32_t> *host_codes);
+
+// Single-model inference (eval_fp32.cu): grids grouped in chunks of up to 128 with one turn count each.
+struct SingleModelParams {
+    const std::uint8_t *genome;      // one genome image
+    std::uint32_t action_count;
+    const std::uint32_t *codes;      // the model's catalog
+    const float *fixed_t;
+    std::uint32_t action_pad;
+    const std::uint32_t *guess_codes;  // [grid][5 turns]
+    const std::uint16_t *tiles;        // [grid][5 turns]
+    const int4 *chunks;                // {turns, first entry of order, grids, 0}
+    const std::uint32_t *order;        // grid indices, grouped by turn count
+    int chunk_count;
+    float *scratch;                    // per CTA: layer-1 accumulators
+    std::int32_t *best_index;          // [grid]; -1 when every action is masked
+    float *best_score;                 // [grid]
+};
+cudaError_t LaunchSingleModelSelect(const SingleModelParams &params, int cta_count, cudaStream_t stream);
 
 // A runtime with explicit sizes (a restored checkpoint's, slab_runtime.cu:1746-1765).
 struct RuntimeShape {

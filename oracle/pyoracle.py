@@ -299,6 +299,8 @@ def ref_ckpt() -> C.CDLL | None:
     L.refconv_plan.argtypes = [_sz, _sz, C.c_uint32, _sz, C.c_void_p, C.POINTER(_sz), C.c_void_p, C.POINTER(_sz),
                                C.c_void_p, C.POINTER(_sz)]
     L.refconv_metrics.argtypes = [C.c_void_p, _sz, _sz, C.c_void_p, _sz, C.c_void_p]
+    L.refsm_select_many.argtypes = [C.c_void_p, _sz, C.c_void_p, _sz, C.c_void_p, C.c_void_p, C.c_void_p, _sz,
+                                    C.c_void_p, C.c_void_p, C.c_void_p]
     L.refckpt_runtime_resume.argtypes = [C.c_char_p, C.c_void_p, _sz, C.c_void_p, _sz, C.POINTER(_sz),
                                          C.POINTER(_sz)]
     return L

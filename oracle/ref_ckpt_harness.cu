@@ -10,6 +10,8 @@
 //                          TryDownloadBoundaryCheckpointPayload uses (slab_runtime.cu:1283-1297)
 //   refart_write / refart_read TryWriteWinnerArtifactToPaths / TryReadWinnerArtifact (model_artifact/)
 //   refconv_plan / refconv_metrics MakeSamplePlan / TryComputeMetrics (genetic_algorithm/genetic_convergence.hpp)
+//   refsm_select_many      TryCreateSingleModelDeviceRuntime + TrySelectNextGuessWithSingleModelDeviceRuntime per
+//                          grid (GPU)
 // Device entry points (drive the reference's whole runtime on the GPU):
 //   refckpt_runtime_capture create, bootstrap, TryCreatePrebreedingCheckpointOnDevice, write
 //   refckpt_runtime_evaluate create, bootstrap, TryEvaluateCurrentGenerationFitnessOnDevice, fitness arrays
@@ -22,6 +24,7 @@
 #include "model_artifact/winner_artifact.cpp"
 #include "model_artifact/winner_artifact_reader.cpp"
 #include "genetic_algorithm/genetic_convergence.hpp"
+#include "inference/single_model_device_runtime.cu"
 
 #include <cstring>
 #include <random>
@@ -267,6 +270,41 @@ int refconv_metrics(const float *values, std::size_t organisms, std::size_t weig
     out[3] = m.pairwise_distance_mean;
     out[4] = m.pairwise_distance_min;
     out[5] = m.pairwise_distance_max;
+    return 1;
+}
+
+// grids: guesses[n][6][5], feedback[n][6][5] (0 green, 1 yellow, 2 grey), turns[n]; per grid the reference's
+// status, action index and score.
+int refsm_select_many(const std::uint8_t *genome, std::size_t genome_bytes, const std::uint8_t *letters,
+                      std::size_t catalog_count, const std::uint8_t *guesses, const std::uint8_t *feedback,
+                      const std::uint8_t *turns, std::size_t n, int *status, std::uint64_t *index, float *score) {
+    namespace inf = neuroevolution::inference;
+    namespace wd = neuroevolution::wordle;
+    static tf::TrainingWordCatalog catalog{};
+    if (!MakeCatalog(letters, catalog_count, catalog)) {
+        return 0;
+    }
+    inf::SingleModelDeviceRuntime runtime{};
+    if (!inf::TryCreateSingleModelDeviceRuntime(genome, genome_bytes, catalog, runtime)) {
+        return 0;
+    }
+    for (std::size_t g = 0; g < n; ++g) {
+        wd::WordleGrid grid{};
+        grid.turn_count = turns[g];
+        for (std::size_t u = 0; u < turns[g] && u < wd::kMaxTurnCount; ++u) {
+            for (std::size_t k = 0; k < 5; ++k) {
+                grid.turns[u].guess.letter_indices[k] = guesses[(g * 6 + u) * 5 + k];
+                grid.turns[u].feedback.values[k] = static_cast<wd::TileFeedback>(feedback[(g * 6 + u) * 5 + k]);
+            }
+        }
+        neuroevolution::model::output_embedding::SelectedAction action{};
+        inf::SingleModelDeviceRuntimeStatusCode st = inf::SingleModelDeviceRuntimeStatusCode::kInvalidRuntime;
+        (void)inf::TrySelectNextGuessWithSingleModelDeviceRuntime(runtime, grid, action, &st);
+        status[g] = static_cast<int>(st);
+        index[g] = action.action_index;
+        score[g] = action.score;
+    }
+    inf::DestroySingleModelDeviceRuntime(runtime);
     return 1;
 }
 
