@@ -232,6 +232,11 @@ int nwg_read_summary(const nwg_runtime *runtime, nwg_fitness_summary *summary);
 
 int nwg_read_evaluation_stats(const nwg_runtime *runtime, nwg_evaluation_stats *stats);
 
+/* Solve rate of each individual of the last evaluation: games won / games played (3 per local word), and their
+ * mean. No reference counterpart (the reference reports fitness only). rates may be NULL. */
+int nwg_read_solve_rates(const nwg_runtime *runtime, float *rates, size_t capacity, size_t *count_out,
+                         double *mean_out);
+
 /* TryAdvanceGenerationOnDevice (slab_runtime.hpp:144-150): evaluate, select, breed, mutate, swap.
  * config and pending may be NULL (reference defaults); callbacks may be NULL. */
 int nwg_advance(nwg_runtime *runtime, uint32_t generation_seed, const nwg_runtime_word_counts *counts,
@@ -469,6 +474,40 @@ int nwg_single_model_set_stream(nwg_single_model *model, void *cuda_stream);
  * (its action zeroed, the others filled). */
 int nwg_single_model_select(nwg_single_model *model, const uint8_t *guess_letters, const uint8_t *feedback,
                             const uint8_t *turn_counts, size_t grid_count, nwg_selected_action *actions);
+
+/* The learned surrogate's network (no reference counterpart): an MLP 8,192 -> 512 -> 128 -> 1 with GELU, BF16
+ * weights in the products, FP32 masters, FP32 accumulation, Adam (lr given, beta 0.9 / 0.999, eps 1e-8). Inputs are
+ * device buffers of BF16 descriptors, [rows][8192], rows a multiple of 128 (NWG_UNSUPPORTED otherwise) and at most
+ * the capacity given at creation. Parameters are one flat FP32 vector: W1 [512][8192], b1, W2 [128][512], b2,
+ * w3 [128], b3. */
+typedef struct nwg_mlp nwg_mlp;
+int nwg_mlp_create(size_t capacity_rows, uint32_t seed, float learning_rate, nwg_mlp **out);
+void nwg_mlp_destroy(nwg_mlp *mlp);
+int nwg_mlp_set_stream(nwg_mlp *mlp, void *cuda_stream);
+size_t nwg_mlp_parameter_count(void);
+/* Copies the parameters out to host_out and/or in from host_in (either may be NULL). */
+int nwg_mlp_parameters(nwg_mlp *mlp, float *host_out, const float *host_in);
+/* y (device, rows floats) = the network's outputs. */
+int nwg_mlp_forward(nwg_mlp *mlp, const uint16_t *x, size_t rows, float *y);
+/* Gradients of mean((y - t)^2) (t: device targets) into grads_out (host, parameter_count floats; may be NULL) and
+ * the loss; no update. */
+int nwg_mlp_gradients(nwg_mlp *mlp, const uint16_t *x, const float *targets, size_t rows, float *grads_out,
+                      float *loss_out);
+/* One Adam step on mean((y - t)^2). */
+int nwg_mlp_train_step(nwg_mlp *mlp, const uint16_t *x, const float *targets, size_t rows);
+
+/* Behavioural descriptors (no reference counterpart): for each of count genomes (device slab, slot indices on the
+ * device), its FP32 policy vectors on the 128 probe states, times scale, rounded to BF16, into out[count][8192]
+ * (device). Probe p has probe_turns[p] <= 4 turns, guess and tiles of turn u at probe_letters / probe_feedback
+ * [(p * 4 + u) * 5 ..] (host arrays). Synchronises the stream. */
+int nwg_descriptors(const void *slab, size_t pitch, const uint32_t *slots, size_t count, const uint8_t *probe_letters,
+                    const uint8_t *probe_feedback, const uint8_t *probe_turns, float scale, uint16_t *out,
+                    void *cuda_stream);
+
+/* Test hook: C[m][n] FP32 = A[m][k] . B[n][k]^T on tcgen05 (BF16 device operands, K contiguous); m % 128, n % 256,
+ * k % 64, lda % 8, ldb % 8 and ldc % 4 zero, bases 16-byte aligned (NWG_UNSUPPORTED otherwise). */
+int nwg_bf16_gemm_nt(const void *a, size_t lda, const void *b, size_t ldb, float *c, size_t ldc, size_t m, size_t n,
+                     size_t k, void *cuda_stream);
 
 /* SwapDeviceSlabGenerationBuffers (slab_runtime.hpp:181). */
 int nwg_swap_generations(nwg_runtime *runtime);

@@ -171,6 +171,9 @@ EXPORTS = [
     "nwg_winner_artifact_read", "nwg_download_next_generation", "nwg_fitness_telemetry_collect",
     "nwg_convergence_telemetry_collect", "nwg_convergence_sample_plan", "nwg_maybe_release_training_shard",
     "nwg_single_model_create", "nwg_single_model_destroy", "nwg_single_model_set_stream", "nwg_single_model_select",
+    "nwg_read_solve_rates", "nwg_mlp_create", "nwg_mlp_destroy", "nwg_mlp_set_stream", "nwg_mlp_parameter_count",
+    "nwg_mlp_parameters", "nwg_mlp_forward", "nwg_mlp_gradients", "nwg_mlp_train_step", "nwg_bf16_gemm_nt",
+    "nwg_descriptors",
 ]
 
 
@@ -231,6 +234,18 @@ def lib() -> C.CDLL:
     L.nwg_single_model_destroy.restype = None
     L.nwg_single_model_set_stream.argtypes = [_vp, _vp]
     L.nwg_single_model_select.argtypes = [_vp, _vp, _vp, _vp, _sz, C.POINTER(SelectedAction)]
+    L.nwg_read_solve_rates.argtypes = [_vp, _vp, _sz, C.POINTER(_sz), C.POINTER(C.c_double)]
+    L.nwg_mlp_create.argtypes = [_sz, C.c_uint32, C.c_float, C.POINTER(_vp)]
+    L.nwg_mlp_destroy.argtypes = [_vp]
+    L.nwg_mlp_destroy.restype = None
+    L.nwg_mlp_set_stream.argtypes = [_vp, _vp]
+    L.nwg_mlp_parameter_count.restype = _sz
+    L.nwg_mlp_parameters.argtypes = [_vp, _vp, _vp]
+    L.nwg_mlp_forward.argtypes = [_vp, _vp, _sz, _vp]
+    L.nwg_mlp_gradients.argtypes = [_vp, _vp, _vp, _sz, _vp, C.POINTER(C.c_float)]
+    L.nwg_mlp_train_step.argtypes = [_vp, _vp, _vp, _sz]
+    L.nwg_bf16_gemm_nt.argtypes = [_vp, _sz, _vp, _sz, _vp, _sz, _sz, _sz, _sz, _vp]
+    L.nwg_descriptors.argtypes = [_vp, _sz, _vp, _sz, _vp, _vp, _vp, C.c_float, _vp, _vp]
     L.nwg_swap_generations.argtypes = [_vp]
     L.nwg_read_status.argtypes = [_vp, C.POINTER(C.c_int)]
     L.nwg_download_current_generation.argtypes = [_vp, _vp, _vp, _vp, _vp, _sz, C.POINTER(_sz), C.POINTER(_sz)]
@@ -447,6 +462,15 @@ class Runtime:
                                                      C.byref(nxt), C.byref(f), C.byref(c)),
               "nwg_maybe_release_training_shard")
         return pending, nxt.value, f, c
+
+    def solve_rates(self):
+        """Per-individual solve rate of the last evaluation (games won / games played) and their mean."""
+        rates = np.zeros(self.population, np.float32)
+        n = _sz()
+        mean = C.c_double()
+        check(lib().nwg_read_solve_rates(self.handle, _np_ptr(rates), rates.size, C.byref(n), C.byref(mean)),
+              "nwg_read_solve_rates")
+        return rates[:n.value], mean.value
 
     def resume(self) -> None:
         """TryResumeGenerationFromCheckpointOnDevice: assemble a restored boundary."""
@@ -673,4 +697,64 @@ class SingleModel:
         index = np.array([out[i].action_index for i in range(n)], np.int64)
         score = np.array([out[i].score for i in range(n)], np.float32)
         return index, score
+
+
+def bf16_gemm_nt(a_ptr: int, lda: int, b_ptr: int, ldb: int, c_ptr: int, ldc: int, m: int, n: int, k: int,
+                 stream: int = 0) -> None:
+    """C[m][n] = A[m][k] . B[n][k]^T on tcgen05 (device pointers; BF16 operands, FP32 output)."""
+    check(lib().nwg_bf16_gemm_nt(a_ptr, lda, b_ptr, ldb, c_ptr, ldc, m, n, k, stream or None), "nwg_bf16_gemm_nt")
+
+
+def descriptors(slab_ptr: int, pitch: int, slots_ptr: int, count: int, probe_letters: np.ndarray,
+                probe_feedback: np.ndarray, probe_turns: np.ndarray, scale: float, out_ptr: int,
+                stream: int = 0) -> None:
+    """Behavioural descriptors of count genomes on 128 probes (probe arrays [128][4][5], [128][4][5], [128])."""
+    letters = np.ascontiguousarray(probe_letters, np.uint8)
+    fb = np.ascontiguousarray(probe_feedback, np.uint8)
+    turns = np.ascontiguousarray(probe_turns, np.uint8)
+    check(lib().nwg_descriptors(slab_ptr, pitch, slots_ptr, count, _np_ptr(letters), _np_ptr(fb), _np_ptr(turns),
+                                scale, out_ptr, stream or None), "nwg_descriptors")
+
+
+class Mlp:
+    """The surrogate network (nwg_mlp): 8,192 -> 512 -> 128 -> 1, GELU, BF16 products, FP32 masters, Adam."""
+
+    def __init__(self, capacity_rows: int, seed: int = 0, learning_rate: float = 1e-3):
+        handle = _vp()
+        check(lib().nwg_mlp_create(capacity_rows, seed, learning_rate, C.byref(handle)), "nwg_mlp_create")
+        self.handle = handle
+        self.count = lib().nwg_mlp_parameter_count()
+
+    def close(self):
+        if self.handle:
+            lib().nwg_mlp_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def parameters(self) -> np.ndarray:
+        out = np.zeros(self.count, np.float32)
+        check(lib().nwg_mlp_parameters(self.handle, _np_ptr(out), None), "nwg_mlp_parameters")
+        return out
+
+    def set_parameters(self, values: np.ndarray) -> None:
+        v = np.ascontiguousarray(values, np.float32)
+        check(lib().nwg_mlp_parameters(self.handle, None, _np_ptr(v)), "nwg_mlp_parameters")
+
+    def forward(self, x_ptr: int, rows: int, y_ptr: int) -> None:
+        check(lib().nwg_mlp_forward(self.handle, x_ptr, rows, y_ptr), "nwg_mlp_forward")
+
+    def gradients(self, x_ptr: int, t_ptr: int, rows: int):
+        g = np.zeros(self.count, np.float32)
+        loss = C.c_float()
+        check(lib().nwg_mlp_gradients(self.handle, x_ptr, t_ptr, rows, _np_ptr(g), C.byref(loss)),
+              "nwg_mlp_gradients")
+        return g, loss.value
+
+    def train_step(self, x_ptr: int, t_ptr: int, rows: int) -> None:
+        check(lib().nwg_mlp_train_step(self.handle, x_ptr, t_ptr, rows), "nwg_mlp_train_step")
 

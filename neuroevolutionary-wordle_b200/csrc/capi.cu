@@ -70,7 +70,7 @@ struct nwg_runtime {
     std::size_t shard_count = 0;
     std::uint32_t *cell_offsets = nullptr, *cell_words = nullptr;
     std::size_t cell_count = 0, cell_word_capacity = 0;
-    std::uint32_t *local_words = nullptr, *chunk_start = nullptr, *score_sum = nullptr;
+    std::uint32_t *local_words = nullptr, *chunk_start = nullptr, *score_sum = nullptr, *won_sum = nullptr;
     unsigned long long *steps = nullptr;
     float *scratch = nullptr;
     int scratch_ctas = 0;
@@ -362,6 +362,7 @@ void FreeRuntime(nwg_runtime *rt) {
                            rt->cur_eval,   rt->next_eval,    rt->cur_has,     rt->next_has,    rt->pairs,
                            rt->slot_used,  rt->status,       rt->summary,     rt->shards,      rt->cell_offsets,
                            rt->cell_words, rt->local_words,  rt->chunk_start, rt->score_sum,   rt->steps,
+                           rt->won_sum,
                            rt->scratch,    rt->tc_tables,    rt->trunk_tables};
     for (void *p : device_ptrs) {
         if (p != nullptr) {
@@ -435,6 +436,7 @@ int EvaluateImpl(nwg_runtime *rt, const nwg_runtime_word_counts *counts, const n
     NWG_TRY(cudaMemsetAsync(rt->cur_eval, 0, rt->max_generation_size * sizeof(std::uint32_t), rt->stream));
     NWG_TRY(cudaMemsetAsync(rt->cur_has, 0, rt->max_generation_size, rt->stream));
     NWG_TRY(cudaMemsetAsync(rt->steps, 0, kStepCounters * sizeof(unsigned long long), rt->stream));
+    NWG_TRY(cudaMemsetAsync(rt->won_sum, 0, population * sizeof(std::uint32_t), rt->stream));
     NWG_TRY(LaunchEvalPrepare(src, population, static_cast<std::uint32_t>(g_catalog.count), rt->local_words,
                               rt->chunk_start, rt->score_sum, rt->status, rt->stream));
     EvalParams p{};
@@ -452,6 +454,7 @@ int EvaluateImpl(nwg_runtime *rt, const nwg_runtime_word_counts *counts, const n
     p.local_words = rt->local_words;
     p.scratch = rt->scratch;
     p.score_sum = rt->score_sum;
+    p.won_sum = rt->won_sum;
     p.steps = rt->steps;
     p.status = rt->status;
     p.trace_episodes = static_cast<std::uint32_t>(trace_episodes);
@@ -699,6 +702,7 @@ int CreateShapedRuntime(const RuntimeShape &shape, nwg_runtime **out) {
     alloc(&rt->local_words, max_gen * sizeof(std::uint32_t));
     alloc(&rt->chunk_start, (max_gen + 1) * sizeof(std::uint32_t));
     alloc(&rt->score_sum, max_gen * sizeof(std::uint32_t));
+    alloc(&rt->won_sum, max_gen * sizeof(std::uint32_t));
     alloc(&rt->steps, kStepCounters * sizeof(unsigned long long));
     alloc(&rt->scratch, static_cast<std::size_t>(rt->scratch_ctas) * EvalScratchFloatsPerCta() * sizeof(float));
     ok = ok && cudaMallocHost(&rt->host_shards, NWG_CATALOG_CAPACITY * sizeof(ShardRecord)) == cudaSuccess;
@@ -1117,6 +1121,39 @@ int nwg_read_evaluation_stats(const nwg_runtime *rt, nwg_evaluation_stats *stats
     stats->fitness_variance_fp64 = rt->host_summary->variance_fp64;
     float ms = 0.0f;
     stats->eval_kernel_ms = cudaEventElapsedTime(&ms, rt->eval_begin, rt->eval_end) == cudaSuccess ? ms : -1.0;
+    return kOk;
+}
+
+int nwg_read_solve_rates(const nwg_runtime *rt, float *rates, size_t capacity, size_t *count_out,
+                         double *mean_out) {
+    if (rt == nullptr || rt->last_eval_population == 0 || rt->last_eval_population != rt->cur_gen_size) {
+        return kPopulationNotEvaluated;
+    }
+    const std::size_t n = rt->cur_gen_size;
+    if (rates != nullptr && capacity < n) {
+        return kInvalidGeneration;
+    }
+    std::vector<std::uint32_t> won(n), words(n);
+    if (cudaStreamSynchronize(rt->stream) != cudaSuccess ||
+        cudaMemcpy(won.data(), rt->won_sum, n * 4, cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(words.data(), rt->local_words, n * 4, cudaMemcpyDeviceToHost) != cudaSuccess) {
+        return kCudaFailure;
+    }
+    double total = 0.0;
+    for (std::size_t i = 0; i < n; ++i) {
+        const double games = 3.0 * static_cast<double>(words[i]);  // three episodes per local word
+        const double rate = games > 0.0 ? static_cast<double>(won[i]) / games : 0.0;
+        if (rates != nullptr) {
+            rates[i] = static_cast<float>(rate);
+        }
+        total += rate;
+    }
+    if (count_out != nullptr) {
+        *count_out = n;
+    }
+    if (mean_out != nullptr) {
+        *mean_out = total / static_cast<double>(n);
+    }
     return kOk;
 }
 

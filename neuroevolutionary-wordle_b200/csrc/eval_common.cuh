@@ -254,7 +254,9 @@ __device__ __forceinline__ int CountActive(ChunkState &st) {
 }
 
 // Encodes turn t of every game (10-column gather, ReLU, 128 -> 64) and appends its 64 inputs to the
-// layer-1 chains held in scratch ([256 outputs][128 games]).
+// layer-1 chains held in scratch ([256 outputs][128 games]). With kMaskByTurns the games of a chunk may have
+// different turn counts (st.turns): a game without turn t appends zeros, which leaves its chains unchanged.
+template <bool kMaskByTurns = false>
 __device__ __forceinline__ void EncodeRound(ChunkState &st, const __half *gh, float *arena, float *scratch, int t) {
     const int tid = threadIdx.x;
     const int ty = tid >> 4;
@@ -309,9 +311,10 @@ __device__ __forceinline__ void EncodeRound(ChunkState &st, const __half *gh, fl
     float *enc = arena;  // [64][kLd] encoded turn, k-major
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
+        const bool live = !kMaskByTurns || t < st.turns[RowOf(ty, i)];
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-            enc[(tx * 4 + j) * kLd + RowOf(ty, i)] = acc[i][j];
+            enc[(tx * 4 + j) * kLd + RowOf(ty, i)] = live ? acc[i][j] : 0.0f;
         }
     }
     // trunk layer 1: chains continue with inputs 1 + 64t .. 64 + 64t
@@ -509,11 +512,16 @@ __device__ __forceinline__ void FinishChunk(const EvalParams &p, ChunkState &st,
                 }
             }
         }
+        std::uint32_t won = st.episode[g] >= 0 && st.won[g] ? 1u : 0u;
         for (int off = 16; off > 0; off >>= 1) {
             score += __shfl_xor_sync(0xffffffffu, score, off);
+            won += __shfl_xor_sync(0xffffffffu, won, off);
         }
         if ((tid & 31) == 0 && score != 0) {
             atomicAdd(p.score_sum + ind, score);
+        }
+        if ((tid & 31) == 0 && won != 0 && p.won_sum != nullptr) {
+            atomicAdd(p.won_sum + ind, won);
         }
     }
     __syncthreads();

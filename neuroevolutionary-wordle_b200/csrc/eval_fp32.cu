@@ -18,6 +18,7 @@
 // and the trunk's first layer keeps its running accumulator from turn to turn (a new turn appends
 // its 64 inputs to the end of the chain). Ties in the argmax go to the lowest action index, and
 // guessed words are masked by word equality, as in the reference.
+#include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <mma.h>
 
@@ -429,7 +430,68 @@ __global__ void __launch_bounds__(kEvalThreads, 2) SingleModelSelectKernel(const
     }
 }
 
+// Behavioural descriptors of a brood: each genome's policy on the 128 probe states, all in one chunk although the
+// probes have 0..4 turns (EncodeRound<true> appends zeros for absent turns; a virgin probe's layer-1 chains start
+// from the bias plus its virgin-flag weight, which is what the t = 0 path of TrunkForward computes). The probes'
+// guesses and tiles are loaded once per CTA; each genome then costs four encode rounds and one trunk pass.
+__global__ void __launch_bounds__(kEvalThreads, 2) DescriptorKernel(const DescriptorParams q) {
+    extern __shared__ __align__(16) float arena[];
+    __shared__ ChunkState st;
+    const int tid = threadIdx.x;
+    EvalParams p{};  // no trace
+    float *scratch = q.scratch + static_cast<std::size_t>(blockIdx.x) * kScratchFloats;
+    if (tid < kProbeStates) {
+        st.turns[tid] = q.probe_turns[tid];
+        for (int u = 0; u < kMaxTurns; ++u) {
+            const bool live = u < kProbeMaxTurns && u < q.probe_turns[tid];
+            st.guess[u][tid] = live ? q.probe_codes[tid * kProbeMaxTurns + u] : 0u;
+            st.tiles[u][tid] = live ? q.probe_tiles[tid * kProbeMaxTurns + u] : std::uint16_t{0};
+        }
+    }
+    __syncthreads();
+    for (std::uint32_t g = blockIdx.x; g < q.count; g += gridDim.x) {
+        const __half *gh = reinterpret_cast<const __half *>(q.slab + static_cast<std::size_t>(q.slots[g]) * q.pitch);
+        for (int idx = tid; idx < kScratchFloats; idx += kEvalThreads) {
+            const int o = idx / kChunkGames;
+            const int probe = idx - o * kChunkGames;
+            const float b = H2F(gh, kTrB1 + o);
+            scratch[idx] = st.turns[probe] == 0 ? __fmaf_rn(H2F(gh, kTrW1 + o * kModelInput), 1.0f, b) : b;
+        }
+        __syncthreads();
+        for (int u = 0; u < kProbeMaxTurns; ++u) {
+            EncodeRound<true>(st, gh, arena, scratch, u);
+        }
+        TrunkForward(p, st, gh, arena, scratch, 1, 0, 0);
+        std::uint16_t *row = q.out + static_cast<std::size_t>(g) * q.out_ld;
+        for (int idx = tid; idx < kDescriptorWidth / 2; idx += kEvalThreads) {
+            const int probe = (2 * idx) >> 6;
+            const int k = (2 * idx) & 63;
+            const __nv_bfloat162 v = __floats2bfloat162_rn(arena[k * kLd + probe] * q.scale,
+                                                           arena[(k + 1) * kLd + probe] * q.scale);
+            reinterpret_cast<__nv_bfloat162 *>(row)[idx] = v;
+        }
+        __syncthreads();
+    }
+}
+
 }  // namespace
+
+cudaError_t LaunchDescriptors(const DescriptorParams &params, int cta_count, cudaStream_t stream) {
+    static bool configured = false;
+    if (!configured) {
+        const cudaError_t e = cudaFuncSetAttribute(DescriptorKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   kArenaFloats * static_cast<int>(sizeof(float)));
+        if (e != cudaSuccess) {
+            return e;
+        }
+        configured = true;
+    }
+    if (cta_count <= 0 || params.count == 0) {
+        return cudaSuccess;
+    }
+    DescriptorKernel<<<cta_count, kEvalThreads, kArenaFloats * sizeof(float), stream>>>(params);
+    return cudaGetLastError();
+}
 
 cudaError_t LaunchSingleModelSelect(const SingleModelParams &params, int cta_count, cudaStream_t stream) {
     static bool configured = false;

@@ -70,6 +70,7 @@ struct EvalParams {
     const std::uint32_t *local_words; // [population]
     float *scratch;                   // per CTA: kChunkGames x 256 layer-1 accumulators
     std::uint32_t *score_sum;         // [population]
+    std::uint32_t *won_sum;           // [population] games won (may be null)
     unsigned long long *steps;        // [0] policy decisions, [1] turns encoded, [2] episodes
     int *status;
     // optional trace (null when unused)
@@ -216,6 +217,32 @@ struct SingleModelParams {
     float *best_score;                 // [grid]
 };
 cudaError_t LaunchSingleModelSelect(const SingleModelParams &params, int cta_count, cudaStream_t stream);
+
+// Behavioural descriptors (eval_fp32.cu): each genome's FP32 policy vectors on 128 fixed probe states of 0..4
+// turns, scaled and rounded to BF16, row g of the output = [probe][64] of genome g.
+constexpr int kProbeStates = 128;
+constexpr int kProbeMaxTurns = 4;
+constexpr int kDescriptorWidth = kProbeStates * 64;  // 8,192
+struct DescriptorParams {
+    const std::uint8_t *slab;
+    std::size_t pitch;
+    const std::uint32_t *slots;        // genome g at slab + slots[g] * pitch
+    std::uint32_t count;
+    const std::uint32_t *probe_codes;  // [probe][4] packed guesses
+    const std::uint16_t *probe_tiles;  // [probe][4] packed feedback
+    const std::uint8_t *probe_turns;   // [probe]
+    float scale;                       // applied before the BF16 rounding
+    float *scratch;                    // per CTA: layer-1 accumulators
+    std::uint16_t *out;                // [count][8192] BF16 bits, row stride out_ld elements
+    std::size_t out_ld;
+};
+cudaError_t LaunchDescriptors(const DescriptorParams &params, int cta_count, cudaStream_t stream);
+
+// C[M][N] FP32 = A[M][K] . B[N][K]^T on tcgen05, A and B BF16 with K contiguous (surrogate_mlp.cu). M % 128,
+// N % 256, K % 64, lda % 8, ldb % 8 and ldc % 4 must be zero and the bases 16-byte aligned (cudaErrorInvalidValue
+// otherwise); *error is set to 1 when a bounded wait gave up.
+cudaError_t LaunchGemmNt(const void *a, std::size_t lda, const void *b, std::size_t ldb, float *c, std::size_t ldc,
+                         std::size_t m, std::size_t n, std::size_t k, int *error, cudaStream_t stream);
 
 // A runtime with explicit sizes (a restored checkpoint's, slab_runtime.cu:1746-1765).
 struct RuntimeShape {

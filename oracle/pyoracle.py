@@ -448,3 +448,63 @@ def ref_convergence_metrics(values: np.ndarray, pairs: np.ndarray) -> np.ndarray
     assert ref_ckpt().refconv_metrics(values.ctypes.data, values.shape[0], values.shape[1], p.ctypes.data, len(p),
                                       out.ctypes.data) == 1
     return out
+
+
+# ---- the surrogate network (test infrastructure: an FP64 restatement of csrc/surrogate_mlp.cu) ----
+
+MLP_SHAPES = (("W1", (512, 8192)), ("b1", (512,)), ("W2", (128, 512)), ("b2", (128,)), ("w3", (128,)), ("b3", (1,)))
+
+
+def mlp_unflatten(flat: np.ndarray) -> dict:
+    out, off = {}, 0
+    for name, shape in MLP_SHAPES:
+        n = int(np.prod(shape))
+        out[name] = np.asarray(flat[off:off + n], np.float64).reshape(shape)
+        off += n
+    return out
+
+
+def bf16_round(a: np.ndarray) -> np.ndarray:
+    """Round-to-nearest-even of float32 values to BF16, returned as float32."""
+    bits = np.ascontiguousarray(a, np.float32).view(np.uint32).astype(np.uint64)
+    bits = (bits + 0x7FFF + ((bits >> 16) & 1)) >> 16 << 16
+    return bits.astype(np.uint32).view(np.float32)
+
+
+def _gelu(x):
+    from scipy.special import erf
+
+    return 0.5 * x * (1.0 + erf(x / np.sqrt(2.0)))
+
+
+def _gelu_grad(x):
+    from scipy.special import erf
+
+    return 0.5 * (1.0 + erf(x / np.sqrt(2.0))) + x * np.exp(-0.5 * x * x) / np.sqrt(2.0 * np.pi)
+
+
+def mlp_forward(flat: np.ndarray, x: np.ndarray, bf16_w1: bool = True) -> tuple[np.ndarray, dict]:
+    """y = b3 + w3 . gelu(b2 + W2 gelu(b1 + W1 x)) in FP64; W1 rounded to BF16 as the device products use it."""
+    p = mlp_unflatten(flat)
+    w1 = bf16_round(p["W1"].astype(np.float32)).astype(np.float64) if bf16_w1 else p["W1"]
+    x = np.asarray(x, np.float64)
+    z1 = x @ w1.T + p["b1"]
+    a1 = _gelu(z1)
+    z2 = a1 @ p["W2"].T + p["b2"]
+    a2 = _gelu(z2)
+    y = a2 @ p["w3"] + p["b3"][0]
+    return y, dict(x=x, z1=z1, a1=a1, z2=z2, a2=a2)
+
+
+def mlp_gradients(flat: np.ndarray, x: np.ndarray, t: np.ndarray, bf16: bool = True) -> tuple[np.ndarray, float]:
+    """Gradients of mean((y - t)^2) in FP64, flat in the parameter order. With bf16 the first layer's weight
+    gradient uses BF16-rounded dZ1, as the device's tensor-core product does."""
+    p = mlp_unflatten(flat)
+    y, c = mlp_forward(flat, x, bf16)
+    n = len(t)
+    dy = 2.0 * (y - np.asarray(t, np.float64)) / n
+    dz2 = np.outer(dy, p["w3"]) * _gelu_grad(c["z2"])
+    dz1 = (dz2 @ p["W2"]) * _gelu_grad(c["z1"])
+    dz1_w = bf16_round(dz1.astype(np.float32)).astype(np.float64) if bf16 else dz1
+    grads = [dz1_w.T @ c["x"], dz1.sum(0), dz2.T @ c["a1"], dz2.sum(0), dy @ c["a2"], np.array([dy.sum()])]
+    return np.concatenate([g.reshape(-1) for g in grads]), float(np.mean((y - t) ** 2))
