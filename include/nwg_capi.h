@@ -509,6 +509,60 @@ int nwg_descriptors(const void *slab, size_t pitch, const uint32_t *slots, size_
 int nwg_bf16_gemm_nt(const void *a, size_t lda, const void *b, size_t ldb, float *c, size_t ldc, size_t m, size_t n,
                      size_t k, void *cuda_stream);
 
+/* Surrogate-screened generation step (no reference counterpart): each cell breeds candidates_per_cell children, the
+ * network (nwg_mlp) scores their behavioural descriptors (policy vectors on 128 fixed probe states of 0..4 turns),
+ * and only the best-scored child of each cell plus an audit sample is played; every child is played instead while
+ * the network is untrained, while the replay ring holds fewer than warmup_pairs pairs, or when the last audit's
+ * Spearman rank correlation fell below spearman_floor. Played (descriptor, fitness) pairs train the network online
+ * (train_steps Adam steps of batch_rows rows from a replay ring of replay_capacity pairs, targets standardised per
+ * minibatch). The population must have per-cell word lists (nwg_set_cell_words) and keeps its size. */
+typedef struct {
+    size_t candidates_per_cell;   /* 4 */
+    float audit_fraction;         /* 0.05 of the candidates */
+    float spearman_floor;         /* 0.6 */
+    size_t replay_capacity;       /* 65,536 */
+    size_t warmup_pairs;          /* pairs in the ring before screening may start */
+    size_t train_steps;           /* per generation */
+    size_t batch_rows;            /* a multiple of 128 */
+    float learning_rate;          /* Adam; 1e-4 */
+    uint32_t seed;                /* probes, network initialisation, audit and minibatch draws */
+    int evaluation_form;          /* NWG_FORM_* used to play the children (NWG_FORM_TC_TRUNK_FP16) */
+    float margin_tau;             /* its margin guard (trunk forms) */
+} nwg_surrogate_config;
+
+typedef struct {
+    size_t generation;            /* index of the generation installed */
+    size_t candidates;            /* children bred */
+    size_t evaluated;             /* children played */
+    bool screened;                /* false: every child was played */
+    float spearman;               /* audit rank correlation of score and fitness (NaN while untrained) */
+    float train_loss;             /* standardised MSE on the last minibatch */
+    size_t train_steps;
+    size_t replay_size;
+    double mean_fitness;          /* of the new generation */
+    double mean_solve_rate;
+    /* on a step that played every child (NaN otherwise; the model's pick also NaN while untrained): the mean
+     * fitness of the model's best-scored child per cell, of candidate 0 (the plain step's child) and of the truly
+     * best child per cell, all from the same brood */
+    double mean_fitness_model_pick;
+    double mean_fitness_first_candidate;
+    double mean_fitness_best_candidate;
+    uint64_t game_steps;          /* decisions played this step */
+    float ms_select_breed, ms_descriptors, ms_inference, ms_evaluation, ms_training, ms_install, ms_total;
+} nwg_surrogate_stats;
+
+typedef struct nwg_surrogate nwg_surrogate;
+
+/* runtime: the population (evaluated or not, per-cell word lists set); catalog_letters: the uploaded catalog's rows
+ * (probe words); secret_pool: catalog indices the probes' secrets come from (NULL: the selectable words). */
+int nwg_surrogate_create(nwg_runtime *runtime, const nwg_surrogate_config *config, const uint8_t *catalog_letters,
+                         size_t catalog_count, const uint32_t *secret_pool, size_t pool_count,
+                         nwg_surrogate **surrogate_out);
+void nwg_surrogate_destroy(nwg_surrogate *surrogate);
+/* One surrogate-screened step of the population (config: selection radius and exponent, breeding, mutation). */
+int nwg_surrogate_advance(nwg_surrogate *surrogate, uint32_t generation_seed, const nwg_runtime_word_counts *counts,
+                          const nwg_generation_assembly_config *config, nwg_surrogate_stats *stats);
+
 /* SwapDeviceSlabGenerationBuffers (slab_runtime.hpp:181). */
 int nwg_swap_generations(nwg_runtime *runtime);
 

@@ -155,6 +155,33 @@ class SelectedAction(C.Structure):
     _fields_ = [("word", C.c_uint8 * 5), ("score", C.c_float), ("action_index", _sz)]
 
 
+class SurrogateConfig(C.Structure):
+    """nwg_surrogate_config (defaults of the learned-surrogate method)."""
+    _fields_ = [("candidates_per_cell", _sz), ("audit_fraction", C.c_float), ("spearman_floor", C.c_float),
+                ("replay_capacity", _sz), ("warmup_pairs", _sz), ("train_steps", _sz), ("batch_rows", _sz),
+                ("learning_rate", C.c_float), ("seed", C.c_uint32), ("evaluation_form", C.c_int),
+                ("margin_tau", C.c_float)]
+
+    def __init__(self, candidates_per_cell=4, audit_fraction=0.05, spearman_floor=0.6, replay_capacity=65536,
+                 warmup_pairs=8192, train_steps=8, batch_rows=1024, learning_rate=1e-4, seed=0, evaluation_form=4,
+                 margin_tau=1e-3):
+        super().__init__(candidates_per_cell, audit_fraction, spearman_floor, replay_capacity, warmup_pairs,
+                         train_steps, batch_rows, learning_rate, seed, evaluation_form, margin_tau)
+
+
+class SurrogateStats(C.Structure):
+    _fields_ = [("generation", _sz), ("candidates", _sz), ("evaluated", _sz), ("screened", C.c_bool),
+                ("spearman", C.c_float), ("train_loss", C.c_float), ("train_steps", _sz), ("replay_size", _sz),
+                ("mean_fitness", C.c_double), ("mean_solve_rate", C.c_double), ("mean_fitness_model_pick", C.c_double),
+                ("mean_fitness_first_candidate", C.c_double), ("mean_fitness_best_candidate", C.c_double),
+                ("game_steps", C.c_uint64)] + [
+        (n, C.c_float) for n in ("ms_select_breed", "ms_descriptors", "ms_inference", "ms_evaluation", "ms_training",
+                                 "ms_install", "ms_total")]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 POST_FITNESS_FN = C.CFUNCTYPE(C.c_bool, _vp, C.POINTER(RuntimeWordCounts), _vp)
 SHARD_RELEASE_FN = C.CFUNCTYPE(C.c_bool, _vp, C.POINTER(RuntimeWordCounts), C.POINTER(PendingInjection), _vp)
 
@@ -173,7 +200,7 @@ EXPORTS = [
     "nwg_single_model_create", "nwg_single_model_destroy", "nwg_single_model_set_stream", "nwg_single_model_select",
     "nwg_read_solve_rates", "nwg_mlp_create", "nwg_mlp_destroy", "nwg_mlp_set_stream", "nwg_mlp_parameter_count",
     "nwg_mlp_parameters", "nwg_mlp_forward", "nwg_mlp_gradients", "nwg_mlp_train_step", "nwg_bf16_gemm_nt",
-    "nwg_descriptors",
+    "nwg_descriptors", "nwg_surrogate_create", "nwg_surrogate_destroy", "nwg_surrogate_advance",
 ]
 
 
@@ -246,6 +273,11 @@ def lib() -> C.CDLL:
     L.nwg_mlp_train_step.argtypes = [_vp, _vp, _vp, _sz]
     L.nwg_bf16_gemm_nt.argtypes = [_vp, _sz, _vp, _sz, _vp, _sz, _sz, _sz, _sz, _vp]
     L.nwg_descriptors.argtypes = [_vp, _sz, _vp, _sz, _vp, _vp, _vp, C.c_float, _vp, _vp]
+    L.nwg_surrogate_create.argtypes = [_vp, C.POINTER(SurrogateConfig), _vp, _sz, _vp, _sz, C.POINTER(_vp)]
+    L.nwg_surrogate_destroy.argtypes = [_vp]
+    L.nwg_surrogate_destroy.restype = None
+    L.nwg_surrogate_advance.argtypes = [_vp, C.c_uint32, C.POINTER(RuntimeWordCounts), C.POINTER(AssemblyConfig),
+                                        C.POINTER(SurrogateStats)]
     L.nwg_swap_generations.argtypes = [_vp]
     L.nwg_read_status.argtypes = [_vp, C.POINTER(C.c_int)]
     L.nwg_download_current_generation.argtypes = [_vp, _vp, _vp, _vp, _vp, _sz, C.POINTER(_sz), C.POINTER(_sz)]
@@ -757,4 +789,36 @@ class Mlp:
 
     def train_step(self, x_ptr: int, t_ptr: int, rows: int) -> None:
         check(lib().nwg_mlp_train_step(self.handle, x_ptr, t_ptr, rows), "nwg_mlp_train_step")
+
+
+class Surrogate:
+    """Surrogate-screened evolution of a Runtime's population (nwg_surrogate_*)."""
+
+    def __init__(self, runtime: "Runtime", catalog: np.ndarray, config: SurrogateConfig | None = None,
+                 secret_pool: np.ndarray | None = None):
+        self.config = config or SurrogateConfig()
+        cat = np.ascontiguousarray(catalog, np.uint8)
+        pool = None if secret_pool is None else np.ascontiguousarray(secret_pool, np.uint32)
+        handle = _vp()
+        check(lib().nwg_surrogate_create(runtime.handle, C.byref(self.config), _np_ptr(cat), len(cat), _np_ptr(pool),
+                                         0 if pool is None else len(pool), C.byref(handle)), "nwg_surrogate_create")
+        self.handle = handle
+        self.runtime = runtime
+
+    def close(self):
+        if self.handle:
+            lib().nwg_surrogate_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def advance(self, seed: int, counts: RuntimeWordCounts, config: AssemblyConfig) -> SurrogateStats:
+        st = SurrogateStats()
+        check(lib().nwg_surrogate_advance(self.handle, seed, C.byref(counts), C.byref(config), C.byref(st)),
+              "nwg_surrogate_advance")
+        return st
 

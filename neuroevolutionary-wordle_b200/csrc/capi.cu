@@ -88,6 +88,8 @@ struct nwg_runtime {
     // the current generation holds released parents (slot 0xFFFFFFFF), as a restored boundary does; it can only
     // be assembled, not evaluated
     bool released_parents = false;
+    // the win counters describe the current generation (false after a generation is installed with known fitness)
+    bool rates_valid = false;
 
     // pinned host staging
     ShardRecord *host_shards = nullptr;
@@ -354,6 +356,20 @@ __global__ void PlanChildSlotsKernel(const std::uint32_t *pairs, std::uint32_t c
     }
 }
 
+// Copies whole slots (pitch bytes, 16-byte vectors) from one slab to another: slot src_slots[i] to dst_slots[i].
+__global__ void CopySlotsKernel(const std::uint8_t *src, std::size_t src_pitch, const std::uint32_t *src_slots,
+                                std::uint8_t *dst, std::size_t dst_pitch, const std::uint32_t *dst_slots,
+                                std::uint32_t n) {
+    const std::size_t vectors = dst_pitch / 16;
+    for (std::uint32_t i = blockIdx.x; i < n; i += gridDim.x) {
+        const uint4 *s = reinterpret_cast<const uint4 *>(src + static_cast<std::size_t>(src_slots[i]) * src_pitch);
+        uint4 *d = reinterpret_cast<uint4 *>(dst + static_cast<std::size_t>(dst_slots[i]) * dst_pitch);
+        for (std::size_t v = threadIdx.x; v < vectors; v += blockDim.x) {
+            d[v] = s[v];
+        }
+    }
+}
+
 void FreeRuntime(nwg_runtime *rt) {
     if (rt == nullptr) {
         return;
@@ -501,6 +517,7 @@ int EvaluateImpl(nwg_runtime *rt, const nwg_runtime_word_counts *counts, const n
     rt->last_eval_population = population;
     rt->last_action_count = rt->action_count;
     rt->last_eval_generation = rt->cur_gen_index;
+    rt->rates_valid = true;
     return kOk;
 }
 
@@ -796,7 +813,81 @@ int ReadGenerationView(const nwg_runtime *rt, GenerationView *out) {
     out->generation_index = rt->cur_gen_index;
     out->generation_size = rt->cur_gen_size;
     out->planned_children = rt->planned_children;
+    out->grid_column_count = rt->grid_column_count;
+    out->stride = rt->stride;
+    out->slot_count = rt->slot_count;
+    out->cell_offsets = rt->cell_offsets;
+    out->cell_words = rt->cell_words;
+    out->cell_count = rt->cell_count;
+    out->evaluated = rt->last_eval_population == rt->cur_gen_size && rt->last_eval_generation == rt->cur_gen_index &&
+                     rt->cur_gen_size > 0 && !rt->released_parents;
+    out->status = rt->status;
     return kOk;
+}
+
+int InstallGeneration(nwg_runtime *rt, const std::uint8_t *src_slab, std::size_t src_pitch,
+                      const std::vector<std::uint32_t> &src_slots, const std::vector<float> &fitness,
+                      std::size_t generation_index) {
+    const std::size_t n = src_slots.size();
+    if (n == 0 || n != fitness.size() || n > rt->max_generation_size || src_pitch != rt->pitch ||
+        n % rt->grid_column_count != 0) {
+        return kInvalidGeneration;
+    }
+    std::vector<std::uint32_t> current(rt->cur_gen_size);
+    if (cudaStreamSynchronize(rt->stream) != cudaSuccess ||
+        (rt->cur_gen_size > 0 &&
+         cudaMemcpy(current.data(), rt->cur_slots, current.size() * 4, cudaMemcpyDeviceToHost) != cudaSuccess)) {
+        return kCudaFailure;
+    }
+    std::vector<std::uint8_t> used(rt->slot_count, 0);
+    for (const std::uint32_t s : current) {
+        if (s < rt->slot_count) {
+            used[s] = 1;
+        }
+    }
+    std::vector<std::uint32_t> target;
+    target.reserve(n);
+    for (std::uint32_t s = 0; s < rt->slot_count && target.size() < n; ++s) {
+        if (!used[s]) {
+            target.push_back(s);
+        }
+    }
+    if (target.size() < n) {
+        return SetHostStatus(rt, kSlabFull);
+    }
+    std::uint32_t *d_src = nullptr;
+    std::vector<std::uint32_t> ones(n, 1u);
+    std::vector<std::uint8_t> has(n, 1u);
+    bool ok = cudaMalloc(&d_src, n * 4) == cudaSuccess &&
+              cudaMemcpyAsync(d_src, src_slots.data(), n * 4, cudaMemcpyHostToDevice, rt->stream) == cudaSuccess &&
+              cudaMemcpyAsync(rt->next_slots, target.data(), n * 4, cudaMemcpyHostToDevice, rt->stream) ==
+                  cudaSuccess &&
+              cudaMemcpyAsync(rt->next_fitness, fitness.data(), n * 4, cudaMemcpyHostToDevice, rt->stream) ==
+                  cudaSuccess &&
+              cudaMemcpyAsync(rt->next_eval, ones.data(), n * 4, cudaMemcpyHostToDevice, rt->stream) == cudaSuccess &&
+              cudaMemcpyAsync(rt->next_has, has.data(), n, cudaMemcpyHostToDevice, rt->stream) == cudaSuccess;
+    if (ok) {
+        CopySlotsKernel<<<256, 256, 0, rt->stream>>>(src_slab, src_pitch, d_src, rt->slab, rt->pitch, rt->next_slots,
+                                                     static_cast<std::uint32_t>(n));
+        ok = cudaGetLastError() == cudaSuccess;
+    }
+    ok = ok && cudaStreamSynchronize(rt->stream) == cudaSuccess;
+    cudaFree(d_src);
+    if (!ok) {
+        return kCudaFailure;
+    }
+    rt->prepared = false;
+    rt->next_gen_index = generation_index;
+    rt->next_gen_size = n;
+    nwg_swap_generations(rt);
+    NWG_TRY(LaunchSummarize(rt->cur_fitness, rt->cur_has, rt->cur_slots, static_cast<std::uint32_t>(n), rt->summary,
+                            rt->status, rt->stream));
+    NWG_TRY(cudaMemcpyAsync(rt->host_summary, rt->summary, sizeof(SummaryDevice), cudaMemcpyDeviceToHost, rt->stream));
+    rt->last_eval_population = n;
+    rt->last_action_count = rt->action_count;
+    rt->last_eval_generation = generation_index;
+    rt->rates_valid = false;
+    return Sync(rt);
 }
 
 int InstallBoundary(nwg_runtime *rt, const std::uint32_t *slots, const float *fitness, const std::uint32_t *eval,
@@ -1126,7 +1217,8 @@ int nwg_read_evaluation_stats(const nwg_runtime *rt, nwg_evaluation_stats *stats
 
 int nwg_read_solve_rates(const nwg_runtime *rt, float *rates, size_t capacity, size_t *count_out,
                          double *mean_out) {
-    if (rt == nullptr || rt->last_eval_population == 0 || rt->last_eval_population != rt->cur_gen_size) {
+    if (rt == nullptr || rt->last_eval_population == 0 || rt->last_eval_population != rt->cur_gen_size ||
+        !rt->rates_valid || rt->last_eval_generation != rt->cur_gen_index) {
         return kPopulationNotEvaluated;
     }
     const std::size_t n = rt->cur_gen_size;

@@ -193,8 +193,20 @@ struct GenerationView {
     const std::uint8_t *has_fitness;
     const std::uint32_t *pairs;  // the last plan's (first, second) parent indices
     std::size_t generation_index, generation_size, planned_children;
+    std::size_t grid_column_count, stride, slot_count;
+    const std::uint32_t *cell_offsets, *cell_words;  // per-cell word lists (CSR), when set
+    std::size_t cell_count;
+    bool evaluated;  // the current generation's fitness is from an evaluation of this generation
+    int *status;
 };
 int ReadGenerationView(const nwg_runtime *rt, GenerationView *out);
+
+// Makes `count` genomes held elsewhere (src_slab at src_pitch, host slot list) the runtime's next generation with
+// their known fitness (one evaluation each), copied into slots the current generation does not use, and swaps
+// it in; the population size and pitch must be the runtime's.
+int InstallGeneration(nwg_runtime *rt, const std::uint8_t *src_slab, std::size_t src_pitch,
+                      const std::vector<std::uint32_t> &src_slots, const std::vector<float> &fitness,
+                      std::size_t generation_index);
 
 // Device catalog tables: packed words [pad] and fixed word features [26][pad], pad = word count rounded up to 128.
 int BuildCatalogTables(const std::uint8_t *letters, std::size_t word_count, std::uint32_t **codes_out,

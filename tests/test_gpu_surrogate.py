@@ -1,0 +1,98 @@
+"""Surrogate-screened evolution on the B200 (no reference counterpart; the plain step is the reference's).
+
+- With one candidate per cell and full evaluation the surrogate step is the plain step: the same plan, the same
+  children byte for byte, the same fitness.
+- A full-evaluation step reports, on the same brood, the mean fitness of the model's pick, of candidate 0 (the
+  plain child) and of the best child; the winners are the best children.
+- A screened step plays the model's pick of each cell plus an audit sample and installs the picks.
+- What the trained network gains over the method without it: at the 4,096-cell, 256-secret workload its pick beats
+  the plain child on average over generations, on the same broods.
+"""
+import numpy as np
+import pytest
+
+from tests import gpu_util as G
+
+pytestmark = pytest.mark.gpu
+capi = G.nwg.capi
+W = G.nwg.workload
+
+
+def _population(A, P, cols, per_cell, seed, form=0):
+    catalog = W.synthetic_words(A, seed)
+    G.upload_catalog_everywhere(catalog)
+    rt = G.nwg.Runtime(A, P, cols)
+    rt.bootstrap(P, seed=seed)
+    rt.set_form(form)
+    sub = W.secret_subset(A, min(A, 2315), seed)
+    off, words = W.fixed_cell_lists(P, per_cell, sub, seed)
+    rt.set_cell_words(off, words)
+    return rt, catalog, capi.word_counts(training=A, action_space=A), sub
+
+
+CFG = capi.assembly_config(radius=1, p=0.05, sigma=0.02)
+
+
+def test_one_candidate_per_cell_is_the_plain_step():
+    rt, catalog, counts, _ = _population(300, 64, 8, 6, 1)
+    plain, _, _, _ = _population(300, 64, 8, 6, 1)
+    sur = capi.Surrogate(rt, catalog, capi.SurrogateConfig(candidates_per_cell=1, warmup_pairs=10**9, batch_rows=128,
+                                                           train_steps=1, replay_capacity=1024, evaluation_form=0))
+    st = sur.advance(77, counts, CFG)
+    plain.advance(77, counts, config=CFG)
+    plain.evaluate(counts)
+    a, b = rt.current_generation(), plain.current_generation()
+    assert st.evaluated == 64 and not st.screened and a["generation_index"] == b["generation_index"] == 1
+    assert np.array_equal(a["fitness"].view(np.uint32), b["fitness"].view(np.uint32))
+    for i in range(64):
+        assert np.array_equal(rt.download_slot(int(a["slots"][i])), plain.download_slot(int(b["slots"][i]))), i
+    sur.close(); rt.close(); plain.close()
+
+
+def test_full_evaluation_reports_picks_and_keeps_the_best():
+    rt, catalog, counts, _ = _population(500, 256, 16, 24, 3)
+    sur = capi.Surrogate(rt, catalog, capi.SurrogateConfig(spearman_floor=2.0, warmup_pairs=0, batch_rows=256,
+                                                           train_steps=16, replay_capacity=8192, seed=1))
+    for g in range(4):
+        st = sur.advance(100 + g, counts, CFG)
+        assert st.evaluated == st.candidates == 1024 and not st.screened
+        assert st.mean_fitness == pytest.approx(st.mean_fitness_best_candidate, rel=1e-12)
+        assert st.mean_fitness_best_candidate >= st.mean_fitness_first_candidate
+        if g == 0:
+            assert np.isnan(st.spearman) and np.isnan(st.mean_fitness_model_pick)
+        else:
+            assert -1.0 <= st.spearman <= 1.0
+            assert st.mean_fitness_first_candidate <= st.mean_fitness_best_candidate
+            assert st.mean_fitness_model_pick <= st.mean_fitness_best_candidate
+        assert st.replay_size == min(1024 * (g + 1), 8192) and st.train_steps == 16
+    gen = rt.current_generation()
+    assert gen["generation_index"] == 4 and gen["has_fitness"].all()
+    assert np.mean(gen["fitness"]) == pytest.approx(st.mean_fitness, rel=1e-6)
+    sur.close(); rt.close()
+
+
+def test_screened_step_plays_picks_and_an_audit():
+    rt, catalog, counts, _ = _population(500, 256, 16, 24, 5)
+    sur = capi.Surrogate(rt, catalog, capi.SurrogateConfig(spearman_floor=-1.0, warmup_pairs=512, batch_rows=256,
+                                                           train_steps=4, replay_capacity=4096, seed=2))
+    first = sur.advance(1, counts, CFG)
+    assert not first.screened and first.evaluated == 1024  # untrained: everything plays
+    second = sur.advance(2, counts, CFG)
+    assert second.screened and second.evaluated == 256 + round(0.05 * 1024)
+    assert not np.isnan(second.spearman)
+    gen = rt.current_generation()
+    assert gen["generation_index"] == 2 and np.mean(gen["fitness"]) == pytest.approx(second.mean_fitness, rel=1e-6)
+    sur.close(); rt.close()
+
+
+def test_trained_network_beats_the_plain_child_on_the_same_broods():
+    rt, catalog, counts, sub = _population(4739, 4096, 64, 256, 0, form=4)
+    sur = capi.Surrogate(rt, catalog, capi.SurrogateConfig(spearman_floor=2.0, seed=1), secret_pool=sub)
+    ratios = []
+    for g in range(10):
+        st = sur.advance(2000 + g, counts, CFG)
+        if not np.isnan(st.mean_fitness_model_pick):
+            ratios.append(st.mean_fitness_model_pick / st.mean_fitness_first_candidate)
+    assert len(ratios) >= 8
+    assert np.mean(ratios) > 1.005, ratios
+    sur.close(); rt.close()
