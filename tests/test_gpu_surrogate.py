@@ -77,11 +77,12 @@ def test_screened_step_plays_picks_and_an_audit():
                                                            train_steps=4, replay_capacity=4096, seed=2))
     first = sur.advance(1, counts, CFG)
     assert not first.screened and first.evaluated == 1024  # untrained: everything plays
-    second = sur.advance(2, counts, CFG)
-    assert second.screened and second.evaluated == 256 + round(0.05 * 1024)
-    assert not np.isnan(second.spearman)
+    second = sur.advance(2, counts, CFG)  # trained now: this step's audit gives the first correlation
+    assert not second.screened and not np.isnan(second.spearman)
+    third = sur.advance(3, counts, CFG)
+    assert third.screened and third.evaluated == 256 + round(0.05 * 1024)
     gen = rt.current_generation()
-    assert gen["generation_index"] == 2 and np.mean(gen["fitness"]) == pytest.approx(second.mean_fitness, rel=1e-6)
+    assert gen["generation_index"] == 3 and np.mean(gen["fitness"]) == pytest.approx(third.mean_fitness, rel=1e-6)
     sur.close(); rt.close()
 
 
