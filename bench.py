@@ -6,9 +6,9 @@ reference crossover temperatures, mutation p = 0.05, sigma = 0.02. Genomes are t
 layout (bootstrap He-normal weights, N(0, 0.05) tails).
 
 The headline form (default --form tc-trunk-fp16) runs encoder, trunk and scoring on tcgen05 with FP16
-operands and a top-2 margin guard (tau = 1e-3) that sends uncertain game steps through the exact FP32
-path. The plain FP32 form is timed on the same workload in the same process and reported beside it
-("plain_fp32"), with the guess agreement and fitness delta of the headline form against it over the
+operands and a top-2 margin guard (--tau, default 1e-3 x the score scale) that sends uncertain game steps
+through the exact FP32 path. The plain FP32 form is timed on the same workload in the same process and
+reported beside it ("plain_fp32"), with the guess agreement and fitness delta of the headline form against it over the
 whole population ("agreement_with_plain"). --form fp32 benchmarks the plain form alone.
 
 On the full workload at N=1 the line also carries "surrogate_vs_plain": the plain FP32 form evolves 50
@@ -556,7 +556,7 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--form", choices=sorted(FORMS), default="tc-trunk-fp16")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP32 comparison and the agreement sample")
-    ap.add_argument("--tau", type=float, default=1e-3, help="margin guard of the tensor-core trunk forms")
+    ap.add_argument("--tau", type=float, default=1e-3, help="margin guard of the tensor-core trunk forms (1e-3 x the score scale)")
     ap.add_argument("--no-surrogate", action="store_true", help="skip the surrogate-vs-plain race")
     ap.add_argument("--surrogate-generations", type=int, default=50)
     args = ap.parse_args()

@@ -504,6 +504,12 @@ int nwg_descriptors(const void *slab, size_t pitch, const uint32_t *slots, size_
                     const uint8_t *probe_feedback, const uint8_t *probe_turns, float scale, uint16_t *out,
                     void *cuda_stream);
 
+/* Test hook: the 16-bit score table (column maxima, K-major tiles, per-tile column moments) that the last evaluation
+ * in a tensor-core form built for one individual of the evaluated generation; bytes_out gets its size (host_out
+ * NULL: size only). NWG_POPULATION_NOT_EVALUATED when no such evaluation ran. */
+int nwg_read_score_table(const nwg_runtime *runtime, size_t individual, void *host_out, size_t capacity,
+                         size_t *bytes_out);
+
 /* Test hook: C[m][n] FP32 = A[m][k] . B[n][k]^T on tcgen05 (BF16 device operands, K contiguous); m % 128, n % 256,
  * k % 64, lda % 8, ldb % 8 and ldc % 4 zero, bases 16-byte aligned (NWG_UNSUPPORTED otherwise). */
 int nwg_bf16_gemm_nt(const void *a, size_t lda, const void *b, size_t ldb, float *c, size_t ldc, size_t m, size_t n,

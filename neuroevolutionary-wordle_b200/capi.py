@@ -198,7 +198,7 @@ EXPORTS = [
     "nwg_winner_artifact_read", "nwg_download_next_generation", "nwg_fitness_telemetry_collect",
     "nwg_convergence_telemetry_collect", "nwg_convergence_sample_plan", "nwg_maybe_release_training_shard",
     "nwg_single_model_create", "nwg_single_model_destroy", "nwg_single_model_set_stream", "nwg_single_model_select",
-    "nwg_read_solve_rates", "nwg_mlp_create", "nwg_mlp_destroy", "nwg_mlp_set_stream", "nwg_mlp_parameter_count",
+    "nwg_read_solve_rates", "nwg_read_score_table", "nwg_mlp_create", "nwg_mlp_destroy", "nwg_mlp_set_stream", "nwg_mlp_parameter_count",
     "nwg_mlp_parameters", "nwg_mlp_forward", "nwg_mlp_gradients", "nwg_mlp_train_step", "nwg_bf16_gemm_nt",
     "nwg_descriptors", "nwg_surrogate_create", "nwg_surrogate_destroy", "nwg_surrogate_advance",
 ]
@@ -262,6 +262,7 @@ def lib() -> C.CDLL:
     L.nwg_single_model_set_stream.argtypes = [_vp, _vp]
     L.nwg_single_model_select.argtypes = [_vp, _vp, _vp, _vp, _sz, C.POINTER(SelectedAction)]
     L.nwg_read_solve_rates.argtypes = [_vp, _vp, _sz, C.POINTER(_sz), C.POINTER(C.c_double)]
+    L.nwg_read_score_table.argtypes = [_vp, _sz, _vp, _sz, C.POINTER(_sz)]
     L.nwg_mlp_create.argtypes = [_sz, C.c_uint32, C.c_float, C.POINTER(_vp)]
     L.nwg_mlp_destroy.argtypes = [_vp]
     L.nwg_mlp_destroy.restype = None
@@ -503,6 +504,15 @@ class Runtime:
         check(lib().nwg_read_solve_rates(self.handle, _np_ptr(rates), rates.size, C.byref(n), C.byref(mean)),
               "nwg_read_solve_rates")
         return rates[:n.value], mean.value
+
+    def score_table(self, individual: int) -> np.ndarray:
+        """Bytes of the 16-bit score table the last tensor-core evaluation built for one individual."""
+        n = _sz()
+        check(lib().nwg_read_score_table(self.handle, individual, None, 0, C.byref(n)), "nwg_read_score_table")
+        out = np.zeros(n.value, np.uint8)
+        check(lib().nwg_read_score_table(self.handle, individual, _np_ptr(out), out.size, C.byref(n)),
+              "nwg_read_score_table")
+        return out
 
     def resume(self) -> None:
         """TryResumeGenerationFromCheckpointOnDevice: assemble a restored boundary."""

@@ -77,6 +77,7 @@ struct nwg_runtime {
     int form = NWG_FORM_FP32;
     std::uint8_t *tc_tables = nullptr;
     std::size_t tc_tables_bytes = 0;
+    std::size_t last_table_pitch = 0;  // of the tables the last tensor-core evaluation built (0: none)
     std::uint8_t *trunk_tables = nullptr;
     float margin_tau = 1.0e-3f;
     // a generation prepared for assembly (evaluated and planned; nwg_prepare_generation / checkpoint restore)
@@ -485,6 +486,7 @@ int EvaluateImpl(nwg_runtime *rt, const nwg_runtime_word_counts *counts, const n
         NWG_TRY(cudaEventRecord(rt->eval_end, rt->stream));
     } else if (rt->form == NWG_FORM_TC_TRUNK_BF16 || rt->form == NWG_FORM_TC_TRUNK_FP16) {
         const bool fp16 = rt->form == NWG_FORM_TC_TRUNK_FP16;
+        rt->last_table_pitch = TcTablePitch(static_cast<std::uint32_t>(selectable));
         NWG_TRY(LaunchBuildTcTables(rt->slab, rt->pitch, rt->cur_slots, population, g_catalog.fixed_t,
                                     static_cast<std::uint32_t>(g_catalog.pad), static_cast<std::uint32_t>(selectable),
                                     rt->tc_tables, fp16, rt->stream));
@@ -499,6 +501,7 @@ int EvaluateImpl(nwg_runtime *rt, const nwg_runtime_word_counts *counts, const n
         // |16-bit product - FP32 product| <= (2u + u^2)|p||e| with u = 2^-8 (BF16: p and e rounded) or 2^-11 (FP16:
         // p rounded, e exact), plus 64-term FP32 accumulation on both sides; with a safety margin.
         const float kappa = fp16 ? 6.5e-4f : 1.0e-2f;
+        rt->last_table_pitch = TcTablePitch(static_cast<std::uint32_t>(selectable));
         NWG_TRY(LaunchBuildTcTables(rt->slab, rt->pitch, rt->cur_slots, population, g_catalog.fixed_t,
                                     static_cast<std::uint32_t>(g_catalog.pad), static_cast<std::uint32_t>(selectable),
                                     rt->tc_tables, fp16, rt->stream));
@@ -1212,6 +1215,29 @@ int nwg_read_evaluation_stats(const nwg_runtime *rt, nwg_evaluation_stats *stats
     stats->fitness_variance_fp64 = rt->host_summary->variance_fp64;
     float ms = 0.0f;
     stats->eval_kernel_ms = cudaEventElapsedTime(&ms, rt->eval_begin, rt->eval_end) == cudaSuccess ? ms : -1.0;
+    return kOk;
+}
+
+int nwg_read_score_table(const nwg_runtime *rt, size_t individual, void *host_out, size_t capacity,
+                         size_t *bytes_out) {
+    if (rt == nullptr || rt->tc_tables == nullptr || rt->last_table_pitch == 0 ||
+        individual >= rt->last_eval_population) {
+        return kPopulationNotEvaluated;
+    }
+    if (bytes_out != nullptr) {
+        *bytes_out = rt->last_table_pitch;
+    }
+    if (host_out == nullptr) {
+        return kOk;
+    }
+    if (capacity < rt->last_table_pitch) {
+        return kInvalidGeneration;
+    }
+    if (cudaStreamSynchronize(rt->stream) != cudaSuccess ||
+        cudaMemcpy(host_out, rt->tc_tables + individual * rt->last_table_pitch, rt->last_table_pitch,
+                   cudaMemcpyDeviceToHost) != cudaSuccess) {
+        return kCudaFailure;
+    }
     return kOk;
 }
 

@@ -413,58 +413,105 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTcKernel(const TcParams q
 
 // Per individual: emax[k] = max over the selectable actions of |e_ak| (header), the embeddings as 16-bit
 // values in the K-major core-matrix layout, 1 KB per 8 actions, zero past the last action, and after the
-// last tile, per tile, the column moments (sum_a e_ak, sum_a e_ak^2) over the tile's actions as float2[64],
-// each summed in a fixed order so that every run gets the same bits.
+// last tile, per tile, the column moments (sum_a e_ak, sum_a e_ak^2) over the tile's actions as float2[64].
+// One CTA per individual walks its tiles. Thread (a, part) builds action a's four 16-byte segments of columns
+// 32 part .. 32 part + 31 (the fixed features from the catalog, the tail from the genome); each warp's stores
+// fill whole 128-byte lines. The values also go to shared memory ([action][65], conflict-free both ways), where
+// thread (column, quarter) sums its quarter of the tile's actions (values and their squares, each operation
+// rounded on its own) in ascending order; the quarters are then combined in a fixed order, so every run gets the
+// same bits.
 template <bool kFp16>
-__global__ void BuildTcTablesKernel(const std::uint8_t *slab, std::size_t pitch, const std::uint32_t *slots,
-                                    const float *fixed_t, std::uint32_t action_pad, std::uint32_t action_count,
-                                    std::uint32_t tiles, std::uint8_t *tables, std::size_t table_pitch) {
-    const std::uint32_t ind = blockIdx.y;
-    const std::uint32_t tile = blockIdx.x;
-    const __half *tail =
-        reinterpret_cast<const __half *>(slab + static_cast<std::size_t>(slots[ind]) * pitch + kTailOffsetBytes);
+__global__ void __launch_bounds__(256) BuildTcTablesKernel(const std::uint8_t *slab, std::size_t pitch,
+                                                           const std::uint32_t *slots, const float *fixed_t,
+                                                           std::uint32_t action_pad, std::uint32_t action_count,
+                                                           std::uint32_t tiles, std::uint8_t *tables,
+                                                           std::size_t table_pitch) {
+    constexpr int kLd = kPolicy + 1;
+    __shared__ float vals[kTileN * kLd];
+    __shared__ float2 part_sum[4][kPolicy];
+    __shared__ float part_max[4][kPolicy];
+    const std::uint32_t ind = blockIdx.x;
+    const std::uint8_t *tail = slab + static_cast<std::size_t>(slots[ind]) * pitch + kTailOffsetBytes;
     std::uint8_t *table = tables + static_cast<std::size_t>(ind) * table_pitch;
-    unsigned int *emax_bits = reinterpret_cast<unsigned int *>(table);
-    std::uint8_t *out = table + 256 + static_cast<std::size_t>(tile) * kTileBytes;
-    __shared__ unsigned int block_max[kPolicy];
-    __shared__ float2 part[4][kPolicy];
-    if (threadIdx.x < kPolicy) {
-        block_max[threadIdx.x] = 0;
-    }
-    __syncthreads();
-    // thread t owns column t % 64 and actions t / 64, t / 64 + 4, ... of the tile
-    float sum = 0.0f;
-    float sum_sq = 0.0f;
-    for (int idx = threadIdx.x; idx < kTileN * kPolicy; idx += blockDim.x) {
-        const int a_local = idx >> 6;
-        const int k = idx & 63;
-        const std::uint32_t a = tile * kTileN + a_local;
-        float v = 0.0f;
-        if (a < action_count) {
-            v = k < kFixedDim ? fixed_t[static_cast<std::size_t>(k) * action_pad + a]
-                              : __half2float(tail[static_cast<std::size_t>(a) * kTailDim + (k - kFixedDim)]);
-            atomicMax(&block_max[k], __float_as_uint(fabsf(v)));
-            sum += v;
-            sum_sq = __fmaf_rn(v, v, sum_sq);
-        }
-        std::uint16_t bits;
-        if constexpr (kFp16) {
-            bits = __half_as_ushort(__float2half_rn(v));
+    float2 *moments = reinterpret_cast<float2 *>(table + 256 + static_cast<std::size_t>(tiles) * kTileBytes);
+    const int t = static_cast<int>(threadIdx.x);
+    const int a_local = t & (kTileN - 1);
+    const int part = t >> 7;     // columns 32 part .. 32 part + 31
+    const int col = t & (kPolicy - 1);
+    const int quarter = t >> 6;  // actions 32 quarter .. 32 quarter + 31 of the tile
+    float run_max = 0.0f;
+    for (std::uint32_t tile = 0; tile < tiles; ++tile) {
+        const std::uint32_t a = tile * kTileN + static_cast<std::uint32_t>(a_local);
+        const bool valid = a < action_count;
+        const std::uint32_t *row =
+            reinterpret_cast<const std::uint32_t *>(tail + static_cast<std::size_t>(valid ? a : 0u) * kTailRowBytes);
+        float v[32];
+        if (part == 0) {
+#pragma unroll
+            for (int k = 0; k < kFixedDim; ++k) {
+                v[k] = valid ? __ldg(fixed_t + static_cast<std::size_t>(k) * action_pad + a) : 0.0f;
+            }
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {  // tail values 0 .. 5 (columns 26 .. 31)
+                const std::uint32_t w = valid ? __ldg(row + i) : 0u;
+                const __half2 h = *reinterpret_cast<const __half2 *>(&w);
+                v[kFixedDim + 2 * i] = __low2float(h);
+                v[kFixedDim + 2 * i + 1] = __high2float(h);
+            }
         } else {
-            bits = __bfloat16_as_ushort(__float2bfloat16_rn(v));
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {  // tail values 6 .. 37 (columns 32 .. 63)
+                const std::uint32_t w = valid ? __ldg(row + 3 + i) : 0u;
+                const __half2 h = *reinterpret_cast<const __half2 *>(&w);
+                v[2 * i] = __low2float(h);
+                v[2 * i + 1] = __high2float(h);
+            }
         }
-        *reinterpret_cast<std::uint16_t *>(out + umma::TileOffset(a_local, k, kPolicy)) = bits;
+        std::uint8_t *out = table + 256 + static_cast<std::size_t>(tile) * kTileBytes;
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            std::uint32_t w[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const float x = v[8 * s + 2 * i];
+                const float y = v[8 * s + 2 * i + 1];
+                if constexpr (kFp16) {
+                    w[i] = static_cast<std::uint32_t>(__half_as_ushort(__float2half_rn(x))) |
+                           (static_cast<std::uint32_t>(__half_as_ushort(__float2half_rn(y))) << 16);
+                } else {
+                    w[i] = static_cast<std::uint32_t>(__bfloat16_as_ushort(__float2bfloat16_rn(x))) |
+                           (static_cast<std::uint32_t>(__bfloat16_as_ushort(__float2bfloat16_rn(y))) << 16);
+                }
+            }
+            *reinterpret_cast<uint4 *>(out + umma::TileOffset(a_local, part * 32 + 8 * s, kPolicy)) =
+                make_uint4(w[0], w[1], w[2], w[3]);
+        }
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+            vals[a_local * kLd + part * 32 + j] = v[j];
+        }
+        __syncthreads();
+        float sum = 0.0f;
+        float sum_sq = 0.0f;
+        for (int i = 0; i < 32; ++i) {
+            const float x = vals[(quarter * 32 + i) * kLd + col];
+            sum = __fadd_rn(sum, x);
+            sum_sq = __fadd_rn(sum_sq, __fmul_rn(x, x));
+            run_max = fmaxf(run_max, fabsf(x));
+        }
+        part_sum[quarter][col] = make_float2(sum, sum_sq);
+        __syncthreads();
+        if (t < kPolicy) {
+            moments[tile * kPolicy + t] =
+                make_float2(((part_sum[0][t].x + part_sum[1][t].x) + part_sum[2][t].x) + part_sum[3][t].x,
+                            ((part_sum[0][t].y + part_sum[1][t].y) + part_sum[2][t].y) + part_sum[3][t].y);
+        }
     }
-    part[threadIdx.x >> 6][threadIdx.x & 63] = make_float2(sum, sum_sq);
+    part_max[quarter][col] = run_max;
     __syncthreads();
-    if (threadIdx.x < kPolicy && block_max[threadIdx.x] != 0) {
-        atomicMax(&emax_bits[threadIdx.x], block_max[threadIdx.x]);
-    }
-    if (threadIdx.x < kPolicy) {
-        const int k = threadIdx.x;
-        const float2 m = make_float2(((part[0][k].x + part[1][k].x) + part[2][k].x) + part[3][k].x,
-                                     ((part[0][k].y + part[1][k].y) + part[2][k].y) + part[3][k].y);
-        reinterpret_cast<float2 *>(table + 256 + static_cast<std::size_t>(tiles) * kTileBytes)[tile * kPolicy + k] = m;
+    if (t < kPolicy) {
+        reinterpret_cast<float *>(table)[t] =
+            fmaxf(fmaxf(part_max[0][t], part_max[1][t]), fmaxf(part_max[2][t], part_max[3][t]));
     }
 }
 
@@ -478,19 +525,17 @@ std::size_t TcTablePitch(std::uint32_t action_count) {
 cudaError_t LaunchBuildTcTables(const std::uint8_t *slab, std::size_t pitch, const std::uint32_t *slots,
                                 std::uint32_t population, const float *fixed_t, std::uint32_t action_pad,
                                 std::uint32_t action_count, std::uint8_t *tables, bool fp16, cudaStream_t stream) {
+    if (population == 0) {
+        return cudaSuccess;
+    }
     const std::size_t table_pitch = TcTablePitch(action_count);
     const std::uint32_t tiles = (action_count + kTileN - 1) / kTileN;
-    cudaError_t e = cudaMemset2DAsync(tables, table_pitch, 0, 256, population, stream);
-    if (e != cudaSuccess) {
-        return e;
-    }
-    dim3 grid(tiles, population);
     if (fp16) {
-        BuildTcTablesKernel<true><<<grid, 256, 0, stream>>>(slab, pitch, slots, fixed_t, action_pad, action_count,
-                                                           tiles, tables, table_pitch);
+        BuildTcTablesKernel<true><<<population, 256, 0, stream>>>(slab, pitch, slots, fixed_t, action_pad,
+                                                                  action_count, tiles, tables, table_pitch);
     } else {
-        BuildTcTablesKernel<false><<<grid, 256, 0, stream>>>(slab, pitch, slots, fixed_t, action_pad, action_count,
-                                                            tiles, tables, table_pitch);
+        BuildTcTablesKernel<false><<<population, 256, 0, stream>>>(slab, pitch, slots, fixed_t, action_pad,
+                                                                   action_count, tiles, tables, table_pitch);
     }
     return cudaGetLastError();
 }
