@@ -497,6 +497,92 @@ def run_ours(args) -> None:
         rt.close()
 
 
+def run_growth(args) -> None:
+    """Batching form with uneven shards: 16,384 individuals on a 128x128 grid, per-cell secret lists of
+    floor(exp(U[ln 32, ln 1024])) words drawn from the first 1,024 catalog words, and the action space widened
+    from 1,024 to 4,739 words in steps of 512 (the last step 131) over 50 generations. Every generation that does
+    not widen runs as one CUDA graph with launch shapes tuned per width (nwg_advance_graphed); a widening
+    generation breeds into the wider slab and injects the new rows directly. As in the reference, the generation
+    byte budget is fixed at creation (16,384 genomes at 1,024 words), so each widening keeps the whole grid rows
+    that still fit; the surviving cells keep their secret lists. Timed on the host with the device synchronised
+    around each generation; game steps are counted on the device."""
+    import torch
+
+    rank, world, local = dist_setup(args.gpus)
+    nwg = importlib.import_module("neuroevolutionary-wordle_b200")
+    W, capi = nwg.workload, nwg.capi
+    population, columns, start, final, step, generations = 16384, 128, 1024, 4739, 512, 50
+    widths = list(range(start + step, final, step)) + [final]
+    widen_at = {round((i + 1) * generations / (len(widths) + 1)): w for i, w in enumerate(widths)}
+    # words past the starting width are injected later, so each needs a hint-grid group (a monochrome word, for
+    # one, has none and the reference rejects its injection): draw replacements for those that lack one
+    pool = W.synthetic_words(2 * final, 0)
+    usable = capi.hint_groups_available(pool)
+    tail = [w for w, ok in zip(pool[start:], usable[start:]) if ok][:final - start]
+    catalog = np.concatenate([pool[:start], np.array(tail, np.uint8)])
+    assert len(catalog) == final
+    capi.upload_catalog(catalog)
+    subset = W.secret_subset(start, start, 0)
+    offsets, words = W.loguniform_cell_lists(population, 32, 1024, subset, rank)
+    rt = nwg.Runtime(start, population, columns, stream=torch.cuda.current_stream().cuda_stream)
+    rt.set_cell_words(offsets, words)
+    rt.set_form(FORMS[args.form])
+    if args.form.startswith("tc-trunk"):
+        rt.set_margin_guard(args.tau)
+    rt.bootstrap(population, seed=rank)
+    cfg = capi.assembly_config(radius=1, p=0.05, sigma=0.02)
+    width = start
+    per_width = {}
+    total_steps, total_s = 0, 0.0
+    with ClockSampler(local) as clocks:
+        for g in range(generations):
+            counts = capi.word_counts(training=start, action_space=width)
+            pending = None
+            if g in widen_at:
+                pending = capi.PendingInjection(True, width, widen_at[g] - width)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            rt.advance_graphed(seed=9000 + g, counts=counts, config=cfg, pending=pending)
+            torch.cuda.synchronize()
+            dt = time.perf_counter() - t0
+            steps = rt.stats().game_steps
+            total_steps += steps
+            total_s += dt
+            row = per_width.setdefault(width, {"generations": 0, "game_steps": 0, "seconds": 0.0})
+            row["generations"] += 1
+            row["game_steps"] += steps
+            row["seconds"] += dt
+            if pending is not None:
+                width = widen_at[g]
+                n = len(rt.current_generation()["slots"])
+                rt.set_cell_words(offsets[:n + 1], words[:offsets[n]])
+    tuning = {}
+    for w in per_width:
+        t = rt.launch_tuning(width=w)
+        tuning[w] = {"decided": bool(t.decided), "eval_ctas": t.eval_ctas, "breed_warps": t.breed_warps,
+                     "eval_ms": [round(x, 3) for x in t.eval_ms], "breed_ms": [round(x, 3) for x in t.breed_ms]}
+    gi = rt.graph_info()
+    value = sum_over_ranks(float(total_steps), world) / max_over_ranks(total_s, world)
+    if rank == 0:
+        print(json.dumps({
+            "metric": "game-steps/s", "value": value, "unit": "game-steps/s", "n_gpus": world, "steps": generations,
+            "warmup": 0, "ms_per_step": 1e3 * total_s / generations, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": DTYPES[args.form], "data": "synthetic", "impl": "ours",
+            "generations_per_s": generations / total_s,
+            "config": {"workload": "p16384_grid128_a1024to4739_loguniform32to1024", "population": population,
+                       "grid": "128x128", "action_width": f"{start} -> {final} in steps of {step}",
+                       "widen_at_generation": widen_at, "secrets_per_cell": "floor(exp(U[ln 32, ln 1024]))",
+                       "secret_words": f"the first {start} catalog words", "form": FORM_NAMES[args.form],
+                       "margin_tau": args.tau, "timing": "host clock around each generation, device synchronised",
+                       "final_population": len(rt.current_generation()["slots"]), "final_width": width},
+            "per_width": {w: {**r, "game_steps_per_s": r["game_steps"] / r["seconds"]} for w, r in per_width.items()},
+            "launch_tuning": tuning,
+            "graphs": {"launches": gi.launches, "instantiations": gi.instantiations, "updates": gi.updates},
+            "clocks": clocks.summary(),
+        }), flush=True)
+    rt.close()
+
+
 def run_reference(args) -> None:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -504,6 +590,10 @@ def run_reference(args) -> None:
     from oracle import pyoracle as O
 
     nwg_workload = importlib.import_module("neuroevolutionary-wordle_b200.workload")
+    if args.workload == "growth":
+        print(json.dumps({"impl": "reference", "unavailable": "the reference's CPU path has no widening run to time; "
+                          "its arm is measured on the full workload"}))
+        return
     wl = {"full": nwg_workload.FULL, "medium": nwg_workload.MEDIUM, "small": nwg_workload.SMALL}[args.workload]
     if O.ref_host() is None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref_host.so was not built"}))
@@ -552,7 +642,8 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["full", "medium", "small"], default="full")
+    ap.add_argument("--workload", choices=["full", "medium", "small", "growth"], default="full",
+                    help="growth: the batching form (16,384 individuals, uneven shards, widening action space)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--form", choices=sorted(FORMS), default="tc-trunk-fp16")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP32 comparison and the agreement sample")
@@ -562,6 +653,8 @@ def main() -> None:
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "growth":
+        run_growth(args)
     else:
         run_ours(args)
 

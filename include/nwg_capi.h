@@ -244,6 +244,47 @@ int nwg_advance(nwg_runtime *runtime, uint32_t generation_seed, const nwg_runtim
                 nwg_post_fitness_fn post_fitness, void *post_fitness_user, nwg_shard_release_fn shard_release,
                 void *shard_release_user, const nwg_shard_release_history *history);
 
+/* Whether each word (5 letter indices 0..25) has the hint-grid group an injection needs (wordle/hint_grid.hpp:76-164;
+ * output_embedding_injection.hpp:123-131 rejects an injection of a word without one). Host only: available[i] = 1
+ * or 0. NWG_INVALID_RUNTIME_CONFIG for a letter out of range. */
+int nwg_hint_groups_available(const uint8_t *letters, size_t count, uint8_t *available);
+
+/* Graphed generation step (no reference counterpart): the same generation as nwg_advance without callbacks or
+ * shard history, with its device work (evaluation, summary, selection, slot plan, breeding and mutation) captured
+ * as one CUDA graph and launched once; the host then checks the status and swaps the generations. The graph is
+ * captured from the same launch code every generation and updated into one executable graph, so the children
+ * and fitness are those of nwg_advance bit for bit. A pending injection runs as nwg_advance (the widening
+ * generation is not graphed). When the runtime's stream is the legacy default stream, the graph runs on a
+ * stream of the runtime's own after the default stream has drained.
+ * While tuning is on (the default), the first three generations at each (action width, form) try launch shapes in
+ * turn (two or one persistent evaluation CTAs per SM, 4, 8 or 16 children per breeding CTA), timing each kernel
+ * with CUDA events, and every later generation at that width uses the fastest; once one CTA per SM has lost by
+ * more than 20% for a form, later widths time only two. The results do not depend on the shapes. */
+int nwg_advance_graphed(nwg_runtime *runtime, uint32_t generation_seed, const nwg_runtime_word_counts *counts,
+                        const nwg_generation_assembly_config *config, const nwg_pending_injection *pending);
+
+typedef struct {
+    size_t launches;        /* graph launches */
+    size_t instantiations;  /* executable graphs built */
+    size_t updates;         /* executable graph updated in place from a new capture */
+} nwg_graph_info;
+
+int nwg_read_graph_info(const nwg_runtime *runtime, nwg_graph_info *info);
+
+typedef struct {
+    int decided;          /* 1 once every candidate shape has been timed */
+    int trials;           /* graphed generations run at this width and form */
+    int eval_ctas;        /* persistent evaluation CTAs chosen (0: not decided) */
+    int breed_warps;      /* children per breeding CTA chosen (0: not decided) */
+    float eval_ms[2];     /* mean evaluation-kernel time at two and at one CTA per SM (0: not tried) */
+    float breed_ms[3];    /* breeding-kernel time at 4, 8 and 16 children per CTA */
+} nwg_launch_tuning;
+
+/* The tuning state for one action width (the genome's action count) and evaluation form. */
+int nwg_read_launch_tuning(const nwg_runtime *runtime, size_t action_width, int form, nwg_launch_tuning *out);
+/* Turns the launch-shape tuning of nwg_advance_graphed on (default) or off (default shapes). */
+int nwg_set_launch_tuning(nwg_runtime *runtime, int enabled);
+
 /* The two halves of nwg_advance (TryPreparePrebreedingBoundaryOnDevice and TryAssemblePreparedGenerationOnDevice,
  * slab_runtime.cu:1374-1680). prepare evaluates the current generation, runs the callbacks, sizes the next
  * generation and plans its parents; assemble breeds (and, when an injection is pending, widens and injects) the

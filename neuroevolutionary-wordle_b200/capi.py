@@ -101,6 +101,15 @@ class GridShape(C.Structure):
     _fields_ = [(n, _sz) for n in ("row_count", "column_count", "cell_count")]
 
 
+class GraphInfo(C.Structure):
+    _fields_ = [(n, _sz) for n in ("launches", "instantiations", "updates")]
+
+
+class LaunchTuning(C.Structure):
+    _fields_ = [("decided", C.c_int), ("trials", C.c_int), ("eval_ctas", C.c_int), ("breed_warps", C.c_int),
+                ("eval_ms", C.c_float * 2), ("breed_ms", C.c_float * 3)]
+
+
 class CheckpointRecord(C.Structure):
     """nwg_checkpoint: RuntimeCheckpoint (slab_runtime.hpp:86-117) with its vectors as pointers."""
     _fields_ = [("schema_version", C.c_uint32), ("genome_layout_version", C.c_uint32), ("resume_phase", C.c_uint32),
@@ -188,7 +197,8 @@ SHARD_RELEASE_FN = C.CFUNCTYPE(C.c_bool, _vp, C.POINTER(RuntimeWordCounts), C.PO
 EXPORTS = [
     "nwg_abi_version", "nwg_status_string", "nwg_upload_catalog", "nwg_create", "nwg_destroy", "nwg_set_stream",
     "nwg_get_info", "nwg_set_evaluation_form", "nwg_set_margin_guard", "nwg_bootstrap", "nwg_set_cell_words", "nwg_evaluate", "nwg_read_summary",
-    "nwg_read_evaluation_stats", "nwg_advance", "nwg_swap_generations", "nwg_read_status",
+    "nwg_read_evaluation_stats", "nwg_advance", "nwg_advance_graphed", "nwg_hint_groups_available", "nwg_read_graph_info",
+    "nwg_read_launch_tuning", "nwg_set_launch_tuning", "nwg_swap_generations", "nwg_read_status",
     "nwg_download_current_generation", "nwg_download_slot", "nwg_upload_slot", "nwg_upload_current_generation",
     "nwg_download_assembly_plan", "nwg_device_slab", "nwg_evaluate_traced", "nwg_select_parents_device",
     "nwg_breed_device", "nwg_bootstrap_device", "nwg_evaluate_noalloc", "nwg_prepare_generation",
@@ -228,6 +238,12 @@ def lib() -> C.CDLL:
                               C.POINTER(PendingInjection), POST_FITNESS_FN, _vp, SHARD_RELEASE_FN, _vp,
                               C.POINTER(ShardReleaseHistory)]
     L.nwg_prepare_generation.argtypes = L.nwg_advance.argtypes
+    L.nwg_advance_graphed.argtypes = [_vp, C.c_uint32, C.POINTER(RuntimeWordCounts), C.POINTER(AssemblyConfig),
+                                      C.POINTER(PendingInjection)]
+    L.nwg_read_graph_info.argtypes = [_vp, C.POINTER(GraphInfo)]
+    L.nwg_hint_groups_available.argtypes = [_vp, _sz, _vp]
+    L.nwg_read_launch_tuning.argtypes = [_vp, _sz, C.c_int, C.POINTER(LaunchTuning)]
+    L.nwg_set_launch_tuning.argtypes = [_vp, C.c_int]
     L.nwg_assemble_prepared.argtypes = [_vp]
     L.nwg_checkpoint_capture.argtypes = L.nwg_advance.argtypes + [_vp, _sz, C.POINTER(CheckpointRecord)]
     L.nwg_checkpoint_restore.argtypes = [C.POINTER(CheckpointRecord), C.POINTER(_vp)]
@@ -313,6 +329,14 @@ def _np_ptr(a: np.ndarray | None):
     return a.ctypes.data
 
 
+def hint_groups_available(letters: np.ndarray) -> np.ndarray:
+    """Per word (rows of 5 letter indices): whether it has the hint-grid group an injection needs."""
+    words = np.ascontiguousarray(letters, np.uint8).reshape(-1, 5)
+    out = np.zeros(len(words), np.uint8)
+    check(lib().nwg_hint_groups_available(_np_ptr(words), len(words), _np_ptr(out)), "nwg_hint_groups_available")
+    return out.astype(bool)
+
+
 def genome_stride_bytes(action_count: int) -> int:
     """Reference genome image size (genetic_algorithm/genome/dynamic_layout.hpp:30-36)."""
     return 0 if action_count == 0 else ((301056 + 76 * action_count + 1) // 2) * 2
@@ -369,6 +393,7 @@ class Runtime:
         self.action_count = action_count
         self.population = population
         self.columns = columns
+        self._form = FORM_FP32
         self._keep = []
         if stream is not None:
             self.set_stream(stream)
@@ -394,6 +419,7 @@ class Runtime:
 
     def set_form(self, form: int) -> None:
         check(lib().nwg_set_evaluation_form(self.handle, form), "nwg_set_evaluation_form")
+        self._form = form
 
     def set_margin_guard(self, tau: float) -> None:
         check(lib().nwg_set_margin_guard(self.handle, tau), "nwg_set_margin_guard")
@@ -435,6 +461,7 @@ class Runtime:
         rt = cls.__new__(cls)
         rt.handle = handle
         rt._keep = []
+        rt._form = FORM_FP32
         info = rt.info()
         rt.action_count = info.action_count
         rt.population = info.max_generation_size
@@ -454,6 +481,29 @@ class Runtime:
         check(lib().nwg_advance(*self._boundary_args(seed, counts, config, pending, post_fitness, shard_release,
                                                      history)), "nwg_advance")
         self.action_count = self.info().action_count  # an injection widens the action space
+
+    def advance_graphed(self, seed: int, counts: RuntimeWordCounts, config: AssemblyConfig | None = None,
+                        pending: PendingInjection | None = None) -> None:
+        """One generation with its device work launched as a CUDA graph (launch shapes tuned per width)."""
+        check(lib().nwg_advance_graphed(self.handle, seed, C.byref(counts), C.byref(config) if config else None,
+                                        C.byref(pending) if pending else None), "nwg_advance_graphed")
+        self.action_count = self.info().action_count
+
+    def graph_info(self) -> GraphInfo:
+        g = GraphInfo()
+        check(lib().nwg_read_graph_info(self.handle, C.byref(g)), "nwg_read_graph_info")
+        return g
+
+    def launch_tuning(self, width: int | None = None, form: int | None = None) -> LaunchTuning:
+        t = LaunchTuning()
+        info = self.info()
+        check(lib().nwg_read_launch_tuning(self.handle, info.action_count if width is None else width,
+                                           self._form if form is None else form, C.byref(t)),
+              "nwg_read_launch_tuning")
+        return t
+
+    def set_launch_tuning(self, enabled: bool) -> None:
+        check(lib().nwg_set_launch_tuning(self.handle, 1 if enabled else 0), "nwg_set_launch_tuning")
 
     def prepare(self, seed: int, counts: RuntimeWordCounts, config: AssemblyConfig | None = None,
                 pending: PendingInjection | None = None, post_fitness=None, shard_release=None,

@@ -24,9 +24,8 @@
 namespace nwg {
 namespace {
 
-constexpr int kBreedWarps = 8;
-constexpr int kEventCapacity = 256;  // queued hits: one window adds at most 128
 constexpr int kFlushAt = 32;
+constexpr int kEventCapacity = kFlushAt + 128;  // queued hits: fewer than kFlushAt, plus at most 128 per window
 
 struct LayerSpan {
     int weights;
@@ -245,11 +244,13 @@ __device__ void CopyRegion(std::uint8_t *__restrict__ dst, const std::uint8_t *_
     }
 }
 
-__global__ void __launch_bounds__(kBreedWarps * 32) BreedKernel(const BreedParams p) {
-    __shared__ EventList events[kBreedWarps];
+// kWarps children per CTA (one warp each); the child images do not depend on it.
+template <int kWarps>
+__global__ void __launch_bounds__(kWarps * 32) BreedKernel(const BreedParams p) {
+    __shared__ EventList events[kWarps];
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
-    const std::uint32_t child = blockIdx.x * kBreedWarps + warp;
+    const std::uint32_t child = blockIdx.x * kWarps + warp;
     if (child >= p.child_count) {
         return;
     }
@@ -363,11 +364,21 @@ __global__ void __launch_bounds__(kBreedWarps * 32) BreedKernel(const BreedParam
 
 }  // namespace
 
-cudaError_t LaunchBreed(const BreedParams &params, cudaStream_t stream) {
+cudaError_t LaunchBreed(const BreedParams &params, cudaStream_t stream, int warps_per_cta) {
     if (params.child_count == 0) {
         return cudaSuccess;
     }
-    BreedKernel<<<(params.child_count + kBreedWarps - 1) / kBreedWarps, kBreedWarps * 32, 0, stream>>>(params);
+    switch (warps_per_cta) {
+        case 4:
+            BreedKernel<4><<<(params.child_count + 3) / 4, 4 * 32, 0, stream>>>(params);
+            break;
+        case 16:
+            BreedKernel<16><<<(params.child_count + 15) / 16, 16 * 32, 0, stream>>>(params);
+            break;
+        default:
+            BreedKernel<8><<<(params.child_count + 7) / 8, 8 * 32, 0, stream>>>(params);
+            break;
+    }
     return cudaGetLastError();
 }
 

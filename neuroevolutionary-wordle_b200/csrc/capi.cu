@@ -15,6 +15,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <limits>
+#include <map>
 #include <mutex>
 #include <new>
 #include <vector>
@@ -102,6 +103,18 @@ struct nwg_runtime {
     cudaEvent_t eval_begin = nullptr;
     cudaEvent_t eval_end = nullptr;
     std::uint64_t last_episodes = 0;
+    // launch shapes: CTAs of the persistent evaluation kernels (0: scratch_ctas) and children per breeding CTA
+    int eval_ctas = 0;
+    int breed_warps = 8;
+    cudaEvent_t breed_begin = nullptr;
+    cudaEvent_t breed_end = nullptr;
+    // graphed generations (nwg_advance_graphed) and the online launch-shape tuning per (width, form)
+    cudaStream_t own_stream = nullptr;  // capture stream when the caller's stream is the legacy default stream
+    cudaGraphExec_t graph_exec = nullptr;
+    nwg_graph_info graph{};
+    bool autotune = true;
+    std::map<std::uint64_t, nwg_launch_tuning> tuning;
+    std::map<int, bool> single_cta_lost;  // per form: one evaluation CTA per SM lost by more than 20% at some width
     std::size_t last_eval_population = 0;
     std::size_t last_action_count = 0;
     std::size_t last_eval_generation = 0;
@@ -398,7 +411,34 @@ void FreeRuntime(nwg_runtime *rt) {
     if (rt->eval_end != nullptr) {
         cudaEventDestroy(rt->eval_end);
     }
+    if (rt->breed_begin != nullptr) {
+        cudaEventDestroy(rt->breed_begin);
+    }
+    if (rt->breed_end != nullptr) {
+        cudaEventDestroy(rt->breed_end);
+    }
+    if (rt->graph_exec != nullptr) {
+        cudaGraphExecDestroy(rt->graph_exec);
+    }
+    if (rt->own_stream != nullptr) {
+        cudaStreamDestroy(rt->own_stream);
+    }
     delete rt;
+}
+
+// A timing event: a plain record, or an event node of the graph while the stream is being captured.
+cudaError_t RecordEvent(cudaEvent_t event, cudaStream_t stream) {
+    cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+    if (stream != nullptr && cudaStreamIsCapturing(stream, &capture) == cudaSuccess &&
+        capture == cudaStreamCaptureStatusActive) {
+        return cudaEventRecordWithFlags(event, stream, cudaEventRecordExternal);
+    }
+    return cudaEventRecord(event, stream);
+}
+
+// CTAs of the persistent evaluation kernels: the tuned count, never more than the scratch holds.
+int EvalGrid(const nwg_runtime *rt) {
+    return rt->eval_ctas > 0 && rt->eval_ctas < rt->scratch_ctas ? rt->eval_ctas : rt->scratch_ctas;
 }
 
 bool ValidWordCounts(const nwg_runtime_word_counts &wc, std::size_t catalog_count) {
@@ -481,9 +521,9 @@ int EvaluateImpl(nwg_runtime *rt, const nwg_runtime_word_counts *counts, const n
     p.trace_policy = static_cast<float *>(policy);
     // at <= 128 selectable actions every form scores on the reference's tensor-tile path, in the plain kernel
     if (rt->form == NWG_FORM_FP32 || selectable <= 128) {
-        NWG_TRY(cudaEventRecord(rt->eval_begin, rt->stream));
-        NWG_TRY(LaunchEvalFp32(p, rt->scratch_ctas, rt->stream));
-        NWG_TRY(cudaEventRecord(rt->eval_end, rt->stream));
+        NWG_TRY(RecordEvent(rt->eval_begin, rt->stream));
+        NWG_TRY(LaunchEvalFp32(p, EvalGrid(rt), rt->stream));
+        NWG_TRY(RecordEvent(rt->eval_end, rt->stream));
     } else if (rt->form == NWG_FORM_TC_TRUNK_BF16 || rt->form == NWG_FORM_TC_TRUNK_FP16) {
         const bool fp16 = rt->form == NWG_FORM_TC_TRUNK_FP16;
         rt->last_table_pitch = TcTablePitch(static_cast<std::uint32_t>(selectable));
@@ -492,10 +532,10 @@ int EvaluateImpl(nwg_runtime *rt, const nwg_runtime_word_counts *counts, const n
                                     rt->tc_tables, fp16, rt->stream));
         NWG_TRY(LaunchBuildTrunkTables(rt->slab, rt->pitch, rt->cur_slots, population, rt->trunk_tables, fp16,
                                        rt->stream));
-        NWG_TRY(cudaEventRecord(rt->eval_begin, rt->stream));
+        NWG_TRY(RecordEvent(rt->eval_begin, rt->stream));
         NWG_TRY(LaunchEvalTct(p, rt->tc_tables, TcTablePitch(static_cast<std::uint32_t>(selectable)), rt->trunk_tables,
-                              rt->margin_tau, fp16, rt->steps + 5, rt->scratch_ctas, rt->stream));
-        NWG_TRY(cudaEventRecord(rt->eval_end, rt->stream));
+                              rt->margin_tau, fp16, rt->steps + 5, EvalGrid(rt), rt->stream));
+        NWG_TRY(RecordEvent(rt->eval_end, rt->stream));
     } else {
         const bool fp16 = rt->form == NWG_FORM_TC_FP16;
         // |16-bit product - FP32 product| <= (2u + u^2)|p||e| with u = 2^-8 (BF16: p and e rounded) or 2^-11 (FP16:
@@ -505,10 +545,10 @@ int EvaluateImpl(nwg_runtime *rt, const nwg_runtime_word_counts *counts, const n
         NWG_TRY(LaunchBuildTcTables(rt->slab, rt->pitch, rt->cur_slots, population, g_catalog.fixed_t,
                                     static_cast<std::uint32_t>(g_catalog.pad), static_cast<std::uint32_t>(selectable),
                                     rt->tc_tables, fp16, rt->stream));
-        NWG_TRY(cudaEventRecord(rt->eval_begin, rt->stream));
+        NWG_TRY(RecordEvent(rt->eval_begin, rt->stream));
         NWG_TRY(LaunchEvalTc(p, rt->tc_tables, TcTablePitch(static_cast<std::uint32_t>(selectable)), kappa, fp16,
-                             rt->steps + 3, rt->scratch_ctas, rt->stream));
-        NWG_TRY(cudaEventRecord(rt->eval_end, rt->stream));
+                             rt->steps + 3, EvalGrid(rt), rt->stream));
+        NWG_TRY(RecordEvent(rt->eval_end, rt->stream));
     }
     NWG_TRY(LaunchFinalizeFitness(rt->score_sum, rt->local_words, population, rt->cur_fitness, rt->cur_eval,
                                   rt->cur_has, rt->status, rt->stream));
@@ -1379,6 +1419,71 @@ int nwg_prepare_generation(nwg_runtime *rt, uint32_t generation_seed, const nwg_
     return kOk;
 }
 
+namespace {
+
+// The device work of assembling planned children without injection: slot plan, breeding, cleared next arrays.
+cudaError_t AssembleLaunch(nwg_runtime *rt, std::uint32_t generation_seed, const nwg_generation_assembly_config &cfg,
+                           std::size_t next_size) {
+    PlanChildSlotsKernel<<<1, 1024, 0, rt->stream>>>(rt->pairs, static_cast<std::uint32_t>(next_size), rt->cur_slots,
+                                                     static_cast<std::uint32_t>(rt->cur_gen_size), rt->slot_used,
+                                                     static_cast<std::uint32_t>(rt->slot_count), rt->next_slots,
+                                                     rt->status);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        return e;
+    }
+    BreedParams bp{};
+    bp.parent_slab = rt->slab;
+    bp.parent_pitch = rt->pitch;
+    bp.parent_slots = rt->cur_slots;
+    bp.child_slab = rt->slab;
+    bp.child_pitch = rt->pitch;
+    bp.child_slots = rt->next_slots;
+    bp.pairs = rt->pairs;
+    bp.child_count = static_cast<std::uint32_t>(next_size);
+    bp.action_count = static_cast<std::uint32_t>(rt->action_count);
+    bp.generation_seed = generation_seed;
+    bp.generation_index = rt->cur_gen_index;
+    bp.crossover_l1 = cfg.breeding.crossover_temperature_level1;
+    bp.crossover_l2 = cfg.breeding.crossover_temperature_level2;
+    bp.crossover_l3 = cfg.breeding.crossover_temperature_level3;
+    bp.mutation_probability = cfg.mutation.mutation_probability;
+    bp.mutation_sigma = cfg.mutation.mutation_sigma;
+    bp.row_scale_probability = cfg.mutation.output_tail_row_scale_mutation_probability;
+    bp.status = rt->status;
+    if (rt->breed_begin != nullptr &&
+        (e = RecordEvent(rt->breed_begin, rt->stream)) != cudaSuccess) {
+        return e;
+    }
+    if ((e = LaunchBreed(bp, rt->stream, rt->breed_warps)) != cudaSuccess) {
+        return e;
+    }
+    if (rt->breed_end != nullptr &&
+        (e = RecordEvent(rt->breed_end, rt->stream)) != cudaSuccess) {
+        return e;
+    }
+    if ((e = cudaMemsetAsync(rt->next_fitness, 0, rt->max_generation_size * sizeof(float), rt->stream)) !=
+            cudaSuccess ||
+        (e = cudaMemsetAsync(rt->next_eval, 0, rt->max_generation_size * sizeof(std::uint32_t), rt->stream)) !=
+            cudaSuccess) {
+        return e;
+    }
+    return cudaMemsetAsync(rt->next_has, 0, rt->max_generation_size, rt->stream);
+}
+
+// Waits for the assembly, then makes the children the current generation.
+int AssembleFinish(nwg_runtime *rt, std::size_t next_size) {
+    const int st = Sync(rt);
+    if (st != kOk) {
+        return st;
+    }
+    rt->next_gen_index = rt->cur_gen_index + 1;
+    rt->next_gen_size = next_size;
+    return nwg_swap_generations(rt);
+}
+
+}  // namespace
+
 // TryAssemblePreparedGenerationOnDevice (slab_runtime.cu:1511-1680): breed (and inject) the planned children,
 // then swap generations.
 int nwg_assemble_prepared(nwg_runtime *rt) {
@@ -1404,41 +1509,8 @@ int nwg_assemble_prepared(nwg_runtime *rt) {
         return AdvanceWithInjection(rt, generation_seed, cfg, injection, hints, rt->prepared_next_action_count,
                                     next_size);
     }
-    PlanChildSlotsKernel<<<1, 1024, 0, rt->stream>>>(rt->pairs, static_cast<std::uint32_t>(next_size), rt->cur_slots,
-                                                     static_cast<std::uint32_t>(rt->cur_gen_size), rt->slot_used,
-                                                     static_cast<std::uint32_t>(rt->slot_count), rt->next_slots,
-                                                     rt->status);
-    NWG_TRY(cudaGetLastError());
-    BreedParams bp{};
-    bp.parent_slab = rt->slab;
-    bp.parent_pitch = rt->pitch;
-    bp.parent_slots = rt->cur_slots;
-    bp.child_slab = rt->slab;
-    bp.child_pitch = rt->pitch;
-    bp.child_slots = rt->next_slots;
-    bp.pairs = rt->pairs;
-    bp.child_count = static_cast<std::uint32_t>(next_size);
-    bp.action_count = static_cast<std::uint32_t>(rt->action_count);
-    bp.generation_seed = generation_seed;
-    bp.generation_index = rt->cur_gen_index;
-    bp.crossover_l1 = cfg.breeding.crossover_temperature_level1;
-    bp.crossover_l2 = cfg.breeding.crossover_temperature_level2;
-    bp.crossover_l3 = cfg.breeding.crossover_temperature_level3;
-    bp.mutation_probability = cfg.mutation.mutation_probability;
-    bp.mutation_sigma = cfg.mutation.mutation_sigma;
-    bp.row_scale_probability = cfg.mutation.output_tail_row_scale_mutation_probability;
-    bp.status = rt->status;
-    NWG_TRY(LaunchBreed(bp, rt->stream));
-    NWG_TRY(cudaMemsetAsync(rt->next_fitness, 0, rt->max_generation_size * sizeof(float), rt->stream));
-    NWG_TRY(cudaMemsetAsync(rt->next_eval, 0, rt->max_generation_size * sizeof(std::uint32_t), rt->stream));
-    NWG_TRY(cudaMemsetAsync(rt->next_has, 0, rt->max_generation_size, rt->stream));
-    const int st = Sync(rt);
-    if (st != kOk) {
-        return st;
-    }
-    rt->next_gen_index = rt->cur_gen_index + 1;
-    rt->next_gen_size = next_size;
-    return nwg_swap_generations(rt);
+    NWG_TRY(AssembleLaunch(rt, generation_seed, cfg, next_size));
+    return AssembleFinish(rt, next_size);
 }
 
 int nwg_advance(nwg_runtime *rt, uint32_t generation_seed, const nwg_runtime_word_counts *counts,
@@ -1448,6 +1520,174 @@ int nwg_advance(nwg_runtime *rt, uint32_t generation_seed, const nwg_runtime_wor
     const int st = nwg_prepare_generation(rt, generation_seed, counts, config, pending, post_fitness, post_fitness_user,
                                           shard_release, shard_release_user, history);
     return st != kOk ? st : nwg_assemble_prepared(rt);
+}
+
+namespace {
+
+constexpr int kBreedWarpChoices[3] = {4, 8, 16};
+
+std::uint64_t TuningKey(std::size_t width, int form) { return (static_cast<std::uint64_t>(width) << 8) | (form & 0xFF); }
+
+}  // namespace
+
+int nwg_advance_graphed(nwg_runtime *rt, uint32_t generation_seed, const nwg_runtime_word_counts *counts,
+                        const nwg_generation_assembly_config *config, const nwg_pending_injection *pending) {
+    if (rt == nullptr || counts == nullptr) {
+        return kInvalidRuntimeConfig;
+    }
+    if (pending != nullptr && pending->enabled) {
+        return nwg_advance(rt, generation_seed, counts, config, pending, nullptr, nullptr, nullptr, nullptr, nullptr);
+    }
+    if (rt->breed_begin == nullptr) {
+        NWG_TRY(cudaEventCreate(&rt->breed_begin));
+        NWG_TRY(cudaEventCreate(&rt->breed_end));
+    }
+    // stream capture needs a stream other than the legacy default stream
+    const cudaStream_t caller = rt->stream;
+    if (caller == nullptr) {
+        if (rt->own_stream == nullptr) {
+            NWG_TRY(cudaStreamCreateWithFlags(&rt->own_stream, cudaStreamNonBlocking));
+        }
+        NWG_TRY(cudaStreamSynchronize(nullptr));
+        rt->stream = rt->own_stream;
+    }
+    // launch shapes of this generation
+    nwg_launch_tuning &tune = rt->tuning[TuningKey(rt->action_count, rt->form)];
+    const bool trial = rt->autotune && !tune.decided;
+    const bool try_single = !rt->single_cta_lost[rt->form];
+    if (trial) {
+        rt->eval_ctas = tune.trials % 2 == 1 && try_single ? std::max(1, rt->scratch_ctas / 2) : rt->scratch_ctas;
+        rt->breed_warps = kBreedWarpChoices[tune.trials % 3];
+    } else if (rt->autotune) {
+        rt->eval_ctas = tune.eval_ctas;
+        rt->breed_warps = tune.breed_warps;
+    } else {
+        rt->eval_ctas = 0;
+        rt->breed_warps = 8;
+    }
+    auto restore = [&](int status) {
+        rt->stream = caller;
+        rt->eval_ctas = 0;
+        rt->breed_warps = 8;
+        return status;
+    };
+    // capture: prepare (no callbacks, so it never waits on the device) and the assembly's device work
+    cudaGraph_t graph = nullptr;
+    if (cudaStreamBeginCapture(rt->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        return restore(kCudaFailure);
+    }
+    int st = nwg_prepare_generation(rt, generation_seed, counts, config, nullptr, nullptr, nullptr, nullptr, nullptr,
+                                    nullptr);
+    const std::uint32_t seed = rt->prepared_seed;
+    const nwg_generation_assembly_config cfg = rt->prepared_config;
+    const std::size_t next_size = rt->planned_children;
+    if (st == kOk) {
+        rt->prepared = false;
+        if (AssembleLaunch(rt, seed, cfg, next_size) != cudaSuccess) {
+            st = kCudaFailure;
+        }
+    }
+    const cudaError_t end = cudaStreamEndCapture(rt->stream, &graph);
+    if (st != kOk || end != cudaSuccess || graph == nullptr) {
+        if (graph != nullptr) {
+            cudaGraphDestroy(graph);
+        }
+        cudaGetLastError();
+        rt->prepared = false;
+        // a rejected call leaves the same status behind as nwg_advance does
+        return restore(st != kOk ? SetHostStatus(rt, st) : kCudaFailure);
+    }
+    cudaGraphExecUpdateResultInfo info{};
+    if (rt->graph_exec != nullptr && cudaGraphExecUpdate(rt->graph_exec, graph, &info) == cudaSuccess) {
+        ++rt->graph.updates;
+    } else {
+        cudaGetLastError();  // a failed update is not an error of the run: instantiate afresh
+        if (rt->graph_exec != nullptr) {
+            cudaGraphExecDestroy(rt->graph_exec);
+            rt->graph_exec = nullptr;
+        }
+        if (cudaGraphInstantiate(&rt->graph_exec, graph, 0) != cudaSuccess) {
+            cudaGraphDestroy(graph);
+            rt->graph_exec = nullptr;
+            return restore(kCudaFailure);
+        }
+        ++rt->graph.instantiations;
+    }
+    cudaGraphDestroy(graph);
+    if (cudaGraphLaunch(rt->graph_exec, rt->stream) != cudaSuccess) {
+        return restore(kCudaFailure);
+    }
+    ++rt->graph.launches;
+    st = AssembleFinish(rt, next_size);
+    if (st == kOk && trial) {
+        float eval_ms = 0.0f, breed_ms = 0.0f;
+        if (cudaEventElapsedTime(&eval_ms, rt->eval_begin, rt->eval_end) == cudaSuccess &&
+            cudaEventElapsedTime(&breed_ms, rt->breed_begin, rt->breed_end) == cudaSuccess) {
+            // running mean per evaluation shape (two CTAs per SM on trials 0 and 2, and on trial 1 too once one CTA
+            // per SM has lost by a wide margin)
+            const int e = tune.trials % 2 == 1 && try_single ? 1 : 0;
+            const int n_before = e == 1 ? 0 : (try_single ? tune.trials / 2 : tune.trials);
+            tune.eval_ms[e] += (eval_ms - tune.eval_ms[e]) / static_cast<float>(n_before + 1);
+            tune.breed_ms[tune.trials % 3] = breed_ms;
+            ++tune.trials;
+            if (tune.trials == 3) {
+                tune.decided = 1;
+                const bool single = tune.eval_ms[1] > 0.0f && tune.eval_ms[1] < tune.eval_ms[0];
+                tune.eval_ctas = single ? std::max(1, rt->scratch_ctas / 2) : rt->scratch_ctas;
+                if (tune.eval_ms[1] > 1.2f * tune.eval_ms[0]) {
+                    rt->single_cta_lost[rt->form] = true;
+                }
+                int best = 0;
+                for (int b = 1; b < 3; ++b) {
+                    best = tune.breed_ms[b] < tune.breed_ms[best] ? b : best;
+                }
+                tune.breed_warps = kBreedWarpChoices[best];
+            }
+        }
+        cudaGetLastError();
+    }
+    return restore(st);
+}
+
+int nwg_hint_groups_available(const uint8_t *letters, size_t count, uint8_t *available) {
+    if (count > 0 && (letters == nullptr || available == nullptr)) {
+        return kInvalidRuntimeConfig;
+    }
+    for (std::size_t i = 0; i < count; ++i) {
+        for (int k = 0; k < kWordLength; ++k) {
+            if (letters[i * kWordLength + k] >= kAlphabet) {
+                return kInvalidRuntimeConfig;
+            }
+        }
+        HintGroup g;
+        available[i] = BuildHintGroup(PackWord(letters + i * kWordLength), g) ? 1 : 0;
+    }
+    return kOk;
+}
+
+int nwg_read_graph_info(const nwg_runtime *rt, nwg_graph_info *info) {
+    if (rt == nullptr || info == nullptr) {
+        return kInvalidRuntimeConfig;
+    }
+    *info = rt->graph;
+    return kOk;
+}
+
+int nwg_read_launch_tuning(const nwg_runtime *rt, size_t action_width, int form, nwg_launch_tuning *out) {
+    if (rt == nullptr || out == nullptr) {
+        return kInvalidRuntimeConfig;
+    }
+    const auto it = rt->tuning.find(TuningKey(action_width, form));
+    *out = it == rt->tuning.end() ? nwg_launch_tuning{} : it->second;
+    return kOk;
+}
+
+int nwg_set_launch_tuning(nwg_runtime *rt, int enabled) {
+    if (rt == nullptr) {
+        return kInvalidRuntimeConfig;
+    }
+    rt->autotune = enabled != 0;
+    return kOk;
 }
 
 int nwg_swap_generations(nwg_runtime *rt) {

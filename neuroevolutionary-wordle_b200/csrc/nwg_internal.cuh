@@ -153,7 +153,7 @@ struct BreedParams {
     float mutation_probability, mutation_sigma, row_scale_probability;
     int *status;
 };
-cudaError_t LaunchBreed(const BreedParams &params, cudaStream_t stream);
+cudaError_t LaunchBreed(const BreedParams &params, cudaStream_t stream, int warps_per_cta = 8);
 
 // ---- output-embedding injection (action-space growth) ----
 cudaError_t LaunchInject(std::uint8_t *slab, std::size_t pitch, const std::uint32_t *child_slots,

@@ -75,3 +75,17 @@ def test_injection_rejects_a_bad_range():
     genome = H.random_genome(rng, 50)
     assert O.inject_tails(genome, 40, catalog, 41, 3)[0] == 2  # must start at the parent's action count
     assert O.inject_tails(genome, 40, catalog, 40, 20)[0] == 1  # beyond the catalog
+
+
+def test_library_hint_group_availability_matches_oracle():
+    """nwg_hint_groups_available (host code of the library) agrees with the oracle's hint-grid construction."""
+    import importlib
+
+    nwg = importlib.import_module("neuroevolutionary-wordle_b200")
+    rng = np.random.default_rng(17)
+    words = np.concatenate([rng.integers(0, 26, (3000, 5)), rng.integers(0, 3, (500, 5)),
+                            np.array([[0, 0, 0, 0, 0], [1, 1, 1, 1, 2], [0, 1, 0, 1, 0], [2, 3, 4, 5, 6]])]).astype(np.uint8)
+    got = nwg.capi.hint_groups_available(words)
+    want = np.array([O.hint_grid_group(w) is not None for w in words])
+    assert np.array_equal(got, want)
+    assert not got[-4] and got[-1]  # a monochrome word has none; five distinct letters always do
