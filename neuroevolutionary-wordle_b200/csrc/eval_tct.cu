@@ -86,6 +86,18 @@ constexpr int kStageLd = 66;   // halfs per staged 64-wide weight row (33 words:
 constexpr int kStageLd3 = 130; // halfs per staged W3 row (65 words)
 static_assert(kOffXStage + kHidden0 * kStageLd * 2 <= kSmemBytes, "staged layer-1 slice");
 static_assert(kOffXStage + kPolicy * kStageLd3 * 2 <= kSmemBytes, "staged W3");
+// FP16 form: the exact path streams its weights from the trunk table (the genome's FP16 values in K-major
+// canonical tiles) through a ring of three 16 KB buffers: page 0 (its 16-bit policy rows saved first) and two
+// buffers in the staging area; the saved rows follow them.
+constexpr int kRing = 3;
+constexpr int kRingTileBytes = 16384;
+constexpr int kOffRing1 = kOffXStage;
+constexpr int kOffRing2 = kOffRing1 + kRingTileBytes;
+constexpr int kOffSavedRows = kOffRing2 + kRingTileBytes;  // [games][64] 16-bit policy values
+constexpr int kMaxSavedRows = (kSmemBytes - kOffSavedRows) / (kPolicy * 2);
+static_assert(kOffXP + kFallbackBatch * kPolicy * 4 <= kOffRing1, "ring buffers after the fallback activations");
+static_assert(kMaxSavedRows >= 64, "saved policy rows");
+constexpr int kWe1GroupBytes = 8 * kKe1 * 2;  // 8 rows of W_e1 in the canonical layout
 
 struct TctState {
     std::uint64_t bar_load[kPages];  // bulk loads into page p (at most one outstanding per barrier)
@@ -93,6 +105,7 @@ struct TctState {
     std::uint64_t bar_mma;           // a trunk phase's MMAs have completed
     std::uint64_t bar_acc[2];        // scoring accumulator buffers
     std::uint64_t bar_drain;
+    std::uint64_t bar_ring[kRing];   // exact-path weight tiles (FP16 form)
     std::uint32_t tmem_base;
     int failed;
     int n_fallback;
@@ -258,6 +271,8 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
     unsigned long long cand_chunks = 0, fallback_steps = 0, exact_chunks = 0, exact_rows = 0;
     // thread 0 only: bulk loads issued / waited per barrier, commits per stage barrier
     std::uint32_t load_issued[kPages] = {0, 0, 0, 0, 0, 0};
+    std::uint32_t ring_issued[kRing] = {0, 0, 0};  // thread 0: exact-path weight tiles issued per ring buffer
+    std::uint32_t ring_waited[kRing] = {0, 0, 0};  // every thread: waits per ring buffer
     std::uint32_t load_waited[kPages] = {0, 0, 0, 0, 0, 0};
     std::uint32_t free_commits[2] = {0, 0};
     // every thread: commits to the phase and accumulator barriers
@@ -282,6 +297,9 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
         umma::MbarInit(&ts.bar_acc[0], 1);
         umma::MbarInit(&ts.bar_acc[1], 1);
         umma::MbarInit(&ts.bar_drain, 1);
+        for (int b = 0; b < kRing; ++b) {
+            umma::MbarInit(&ts.bar_ring[b], 1);
+        }
         ts.failed = 0;
     }
     umma::FenceBeforeSync();
@@ -891,8 +909,290 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
                 reinterpret_cast<const __half *>(reinterpret_cast<const std::uint8_t *>(gh) + kTailOffsetBytes);
             const float *cand_v = reinterpret_cast<const float *>(smem + kOffCandV);
             const int *cand_id = reinterpret_cast<const int *>(smem + kOffCandId);
+            // FP16 form with few fallback games: weights streamed from the trunk table (see fallback_trunk_ring)
+            const bool ring = kFp16 && nf <= kMaxSavedRows;
+            std::uint8_t *saved = smem + kOffSavedRows;
+            if (ring) {
+                for (int i = tid; i < nf * 8; i += kEvalThreads) {
+                    const int g = ts.fallback_games[i >> 3];
+                    reinterpret_cast<uint4 *>(saved)[i] =
+                        *reinterpret_cast<const uint4 *>(page(0) + umma::TileOffset(g, (i & 7) * 8, kPolicy));
+                }
+                __syncthreads();
+            }
+            // the 16-bit policy value pair (k, k + 1) of fallback game number fi, game row g
+            auto policy16 = [&](int fi, int g, int k) {
+                return ring ? *reinterpret_cast<const std::uint32_t *>(saved + fi * kPolicy * 2 + k * 2)
+                            : *reinterpret_cast<const std::uint32_t *>(page(0) + umma::TileOffset(g, k, kPolicy));
+            };
+            // The exact trunk of batch games b0 .. b0 + nb - 1 into xp, the plain form's FP32 chains in their order,
+            // with every weight tile copied in by bulk copies two tiles ahead of its use: W_e1 in three row
+            // groups, W_e2, then per turn the two 128-row halves of its W1 slot, the four K-chunks of W2, and W3.
+            auto fallback_trunk_ring = [&](int b0, int nb) {
+                float *hid = reinterpret_cast<float *>(smem + kOffXHid);
+                float *enc = reinterpret_cast<float *>(smem + kOffXEnc);
+                float *x0 = reinterpret_cast<float *>(smem + kOffXH0);
+                float *x1 = reinterpret_cast<float *>(smem + kOffXH1);
+                float *xp = reinterpret_cast<float *>(smem + kOffXP);
+                const int enc_tiles = t > 0 ? 4 : 0;
+                const int n_tiles = enc_tiles + 2 * t + 5;
+                auto buffer = [&](int i) { return i % kRing == 0 ? page(0) : smem + (i % kRing == 1 ? kOffRing1 : kOffRing2); };
+                auto issue = [&](int i) {  // thread 0
+                    int kind = i < enc_tiles ? (i < 3 ? 0 : 1) : (i - enc_tiles < 2 * t ? 2 : (i - enc_tiles - 2 * t < 4 ? 3 : 4));
+                    std::size_t off = 0;
+                    std::uint32_t bytes = kRingTileBytes;
+                    if (kind == 0) {
+                        off = kTblWe1 + static_cast<std::size_t>(i) * 6 * kWe1GroupBytes;
+                        bytes = (i < 2 ? 6 : 4) * kWe1GroupBytes;
+                    } else if (kind == 1) {
+                        off = kTblWe2;
+                    } else if (kind == 2) {
+                        off = kTblW1 + static_cast<std::size_t>(i - enc_tiles) * kRingTileBytes;
+                    } else if (kind == 3) {
+                        off = kTblW2 + static_cast<std::size_t>(i - enc_tiles - 2 * t) * kW2ChunkBytes;
+                    } else {
+                        off = kTblW3;
+                    }
+                    BulkLoad(buffer(i), ttab + off, bytes, &ts.bar_ring[i % kRing]);
+                    ++ring_issued[i % kRing];
+                };
+                if (tid == 0) {
+                    umma::FenceProxyAsyncShared();
+                    for (int i = 0; i < kRing && i < n_tiles; ++i) {
+                        issue(i);
+                    }
+                }
+                // layer-1 accumulators: output o_local (+128 h) for games sub, sub + 2, sub + 4, sub + 6
+                const int o_local = tid & 127;
+                const int sub = tid >> 7;
+                float acc1a[4], acc1b[4];  // rows o_local and 128 + o_local
+                {
+                    const float init_a = t == 0 ? __fmaf_rn(H2F(gh, kTrW1 + o_local * kModelInput), 1.0f,
+                                                            ts.b1[o_local])
+                                                : ts.b1[o_local];
+                    const int ob = 128 + o_local;
+                    const float init_b =
+                        t == 0 ? __fmaf_rn(H2F(gh, kTrW1 + ob * kModelInput), 1.0f, ts.b1[ob]) : ts.b1[ob];
+#pragma unroll
+                    for (int r = 0; r < 4; ++r) {
+                        acc1a[r] = init_a;
+                        acc1b[r] = init_b;
+                    }
+                }
+                // a batch of at most two games needs one chain per thread (game sub), otherwise four
+                const bool pair = nb <= 2;
+                auto layer1_rows = [&](float (&acc)[4], const std::uint8_t *w, int u) {
+                    const std::uint8_t *wrow = w + (o_local >> 3) * 1024 + (o_local & 7) * 16;
+                    if (pair) {
+                        const float *x = enc + ((sub < nb ? sub : 0) * 5 + u) * kEncoderOut;
+                        for (int k8 = 0; k8 < kEncoderOut / 8; ++k8) {
+                            const uint4 w8 = *reinterpret_cast<const uint4 *>(wrow + k8 * 128);
+                            const __half *h8 = reinterpret_cast<const __half *>(&w8);
+#pragma unroll
+                            for (int e = 0; e < 8; ++e) {
+                                acc[0] = __fmaf_rn(x[k8 * 8 + e], __half2float(h8[e]), acc[0]);
+                            }
+                        }
+                        return;
+                    }
+                    for (int k8 = 0; k8 < kEncoderOut / 8; ++k8) {
+                        const uint4 w8 = *reinterpret_cast<const uint4 *>(wrow + k8 * 128);
+                        const __half *h8 = reinterpret_cast<const __half *>(&w8);
+#pragma unroll
+                        for (int e = 0; e < 8; ++e) {
+                            const float wv = __half2float(h8[e]);
+#pragma unroll
+                            for (int r = 0; r < 4; ++r) {
+                                const int f = sub + 2 * r;
+                                const int fs = f < nb ? f : 0;
+                                acc[r] = __fmaf_rn(enc[(fs * 5 + u) * kEncoderOut + k8 * 8 + e], wv, acc[r]);
+                            }
+                        }
+                    }
+                };
+                auto store_x0 = [&]() {
+#pragma unroll
+                    for (int r = 0; r < 4; ++r) {
+                        const int f = sub + 2 * r;
+                        if (f < nb) {
+                            x0[f * kHidden0 + o_local] = acc1a[r] < 0.0f ? 0.0f : acc1a[r];
+                            x0[f * kHidden0 + 128 + o_local] = acc1b[r] < 0.0f ? 0.0f : acc1b[r];
+                        }
+                    }
+                };
+                float acc2[4];
+#pragma unroll
+                for (int r = 0; r < 4; ++r) {
+                    acc2[r] = ts.b2[o_local];
+                }
+                for (int i = 0; i < n_tiles; ++i) {
+                    const int b = i % kRing;
+                    wait_bar(&ts.bar_ring[b], ring_waited[b] & 1u);
+                    ++ring_waited[b];
+                    const std::uint8_t *w = buffer(i);
+                    if (i < enc_tiles && i < 3) {
+                        // encoder hidden rows of this group: EncodeRound's gather chain, ascending feature order
+                        const int r0 = i * 48;
+                        const int rows = i < 2 ? 48 : 32;
+                        for (int idx = tid; idx < nb * t * rows; idx += kEvalThreads) {
+                            const int ol = idx % rows;
+                            const int fu = idx / rows;
+                            const int f = fu / t;
+                            const int u = fu - f * t;
+                            const int o = r0 + ol;
+                            const int g = ts.fallback_games[b0 + f];
+                            const std::uint32_t code = cs.guess[u][g];
+                            const std::uint32_t tiles = cs.tiles[u][g];
+                            const std::uint8_t *row = w + (ol >> 3) * kWe1GroupBytes + (o & 7) * 16;
+                            auto we1 = [&](int feature) {
+                                return __half2float(*reinterpret_cast<const __half *>(row + (feature >> 3) * 128 +
+                                                                                     (feature & 7) * 2));
+                            };
+                            float hsum = ts.be1[o];
+                            for (int pos = 0; pos < kWordLength; ++pos) {
+                                hsum = __fmaf_rn(we1(pos * kAlphabet + static_cast<int>(WordLetter(code, pos))), 1.0f,
+                                                 hsum);
+                            }
+                            for (int pos = 0; pos < kWordLength; ++pos) {
+                                hsum = __fmaf_rn(we1(kWordLength * kAlphabet + pos * 3 +
+                                                     static_cast<int>((tiles >> (2 * pos)) & 3u)),
+                                                 1.0f, hsum);
+                            }
+                            hid[(f * 5 + u) * kEncoderHidden + o] = hsum < 0.0f ? 0.0f : hsum;
+                        }
+                    } else if (i < enc_tiles) {
+                        // encoder output: thread (j, group), five chains at once, 8 weights per 16-byte read
+                        const int j = tid & (kEncoderOut - 1);
+                        const int grp = tid >> 6;
+                        const int pairs = nb * t;
+                        const std::uint8_t *wrow = w + (j >> 3) * (kEncoderHidden / 8) * 128 + (j & 7) * 16;
+                        for (int q0 = grp; q0 < pairs; q0 += 20) {
+                            float acc[5];
+                            int base[5];
+#pragma unroll
+                            for (int r = 0; r < 5; ++r) {
+                                const int qq = q0 + 4 * r;
+                                const int f = qq < pairs ? qq / t : 0;
+                                const int u = qq < pairs ? qq - f * t : 0;
+                                base[r] = (f * 5 + u) * kEncoderHidden;
+                                acc[r] = ts.be2[j];
+                            }
+                            for (int o8 = 0; o8 < kEncoderHidden / 8; ++o8) {
+                                const uint4 w8 = *reinterpret_cast<const uint4 *>(wrow + o8 * 128);
+                                const __half *h8 = reinterpret_cast<const __half *>(&w8);
+#pragma unroll
+                                for (int e = 0; e < 8; ++e) {
+                                    const float wv = __half2float(h8[e]);
+#pragma unroll
+                                    for (int r = 0; r < 5; ++r) {
+                                        acc[r] = __fmaf_rn(hid[base[r] + o8 * 8 + e], wv, acc[r]);
+                                    }
+                                }
+                            }
+#pragma unroll
+                            for (int r = 0; r < 5; ++r) {
+                                const int qq = q0 + 4 * r;
+                                if (qq < pairs) {
+                                    const int f = qq / t;
+                                    const int u = qq - f * t;
+                                    enc[(f * 5 + u) * kEncoderOut + j] = acc[r];
+                                }
+                            }
+                        }
+                    } else if (i - enc_tiles < 2 * t) {
+                        // layer 1, turn u, rows 128 h .. 128 h + 127: the chains continue in ascending input order
+                        const int u = (i - enc_tiles) >> 1;
+                        if (((i - enc_tiles) & 1) == 0) {
+                            layer1_rows(acc1a, w, u);
+                        } else {
+                            layer1_rows(acc1b, w, u);
+                            if (u == t - 1) {
+                                store_x0();
+                            }
+                        }
+                    } else if (i - enc_tiles - 2 * t < 4) {
+                        // layer 2, K-chunk kc: thread (n, parity) over the batch games of its parity
+                        const int kc = i - enc_tiles - 2 * t;
+                        if (kc == 0 && t == 0) {  // no turn: every output is relu(b1 + W1[:, 0])
+                            store_x0();
+                            __syncthreads();
+                        }
+                        const std::uint8_t *wrow = w + (o_local >> 3) * 1024 + (o_local & 7) * 16;
+                        if (pair) {
+                            const float *x = x0 + (sub < nb ? sub : 0) * kHidden0 + kc * 64;
+                            for (int k8 = 0; k8 < 8; ++k8) {
+                                const uint4 w8 = *reinterpret_cast<const uint4 *>(wrow + k8 * 128);
+                                const __half *h8 = reinterpret_cast<const __half *>(&w8);
+#pragma unroll
+                                for (int e = 0; e < 8; ++e) {
+                                    acc2[0] = __fmaf_rn(x[k8 * 8 + e], __half2float(h8[e]), acc2[0]);
+                                }
+                            }
+                        } else {
+                            for (int k8 = 0; k8 < 8; ++k8) {
+                                const uint4 w8 = *reinterpret_cast<const uint4 *>(wrow + k8 * 128);
+                                const __half *h8 = reinterpret_cast<const __half *>(&w8);
+#pragma unroll
+                                for (int e = 0; e < 8; ++e) {
+                                    const float wv = __half2float(h8[e]);
+#pragma unroll
+                                    for (int r = 0; r < 4; ++r) {
+                                        const int f = sub + 2 * r;
+                                        const int fs = f < nb ? f : 0;
+                                        acc2[r] = __fmaf_rn(x0[fs * kHidden0 + kc * 64 + k8 * 8 + e], wv, acc2[r]);
+                                    }
+                                }
+                            }
+                        }
+                        if (kc == 3) {
+#pragma unroll
+                            for (int r = 0; r < 4; ++r) {
+                                const int f = sub + 2 * r;
+                                if (f < nb) {
+                                    x1[f * kHidden1 + o_local] = acc2[r] < 0.0f ? 0.0f : acc2[r];
+                                }
+                            }
+                        }
+                    } else {
+                        // layer 3: thread (j, group of four) over two batch games
+                        const int j = tid & 63;
+                        const int grp = tid >> 6;
+                        float acc[2] = {ts.b3[j], ts.b3[j]};
+                        const std::uint8_t *wrow = w + (j >> 3) * (kHidden1 / 8) * 128 + (j & 7) * 16;
+                        for (int k8 = 0; k8 < kHidden1 / 8; ++k8) {
+                            const uint4 w8 = *reinterpret_cast<const uint4 *>(wrow + k8 * 128);
+                            const __half *h8 = reinterpret_cast<const __half *>(&w8);
+#pragma unroll
+                            for (int e = 0; e < 8; ++e) {
+                                const float wv = __half2float(h8[e]);
+#pragma unroll
+                                for (int r = 0; r < 2; ++r) {
+                                    const int f = grp + 4 * r;
+                                    const int fs = f < nb ? f : 0;
+                                    acc[r] = __fmaf_rn(x1[fs * kHidden1 + k8 * 8 + e], wv, acc[r]);
+                                }
+                            }
+                        }
+#pragma unroll
+                        for (int r = 0; r < 2; ++r) {
+                            const int f = grp + 4 * r;
+                            if (f < nb) {
+                                xp[f * kPolicy + j] = acc[r];
+                            }
+                        }
+                    }
+                    __syncthreads();
+                    if (tid == 0 && i + kRing < n_tiles) {
+                        umma::FenceProxyAsyncShared();
+                        issue(i + kRing);
+                    }
+                }
+            };
             for (int b0 = 0; b0 < nf; b0 += kFallbackBatch) {
                 const int nb = nf - b0 < kFallbackBatch ? nf - b0 : kFallbackBatch;
+                if (ring) {
+                    fallback_trunk_ring(b0, nb);
+                } else {
                 // encoder hidden layer of every turn (EncodeRound's gather chain), W_e1 staged in shared memory
                 {
                     const uint4 *src = reinterpret_cast<const uint4 *>(gh + kEncW1);
@@ -1091,6 +1391,7 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
                         }
                     }
                 }
+                }  // existing staged path
                 if (tid == 0) {
                     *fb_count = 0;
                 }
@@ -1113,8 +1414,7 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
                     float dev = 0.0f;
                     float mag = 0.0f;
                     for (int k = 0; k < kPolicy; k += 2) {
-                        const std::uint32_t bits =
-                            *reinterpret_cast<const std::uint32_t *>(page(0) + umma::TileOffset(g, k, kPolicy));
+                        const std::uint32_t bits = policy16(b0 + f, g, k);
                         const float2 r = Unpack2<kFp16>(bits);
                         dev = __fmaf_rn(fabsf(r.x - xp[f * kPolicy + k]), ts.emax[k], dev);
                         dev = __fmaf_rn(fabsf(r.y - xp[f * kPolicy + k + 1]), ts.emax[k + 1], dev);
@@ -1223,6 +1523,12 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
             while (load_waited[b] < load_issued[b]) {
                 (void)umma::MbarWait(&ts.bar_load[b], load_waited[b] & 1u, 1u << 22);
                 ++load_waited[b];
+            }
+        }
+        for (int b = 0; b < kRing; ++b) {
+            while (ring_waited[b] < ring_issued[b]) {
+                (void)umma::MbarWait(&ts.bar_ring[b], ring_waited[b] & 1u, 1u << 22);
+                ++ring_waited[b];
             }
         }
     }
