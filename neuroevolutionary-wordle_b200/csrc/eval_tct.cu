@@ -217,6 +217,29 @@ __device__ __forceinline__ float ApproxScore(const std::uint8_t *a_tile, int g, 
     return (acc[0] + acc[1]) + (acc[2] + acc[3]);
 }
 
+// Three-input maximum (one sm_100 instruction).
+__device__ __forceinline__ float Max3(float a, float b, float c) {
+    float d;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+
+// Maximum of v[base .. base + 31] in 16 three-input steps.
+__device__ __forceinline__ float Max32(const float (&v)[64], int base) {
+    float m[12];
+#pragma unroll
+    for (int j = 0; j < 10; ++j) {
+        m[j] = Max3(v[base + 3 * j], v[base + 3 * j + 1], v[base + 3 * j + 2]);
+    }
+    m[10] = v[base + 30];
+    m[11] = v[base + 31];
+    const float a = Max3(m[0], m[1], m[2]);
+    const float b = Max3(m[3], m[4], m[5]);
+    const float c = Max3(m[6], m[7], m[8]);
+    const float d = Max3(m[9], m[10], m[11]);
+    return fmaxf(Max3(a, b, c), d);
+}
+
 // Copies `rows` rows of `cols` (a multiple of 32) 16-bit values, source row stride src_ld, destination row
 // stride dst_ld, into shared memory: a warp per row so that each load instruction reads consecutive halfs,
 // with 16 rows' loads issued before any store.
@@ -670,14 +693,8 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
                             }
                         }
                     }
-#pragma unroll
-                    for (int w = 16; w > 0; w >>= 1) {
-#pragma unroll
-                        for (int j = 0; j < w; ++j) {
-                            v[j] = fmaxf(v[j], v[j + w]);
-                            v[32 + j] = fmaxf(v[32 + j], v[32 + j + w]);
-                        }
-                    }
+                    v[0] = Max32(v, 0);
+                    v[32] = Max32(v, 32);
                     InsertTop4(tv, ti, v[0], tile * 4 + half * 2);
                     InsertTop4(tv, ti, v[32], tile * 4 + half * 2 + 1);
                 }
