@@ -479,24 +479,41 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
         };
 
         // ---- trunk at turn count t: leaves the 16-bit policy operand in page 0 ----
+        // ---- trunk at turn count t: leaves the 16-bit policy operand in page 0 ----
+        // Layer 1's 16-bit activations h0 stay in tensor memory as layer 2's A operand: the thread that reads row
+        // r's accumulator columns 128 h .. 128 h + 127 writes their activations, two per column, into columns
+        // 128 h .. 128 h + 63 it has already read, so shared memory holds all of W2 and W3 before layer 2 starts.
+        // Layer 2 then accumulates outputs 0-63 in columns 64-127 and 64-127 in columns 192-255 (N = 64 each).
+        auto load_layer23 = [&]() {  // thread 0: W2's four K-chunks into pages 0-3, W3 into page 4
+            umma::FenceProxyAsyncShared();
+            for (int kc = 0; kc < 4; ++kc) {
+                load(kc, page(kc), ttab + kTblW2 + kc * kW2ChunkBytes, kW2ChunkBytes);
+            }
+            load(4, page(4), ttab + kTblW3, kPolicy * kHidden1 * 2);
+        };
+        auto store_h0 = [&](int j, const float (&v)[32]) {  // K = 128 half + 32 j .. + 31
+            std::uint32_t r[16];
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+                r[i] = Pack2<kFp16>(v[2 * i], v[2 * i + 1]);
+            }
+            umma::Store16(tmem + static_cast<std::uint32_t>(half * 128 + j * 16) + lane_bits, r);
+        };
         auto trunk = [&](int t, int step) {
-            std::uint8_t *h0 = page(0);  // [128][256], pages 0..3
             if (t == 0) {
-                for (int i = tid; i < kChunkGames * (kHidden0 / 8); i += kEvalThreads) {
-                    const int g = i >> 5;
-                    const int c0 = (i & 31) * 8;
-                    uint4 w;
-                    w.x = Pack2<kFp16>(ts.virgin[c0 + 0], ts.virgin[c0 + 1]);
-                    w.y = Pack2<kFp16>(ts.virgin[c0 + 2], ts.virgin[c0 + 3]);
-                    w.z = Pack2<kFp16>(ts.virgin[c0 + 4], ts.virgin[c0 + 5]);
-                    w.w = Pack2<kFp16>(ts.virgin[c0 + 6], ts.virgin[c0 + 7]);
-                    *reinterpret_cast<uint4 *>(h0 + umma::TileOffset(g, c0, kHidden0)) = w;
-                }
                 if (tid == 0) {
-                    umma::FenceProxyAsyncShared();
-                    load(4, page(4), ttab + kTblW2, kW2ChunkBytes);
-                    load(5, page(5), ttab + kTblW2 + kW2ChunkBytes, kW2ChunkBytes);
+                    load_layer23();
                 }
+                float v[32];
+#pragma unroll 1
+                for (int j = 0; j < 4; ++j) {
+#pragma unroll
+                    for (int i = 0; i < 32; ++i) {
+                        v[i] = ts.virgin[half * 128 + j * 32 + i];
+                    }
+                    store_h0(j, v);
+                }
+                umma::WaitStore();
                 phase_sync();
             } else {
                 // layer 1: stage 0 = {enc page 2, W1 pages 3-4}, stage 1 = {enc page 5, W1 pages 0-1};
@@ -531,9 +548,7 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
                 commit_mma();
                 wait_mma();
                 if (tid == 0) {
-                    umma::FenceProxyAsyncShared();
-                    load(4, page(4), ttab + kTblW2, kW2ChunkBytes);
-                    load(5, page(5), ttab + kTblW2 + kW2ChunkBytes, kW2ChunkBytes);
+                    load_layer23();  // every page is free once layer 1's MMAs are done
                 }
                 float v[32];
 #pragma unroll 1
@@ -545,24 +560,27 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
                         const float h = v[i] + ts.b1[c0 + i];
                         v[i] = h < 0.0f ? 0.0f : h;
                     }
-                    StoreRow32<kFp16>(h0, row, c0, kHidden0, v);
+                    store_h0(j, v);
                 }
+                umma::WaitStore();
                 phase_sync();
             }
-            // layer 2: W2 chunks stream through pages 4 and 5; W3 follows into page 4
+            // layer 2: A (h0) from tensor memory, 16 K-steps per half of the outputs
             if (tid == 0) {
                 for (int kc = 0; kc < 4; ++kc) {
-                    const int b = 4 + (kc & 1);
-                    wait_load(b);
+                    wait_load(kc);
                     umma::FenceAfterSync();
-                    MmaK(tmem, h0 + kc * 1024, kHidden0, page(b), 64, 4, idesc128, kc > 0);
-                    commit_free(kc & 1);
-                    if (kc < 2) {
-                        wait_free(kc & 1);
-                        load(b, page(b), ttab + kTblW2 + (kc + 2) * kW2ChunkBytes, kW2ChunkBytes);
-                    } else if (kc == 2) {
-                        wait_free(0);
-                        load(4, page(4), ttab + kTblW3, kPolicy * kHidden1 * 2);
+                    const std::uint32_t b_addr = umma::SmemAddress(page(kc));
+#pragma unroll
+                    for (int g = 0; g < 2; ++g) {
+#pragma unroll
+                        for (int s4 = 0; s4 < 4; ++s4) {
+                            const int s = 4 * kc + s4;
+                            const std::uint32_t a_col = s < 8 ? 8u * s : 128u + 8u * (s - 8);
+                            const std::uint64_t bd = umma::SmemDescriptor(b_addr + g * 8 * 1024 + s4 * 256, 128,
+                                                                          (64 / 8) * 128);
+                            umma::MmaTs(tmem + 64u + 128u * g, tmem + a_col, bd, idesc64, s > 0);
+                        }
                     }
                 }
             }
@@ -583,7 +601,7 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
 #pragma unroll 1
                 for (int j = 0; j < 2; ++j) {
                     const int c0 = half * 64 + j * 32;
-                    umma::Load32(tmem + static_cast<std::uint32_t>(c0) + lane_bits, v);
+                    umma::Load32(tmem + static_cast<std::uint32_t>(64 + 128 * half + j * 32) + lane_bits, v);
 #pragma unroll
                     for (int i = 0; i < 32; ++i) {
                         const float h = v[i] + ts.b2[c0 + i];

@@ -73,6 +73,16 @@ __device__ __forceinline__ void Mma(std::uint32_t tmem_d, std::uint64_t a_desc, 
         "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate ? 1u : 0u));
 }
 
+// D[tmem] (+)= A[tmem] x B[smem]^T with the A operand in tensor memory: row i of A in lane i, two 16-bit
+// elements per 32-bit column in ascending K order (the lower element in the low half), issued by one thread.
+__device__ __forceinline__ void MmaTs(std::uint32_t tmem_d, std::uint32_t tmem_a, std::uint64_t b_desc,
+                                      std::uint32_t idesc, bool accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+        "r"(tmem_a), "l"(b_desc), "r"(idesc), "r"(accumulate ? 1u : 0u));
+}
+
 // Arrive on the mbarrier once every previously issued MMA of this thread has completed.
 __device__ __forceinline__ void Commit(std::uint64_t *mbar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
@@ -102,6 +112,15 @@ __device__ __forceinline__ bool MbarWait(std::uint64_t *mbar, std::uint32_t pari
     }
     return false;
 }
+
+// Writes 16 consecutive 32-bit columns of this thread's TMEM lane (warp w writes lanes 32w..32w+31); WaitStore
+// makes them visible before a later tensor-core read.
+__device__ __forceinline__ void Store16(std::uint32_t taddr, const std::uint32_t (&r)[16]) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};" ::"r"(taddr), "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15])
+                 : "memory");
+}
+
+__device__ __forceinline__ void WaitStore() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
 // 32 consecutive FP32 accumulator columns of this thread's TMEM lane (warp w reads lanes 32w..32w+31).
 __device__ __forceinline__ void Load32(std::uint32_t taddr, float (&v)[32]) {
