@@ -135,26 +135,27 @@ def barrier(world: int):
         dist.barrier()
 
 
-def max_over_ranks(value: float, world: int) -> float:
+def _all_reduce(value: float, world: int, op_name: str) -> float:
+    """One FP64 all-reduce over the ranks (a device tensor under NCCL, a host tensor under gloo)."""
     if world == 1:
         return value
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    device = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=getattr(dist.ReduceOp, op_name))
     return float(t.item())
+
+
+def max_over_ranks(value: float, world: int) -> float:
+    """The slowest rank's time: every multi-GPU number is timed as the maximum over ranks."""
+    return _all_reduce(value, world, "MAX")
 
 
 def sum_over_ranks(value: float, world: int) -> float:
-    if world == 1:
-        return value
-    import torch
-    import torch.distributed as dist
-
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+    """Work summed over ranks (each rank evolves its own population: weak scaling)."""
+    return _all_reduce(value, world, "SUM")
 
 
 def cpu_reference_rate(catalog, offsets, words, genomes_u16, action_count, sample_individuals, threads):
@@ -657,6 +658,10 @@ def main() -> None:
         run_growth(args)
     else:
         run_ours(args)
+    import torch.distributed as dist
+
+    if dist.is_available() and dist.is_initialized():
+        dist.destroy_process_group()
 
 
 if __name__ == "__main__":
