@@ -188,12 +188,17 @@ __device__ __forceinline__ void MmaK(std::uint32_t d, const std::uint8_t *a, int
     }
 }
 
-// a x b + c with FP16 factors (bit patterns in the low 16 bits) and an FP32 addend, rounded once.
-__device__ __forceinline__ float FmaF16(std::uint32_t a, std::uint32_t b, float c) {
+// a x b + c with 16-bit factors (FP16 or BF16 bit patterns in the low 16 bits) and an FP32 addend, rounded once.
+template <bool kFp16>
+__device__ __forceinline__ float Fma16(std::uint32_t a, std::uint32_t b, float c) {
     float d;
     const unsigned short ha = static_cast<unsigned short>(a);
     const unsigned short hb = static_cast<unsigned short>(b);
-    asm("fma.rn.f32.f16 %0, %1, %2, %3;" : "=f"(d) : "h"(ha), "h"(hb), "f"(c));
+    if constexpr (kFp16) {
+        asm("fma.rn.f32.f16 %0, %1, %2, %3;" : "=f"(d) : "h"(ha), "h"(hb), "f"(c));
+    } else {
+        asm("fma.rn.f32.bf16 %0, %1, %2, %3;" : "=f"(d) : "h"(ha), "h"(hb), "f"(c));
+    }
     return d;
 }
 
@@ -217,17 +222,10 @@ __device__ __forceinline__ float ApproxScore(const std::uint8_t *a_tile, int g, 
         const std::uint32_t ev[4] = {e[kg].x, e[kg].y, e[kg].z, e[kg].w};
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
-            if constexpr (kFp16) {
-                // both factors FP16: the product is formed exactly and added with one rounding, as fmaf does on
-                // the converted values, without the conversions
-                acc[i] = FmaF16(pv[i] & 0xFFFFu, ev[i] & 0xFFFFu, acc[i]);
-                acc[i] = FmaF16(pv[i] >> 16, ev[i] >> 16, acc[i]);
-            } else {
-                const float2 pp = Unpack2<kFp16>(pv[i]);
-                const float2 ee = Unpack2<kFp16>(ev[i]);
-                acc[i] = __fmaf_rn(pp.x, ee.x, acc[i]);
-                acc[i] = __fmaf_rn(pp.y, ee.y, acc[i]);
-            }
+            // both factors 16-bit: the product is formed exactly and added with one rounding, as fmaf does on the
+            // converted values, without the conversions
+            acc[i] = Fma16<kFp16>(pv[i] & 0xFFFFu, ev[i] & 0xFFFFu, acc[i]);
+            acc[i] = Fma16<kFp16>(pv[i] >> 16, ev[i] >> 16, acc[i]);
         }
     }
     return (acc[0] + acc[1]) + (acc[2] + acc[3]);
