@@ -84,21 +84,6 @@ struct EventList {
     std::uint8_t second[kEventCapacity];
 };
 
-__device__ __forceinline__ int NextHit(unsigned long long lo, unsigned long long hi, int r) {
-    if (r < 64) {
-        const unsigned long long x = lo & (~0ull << r);
-        if (x) {
-            return __ffsll(static_cast<long long>(x)) - 1;
-        }
-        return hi ? 64 + __ffsll(static_cast<long long>(hi)) - 1 : 128;
-    }
-    if (r >= 128) {
-        return 128;
-    }
-    const unsigned long long x = hi & (~0ull << (r - 64));
-    return x ? 64 + __ffsll(static_cast<long long>(x)) - 1 : 128;
-}
-
 __device__ __forceinline__ void ApplyNormal(__half *values, std::uint32_t v, const Stream &s, unsigned long long pair,
                                             bool second, float sigma) {
     const float old = __half2float(values[v]);
@@ -174,7 +159,10 @@ __device__ void MutateRun(__half *values, std::uint32_t count, Stream &s, float 
         const unsigned long long lo = static_cast<unsigned long long>(m0) | (static_cast<unsigned long long>(m1) << 32);
         const unsigned long long hi = static_cast<unsigned long long>(m2) | (static_cast<unsigned long long>(m3) << 32);
         while (v < count && r < 128) {
-            const int h = NextHit(lo, hi, r);
+            const unsigned long long xlo = r < 64 ? (lo & (~0ull << (r & 63))) : 0ull;
+            const unsigned long long xhi = r < 64 ? hi : (hi & (~0ull << ((r - 64) & 63)));
+            const int h = xlo != 0ull ? __ffsll(static_cast<long long>(xlo)) - 1
+                                      : (xhi != 0ull ? 63 + __ffsll(static_cast<long long>(xhi)) : 128);
             const std::uint32_t misses = static_cast<std::uint32_t>(h - r);
             if (misses >= count - v) {
                 r += static_cast<int>(count - v);
@@ -188,20 +176,15 @@ __device__ void MutateRun(__half *values, std::uint32_t count, Stream &s, float 
             }
             // value v is hit at draw position window + r
             if (with_normals) {
-                if (lane == 0) {
-                    ev.value[n_events] = v;
-                    ev.pair[n_events] = s.cached ? s.cached_pair : window + r + 1;
-                    ev.second[n_events] = s.cached ? 1 : 0;
-                }
+                const bool cached = s.cached;
+                const unsigned long long fresh_pair = window + static_cast<unsigned>(r) + 1;
+                ev.value[n_events] = v;  // every lane stores the same values
+                ev.pair[n_events] = cached ? s.cached_pair : fresh_pair;
+                ev.second[n_events] = cached ? 1 : 0;
                 ++n_events;
-                if (s.cached) {
-                    s.cached = false;
-                    r += 1;
-                } else {
-                    s.cached = true;
-                    s.cached_pair = window + r + 1;
-                    r += 3;
-                }
+                s.cached_pair = cached ? s.cached_pair : fresh_pair;
+                s.cached = !cached;
+                r += cached ? 1 : 3;
             } else {
                 r += 1;
             }
