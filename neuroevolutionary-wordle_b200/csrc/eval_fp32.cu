@@ -477,14 +477,11 @@ __global__ void __launch_bounds__(kEvalThreads, 2) DescriptorKernel(const Descri
 }  // namespace
 
 cudaError_t LaunchDescriptors(const DescriptorParams &params, int cta_count, cudaStream_t stream) {
-    static bool configured = false;
-    if (!configured) {
-        const cudaError_t e = cudaFuncSetAttribute(DescriptorKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                   kArenaFloats * static_cast<int>(sizeof(float)));
-        if (e != cudaSuccess) {
-            return e;
-        }
-        configured = true;
+    static std::atomic<unsigned long long> configured{0};
+    if (const cudaError_t e =
+            RaiseSharedLimit(DescriptorKernel, kArenaFloats * static_cast<int>(sizeof(float)), configured);
+        e != cudaSuccess) {
+        return e;
     }
     if (cta_count <= 0 || params.count == 0) {
         return cudaSuccess;
@@ -494,15 +491,11 @@ cudaError_t LaunchDescriptors(const DescriptorParams &params, int cta_count, cud
 }
 
 cudaError_t LaunchSingleModelSelect(const SingleModelParams &params, int cta_count, cudaStream_t stream) {
-    static bool configured = false;
-    if (!configured) {
-        const cudaError_t e = cudaFuncSetAttribute(SingleModelSelectKernel,
-                                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                   kArenaFloats * static_cast<int>(sizeof(float)));
-        if (e != cudaSuccess) {
-            return e;
-        }
-        configured = true;
+    static std::atomic<unsigned long long> configured{0};
+    if (const cudaError_t e =
+            RaiseSharedLimit(SingleModelSelectKernel, kArenaFloats * static_cast<int>(sizeof(float)), configured);
+        e != cudaSuccess) {
+        return e;
     }
     if (cta_count <= 0 || params.chunk_count <= 0) {
         return cudaSuccess;
@@ -536,14 +529,11 @@ cudaError_t LaunchEvalPrepare(const WordSource &source, std::uint32_t population
 }
 
 cudaError_t LaunchEvalFp32(const EvalParams &params, int cta_count, cudaStream_t stream) {
-    static bool configured = false;
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(EvalFp32Kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             kArenaFloats * static_cast<int>(sizeof(float)));
-        if (e != cudaSuccess) {
-            return e;
-        }
-        configured = true;
+    static std::atomic<unsigned long long> configured{0};
+    if (const cudaError_t e =
+            RaiseSharedLimit(EvalFp32Kernel, kArenaFloats * static_cast<int>(sizeof(float)), configured);
+        e != cudaSuccess) {
+        return e;
     }
     if (cta_count <= 0) {
         return cudaSuccess;

@@ -542,17 +542,12 @@ cudaError_t LaunchBuildTcTables(const std::uint8_t *slab, std::size_t pitch, con
 
 cudaError_t LaunchEvalTc(const EvalParams &params, const std::uint8_t *tables, std::size_t table_pitch, float kappa,
                          bool fp16, unsigned long long *tc_counters, int cta_count, cudaStream_t stream) {
-    static bool configured[2] = {false, false};
     const int arena_bytes = kArenaFloats * static_cast<int>(sizeof(float));
-    if (!configured[fp16 ? 1 : 0]) {
-        cudaError_t e = fp16 ? cudaFuncSetAttribute(EvalTcKernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                    arena_bytes)
-                             : cudaFuncSetAttribute(EvalTcKernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                    arena_bytes);
-        if (e != cudaSuccess) {
-            return e;
-        }
-        configured[fp16 ? 1 : 0] = true;
+    static std::atomic<unsigned long long> configured[2]{{0}, {0}};
+    if (const cudaError_t e = fp16 ? RaiseSharedLimit(EvalTcKernel<true>, arena_bytes, configured[1])
+                                   : RaiseSharedLimit(EvalTcKernel<false>, arena_bytes, configured[0]);
+        e != cudaSuccess) {
+        return e;
     }
     if (cta_count <= 0) {
         return cudaSuccess;

@@ -1647,16 +1647,11 @@ cudaError_t LaunchBuildTrunkTables(const std::uint8_t *slab, std::size_t pitch, 
 cudaError_t LaunchEvalTct(const EvalParams &params, const std::uint8_t *embed_tables, std::size_t embed_pitch,
                           const std::uint8_t *trunk_tables, float tau, bool fp16, unsigned long long *counters,
                           int cta_count, cudaStream_t stream) {
-    static bool configured[2] = {false, false};
-    if (!configured[fp16 ? 1 : 0]) {
-        cudaError_t e = fp16 ? cudaFuncSetAttribute(EvalTctKernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                    kSmemBytes)
-                             : cudaFuncSetAttribute(EvalTctKernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                    kSmemBytes);
-        if (e != cudaSuccess) {
-            return e;
-        }
-        configured[fp16 ? 1 : 0] = true;
+    static std::atomic<unsigned long long> configured[2]{{0}, {0}};
+    if (const cudaError_t e = fp16 ? RaiseSharedLimit(EvalTctKernel<true>, kSmemBytes, configured[1])
+                                   : RaiseSharedLimit(EvalTctKernel<false>, kSmemBytes, configured[0]);
+        e != cudaSuccess) {
+        return e;
     }
     if (cta_count <= 0) {
         return cudaSuccess;

@@ -179,15 +179,11 @@ cudaError_t LaunchInject(std::uint8_t *slab, std::size_t pitch, const std::uint3
                          const std::uint32_t *guess_codes, const std::uint16_t *tiles, const int4 *chunks,
                          const std::uint32_t *order, int chunk_count, float *scratch, float *sums, int cta_count,
                          int *status, cudaStream_t stream) {
-    static bool configured = false;
     const int arena_bytes = kArenaFloats * static_cast<int>(sizeof(float));
-    if (!configured) {
-        const cudaError_t e = cudaFuncSetAttribute(InjectKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                   arena_bytes);
-        if (e != cudaSuccess) {
-            return e;
-        }
-        configured = true;
+    static std::atomic<unsigned long long> configured{0};
+    if (const cudaError_t e = RaiseSharedLimit(InjectKernel, arena_bytes, configured);
+        e != cudaSuccess) {
+        return e;
     }
     if (child_count == 0 || cta_count <= 0) {
         return cudaSuccess;

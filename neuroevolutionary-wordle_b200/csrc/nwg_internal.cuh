@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstddef>
 #include <cstdint>
 #include <vector>
@@ -271,5 +272,25 @@ int InstallBoundary(nwg_runtime *rt, const std::uint32_t *slots, const float *fi
                     const std::uint32_t *pairs, std::size_t child_count, std::uint32_t seed,
                     const nwg_generation_assembly_config &config, const nwg_pending_injection &injection,
                     std::size_t next_action_count);
+
+// Raises a kernel's dynamic shared memory limit on the current device. The limit belongs to each device's
+// context, so `devices_done` keeps one bit per device ordinal and the attribute is set once per device.
+template <typename Kernel>
+inline cudaError_t RaiseSharedLimit(Kernel kernel, int bytes, std::atomic<unsigned long long> &devices_done) {
+    int device = 0;
+    cudaError_t e = cudaGetDevice(&device);
+    if (e != cudaSuccess) {
+        return e;
+    }
+    const unsigned long long bit = 1ull << (device & 63);
+    if ((devices_done.load(std::memory_order_acquire) & bit) != 0) {
+        return cudaSuccess;
+    }
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) {
+        devices_done.fetch_or(bit, std::memory_order_acq_rel);
+    }
+    return e;
+}
 
 }  // namespace nwg

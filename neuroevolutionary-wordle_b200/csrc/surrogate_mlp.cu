@@ -347,14 +347,10 @@ namespace nwg {
 
 cudaError_t LaunchGemmNt(const void *a, std::size_t lda, const void *b, std::size_t ldb, float *c, std::size_t ldc,
                          std::size_t m, std::size_t n, std::size_t k, int *error, cudaStream_t stream) {
-    static bool configured = false;
-    if (!configured) {
-        const cudaError_t e = cudaFuncSetAttribute(GemmNtKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                   kGemmSmem);
-        if (e != cudaSuccess) {
-            return e;
-        }
-        configured = true;
+    static std::atomic<unsigned long long> configured{0};
+    if (const cudaError_t e = RaiseSharedLimit(GemmNtKernel, kGemmSmem, configured);
+        e != cudaSuccess) {
+        return e;
     }
     if (m % kBM != 0 || n % kBN != 0 || k % kBK != 0 || lda % 8 != 0 || ldb % 8 != 0 || ldc % 4 != 0 ||
         (reinterpret_cast<std::uintptr_t>(a) & 15u) != 0 || (reinterpret_cast<std::uintptr_t>(b) & 15u) != 0 ||
