@@ -103,7 +103,8 @@ struct TctState {
     std::uint64_t bar_load[kPages];  // bulk loads into page p (at most one outstanding per barrier)
     std::uint64_t bar_free[2];       // trunk operand stages released by completed MMAs
     std::uint64_t bar_mma;           // a trunk phase's MMAs have completed
-    std::uint64_t bar_acc[2];        // scoring accumulator buffers
+    std::uint64_t bar_acc[2];        // scoring accumulator buffers: MMAs completed
+    std::uint64_t bar_empty[2];      // scoring accumulator buffers: every warp has read them
     std::uint64_t bar_drain;
     std::uint64_t bar_ring[kRing];   // exact-path weight tiles (FP16 form)
     std::uint32_t tmem_base;
@@ -120,6 +121,7 @@ struct TctState {
     float emax[kPolicy];
     float var[kPolicy];  // per-column variance of the embeddings over the selectable actions
     float s_part[2][kChunkGames];
+    std::uint32_t load_sync[2][kPages];  // thread 0's load counters, handed to every thread for the scoring loop
 };
 
 struct TctParams {
@@ -315,6 +317,7 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
     // every thread: commits to the phase and accumulator barriers
     std::uint32_t mma_commits = 0;
     std::uint32_t acc_commits[2] = {0, 0};
+    std::uint32_t empty_arrivals[2] = {0, 0};  // every thread: warp releases per scoring accumulator buffer
     const std::uint32_t total_chunks = p.chunk_start[p.population];
     const std::uint32_t idesc128 = InstrDesc<kFp16>(128, 128);
     const std::uint32_t idesc64 = InstrDesc<kFp16>(128, 64);
@@ -333,6 +336,8 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
         umma::MbarInit(&ts.bar_mma, 1);
         umma::MbarInit(&ts.bar_acc[0], 1);
         umma::MbarInit(&ts.bar_acc[1], 1);
+        umma::MbarInit(&ts.bar_empty[0], kEvalThreads / 32);
+        umma::MbarInit(&ts.bar_empty[1], kEvalThreads / 32);
         umma::MbarInit(&ts.bar_drain, 1);
         for (int b = 0; b < kRing; ++b) {
             umma::MbarInit(&ts.bar_ring[b], 1);
@@ -679,18 +684,43 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
         };
 
         // ---- scoring: per game, the four largest 32-action chunk maxima of each half of the columns ----
+        // No block barrier inside the tile loop. Tile k's MMAs are issued by lane 0 of warp k % 8 once the tile's
+        // embedding stage has landed and every warp has released accumulator buffer k & 1 (bar_empty); the same
+        // lane refills the stage with tile k + kEmbedStages once tile k's MMAs have completed. Issuing stalls the
+        // issuing thread while the tensor core takes the instructions, so the stall rotates over the warps and the
+        // MMAs, the copies and the epilogues overlap. The load counters advance alike in every thread, which keeps
+        // thread 0's exact for the phases that follow.
         auto score_tiles = [&]() {
+            constexpr int kWarps = kEvalThreads / 32;
             const std::uint8_t *a_tile = page(0);
-            auto issue = [&](int tile) {
+            if (tid == 0) {
+                for (int b = 1; b <= kEmbedStages; ++b) {
+                    ts.load_sync[0][b] = load_issued[b];
+                    ts.load_sync[1][b] = load_waited[b];
+                }
+            }
+            __syncthreads();
+            for (int b = 1; b <= kEmbedStages; ++b) {
+                load_issued[b] = ts.load_sync[0][b];
+                load_waited[b] = ts.load_sync[1][b];
+            }
+            auto issue = [&](int tile) {  // lane 0 of warp tile % kWarps
                 const int acc = tile & 1;
-                MmaK(tmem + static_cast<std::uint32_t>(acc * kTileN), a_tile, kPolicy, page(1 + tile % kEmbedStages),
-                     kPolicy, kPolicy / 16, idesc128, false);
+                const int b = 1 + tile % kEmbedStages;
+                wait_bar(&ts.bar_load[b], load_waited[b] & 1u);
+                if (tile >= 2) {  // tile - 2 was the buffer's last tile; this thread has released it already
+                    wait_bar(&ts.bar_empty[acc], (empty_arrivals[acc] - 1u) & 1u);
+                }
+                umma::FenceAfterSync();
+                MmaK(tmem + static_cast<std::uint32_t>(acc * kTileN), a_tile, kPolicy, page(b), kPolicy, kPolicy / 16,
+                     idesc128, false);
                 umma::Commit(&ts.bar_acc[acc]);
             };
-            if (tid == 0) {
-                wait_load(1);
-                umma::FenceAfterSync();
-                issue(0);
+            if (n_tiles > 0) {
+                if (tid == 0) {
+                    issue(0);
+                }
+                ++load_waited[1];
             }
             float tv[kTopK];
             int ti[kTopK];
@@ -701,18 +731,25 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
             }
             for (int tile = 0; tile < n_tiles; ++tile) {
                 const int buf = tile & 1;
-                if (tid == 0 && tile + 1 < n_tiles) {
-                    wait_load(1 + (tile + 1) % kEmbedStages);
-                    umma::FenceAfterSync();
-                    issue(tile + 1);
+                const int next = tile + 1;
+                if (next < n_tiles) {
+                    if (warp == next % kWarps && lane == 0) {
+                        issue(next);
+                    }
+                    ++load_waited[1 + next % kEmbedStages];
                 }
                 wait_bar(&ts.bar_acc[buf], acc_commits[buf] & 1u);
                 ++acc_commits[buf];
                 umma::FenceAfterSync();
-                if (tid == 0 && tile + kEmbedStages < n_tiles) {
-                    const int b = 1 + tile % kEmbedStages;  // tile's MMA has completed: its stage is free
-                    load(b, page(b), embed + static_cast<std::size_t>(tile + kEmbedStages) * kPageBytes, kPageBytes);
+                if (tile + kEmbedStages < n_tiles) {
+                    const int b = 1 + tile % kEmbedStages;  // tile's MMAs have completed: its stage is free
+                    if (warp == tile % kWarps && lane == 0) {
+                        BulkLoad(page(b), embed + static_cast<std::size_t>(tile + kEmbedStages) * kPageBytes,
+                                 kPageBytes, &ts.bar_load[b]);
+                    }
+                    ++load_issued[b];
                 }
+                __syncwarp();
                 const bool last = tile + 1 == n_tiles;
                 {
                     float v[64];
@@ -731,7 +768,11 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
                     InsertTop4(tv, ti, v[32], tile * 4 + half * 2 + 1);
                 }
                 umma::FenceBeforeSync();
-                __syncthreads();
+                __syncwarp();
+                if (lane == 0) {
+                    umma::MbarArrive(&ts.bar_empty[buf]);
+                }
+                ++empty_arrivals[buf];
             }
             float *cand_v = reinterpret_cast<float *>(smem + kOffCandV);
             int *cand_id = reinterpret_cast<int *>(smem + kOffCandId);
