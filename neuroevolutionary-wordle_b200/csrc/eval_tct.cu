@@ -104,7 +104,6 @@ struct TctState {
     std::uint64_t bar_free[2];       // trunk operand stages released by completed MMAs
     std::uint64_t bar_mma;           // a trunk phase's MMAs have completed
     std::uint64_t bar_acc[2];        // scoring accumulator buffers: MMAs completed
-    std::uint64_t bar_empty[2];      // scoring accumulator buffers: every warp has read them
     std::uint64_t bar_drain;
     std::uint64_t bar_ring[kRing];   // exact-path weight tiles (FP16 form)
     std::uint32_t tmem_base;
@@ -121,7 +120,8 @@ struct TctState {
     float emax[kPolicy];
     float var[kPolicy];  // per-column variance of the embeddings over the selectable actions
     float s_part[2][kChunkGames];
-    std::uint32_t load_sync[2][kPages];  // thread 0's load counters, handed to every thread for the scoring loop
+    std::uint32_t load_sync;             // thread 0's load phase bits, handed to every thread for the scoring loop
+    std::uint32_t readers[2];            // warps that have read each scoring accumulator buffer (8 per tile)
 };
 
 struct TctParams {
@@ -308,16 +308,17 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
         reinterpret_cast<std::uint8_t *>(p.scratch + static_cast<std::size_t>(blockIdx.x) * kScratchFloats);
     unsigned long long decisions = 0, encoded = 0, episodes = 0;
     unsigned long long cand_chunks = 0, fallback_steps = 0, exact_chunks = 0, exact_rows = 0;
-    // thread 0 only: bulk loads issued / waited per barrier, commits per stage barrier
-    std::uint32_t load_issued[kPages] = {0, 0, 0, 0, 0, 0};
-    std::uint32_t ring_issued[kRing] = {0, 0, 0};  // thread 0: exact-path weight tiles issued per ring buffer
-    std::uint32_t ring_waited[kRing] = {0, 0, 0};  // every thread: waits per ring buffer
-    std::uint32_t load_waited[kPages] = {0, 0, 0, 0, 0, 0};
-    std::uint32_t free_commits[2] = {0, 0};
-    // every thread: commits to the phase and accumulator barriers
+    // Barrier bookkeeping as one bit per barrier in registers (each barrier has at most one copy or commit
+    // outstanding): the parity of the next wait, and for the copies whether one is in flight.
+    // thread 0 only: page loads, their flight bits, exact-path ring tiles in flight, stage commits mod 2
+    std::uint32_t load_phase = 0;
+    std::uint32_t load_pending = 0;
+    std::uint32_t ring_pending = 0;
+    std::uint32_t free_parity = 0;
+    // every thread: ring waits, phase commits, accumulator waits
+    std::uint32_t ring_phase = 0;
     std::uint32_t mma_commits = 0;
-    std::uint32_t acc_commits[2] = {0, 0};
-    std::uint32_t empty_arrivals[2] = {0, 0};  // every thread: warp releases per scoring accumulator buffer
+    std::uint32_t acc_phase = 0;
     const std::uint32_t total_chunks = p.chunk_start[p.population];
     const std::uint32_t idesc128 = InstrDesc<kFp16>(128, 128);
     const std::uint32_t idesc64 = InstrDesc<kFp16>(128, 64);
@@ -336,8 +337,8 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
         umma::MbarInit(&ts.bar_mma, 1);
         umma::MbarInit(&ts.bar_acc[0], 1);
         umma::MbarInit(&ts.bar_acc[1], 1);
-        umma::MbarInit(&ts.bar_empty[0], kEvalThreads / 32);
-        umma::MbarInit(&ts.bar_empty[1], kEvalThreads / 32);
+        ts.readers[0] = 0;
+        ts.readers[1] = 0;
         umma::MbarInit(&ts.bar_drain, 1);
         for (int b = 0; b < kRing; ++b) {
             umma::MbarInit(&ts.bar_ring[b], 1);
@@ -360,17 +361,18 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
     // thread 0 only
     auto load = [&](int b, void *dst, const void *src, std::uint32_t bytes) {
         BulkLoad(dst, src, bytes, &ts.bar_load[b]);
-        ++load_issued[b];
+        load_pending |= 1u << b;
     };
     auto wait_load = [&](int b) {
-        wait_bar(&ts.bar_load[b], load_waited[b] & 1u);
-        ++load_waited[b];
+        wait_bar(&ts.bar_load[b], (load_phase >> b) & 1u);
+        load_phase ^= 1u << b;
+        load_pending &= ~(1u << b);
     };
     auto commit_free = [&](int s) {
         umma::Commit(&ts.bar_free[s]);
-        ++free_commits[s];
+        free_parity ^= 1u << s;
     };
-    auto wait_free = [&](int s) { wait_bar(&ts.bar_free[s], (free_commits[s] - 1u) & 1u); };
+    auto wait_free = [&](int s) { wait_bar(&ts.bar_free[s], ((free_parity >> s) & 1u) ^ 1u); };
     // every thread (uniform control flow)
     auto commit_mma = [&]() {
         if (tid == 0) {
@@ -684,43 +686,34 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
         };
 
         // ---- scoring: per game, the four largest 32-action chunk maxima of each half of the columns ----
-        // No block barrier inside the tile loop. Tile k's MMAs are issued by lane 0 of warp k % 8 once the tile's
-        // embedding stage has landed and every warp has released accumulator buffer k & 1 (bar_empty); the same
-        // lane refills the stage with tile k + kEmbedStages once tile k's MMAs have completed. Issuing stalls the
-        // issuing thread while the tensor core takes the instructions, so the stall rotates over the warps and the
-        // MMAs, the copies and the epilogues overlap. The load counters advance alike in every thread, which keeps
-        // thread 0's exact for the phases that follow.
+        // No block barrier inside the tile loop. Thread 0 issues tiles 0 and 1; after that, the last warp to finish
+        // reading tile k's accumulator buffer (an arrival counter per buffer) refills tile k's embedding stage with
+        // tile k + kEmbedStages and issues tile k + 2 into the buffer it has just released. Issuing stalls the
+        // issuing thread while the tensor core takes the instructions, and the last reader of a buffer would wait
+        // for the buffer's next tile in any case, so the stall stays off the critical path while the other warps
+        // read the other buffer. The load counters advance alike in every thread, which keeps thread 0's exact for
+        // the phases that follow.
         auto score_tiles = [&]() {
-            constexpr int kWarps = kEvalThreads / 32;
             const std::uint8_t *a_tile = page(0);
             if (tid == 0) {
-                for (int b = 1; b <= kEmbedStages; ++b) {
-                    ts.load_sync[0][b] = load_issued[b];
-                    ts.load_sync[1][b] = load_waited[b];
-                }
+                ts.load_sync = load_phase;
             }
             __syncthreads();
-            for (int b = 1; b <= kEmbedStages; ++b) {
-                load_issued[b] = ts.load_sync[0][b];
-                load_waited[b] = ts.load_sync[1][b];
-            }
-            auto issue = [&](int tile) {  // lane 0 of warp tile % kWarps
+            load_phase = ts.load_sync;
+            auto issue = [&](int tile) {  // one thread
                 const int acc = tile & 1;
                 const int b = 1 + tile % kEmbedStages;
-                wait_bar(&ts.bar_load[b], load_waited[b] & 1u);
-                if (tile >= 2) {  // tile - 2 was the buffer's last tile; this thread has released it already
-                    wait_bar(&ts.bar_empty[acc], (empty_arrivals[acc] - 1u) & 1u);
-                }
+                wait_bar(&ts.bar_load[b], (load_phase >> b) & 1u);
                 umma::FenceAfterSync();
                 MmaK(tmem + static_cast<std::uint32_t>(acc * kTileN), a_tile, kPolicy, page(b), kPolicy, kPolicy / 16,
                      idesc128, false);
                 umma::Commit(&ts.bar_acc[acc]);
             };
-            if (n_tiles > 0) {
+            for (int k = 0; k < 2 && k < n_tiles; ++k) {
                 if (tid == 0) {
-                    issue(0);
+                    issue(k);
                 }
-                ++load_waited[1];
+                load_phase ^= 1u << (1 + k % kEmbedStages);
             }
             float tv[kTopK];
             int ti[kTopK];
@@ -731,24 +724,9 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
             }
             for (int tile = 0; tile < n_tiles; ++tile) {
                 const int buf = tile & 1;
-                const int next = tile + 1;
-                if (next < n_tiles) {
-                    if (warp == next % kWarps && lane == 0) {
-                        issue(next);
-                    }
-                    ++load_waited[1 + next % kEmbedStages];
-                }
-                wait_bar(&ts.bar_acc[buf], acc_commits[buf] & 1u);
-                ++acc_commits[buf];
+                wait_bar(&ts.bar_acc[buf], (acc_phase >> buf) & 1u);
+                acc_phase ^= 1u << buf;
                 umma::FenceAfterSync();
-                if (tile + kEmbedStages < n_tiles) {
-                    const int b = 1 + tile % kEmbedStages;  // tile's MMAs have completed: its stage is free
-                    if (warp == tile % kWarps && lane == 0) {
-                        BulkLoad(page(b), embed + static_cast<std::size_t>(tile + kEmbedStages) * kPageBytes,
-                                 kPageBytes, &ts.bar_load[b]);
-                    }
-                    ++load_issued[b];
-                }
                 __syncwarp();
                 const bool last = tile + 1 == n_tiles;
                 {
@@ -770,10 +748,25 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
                 umma::FenceBeforeSync();
                 __syncwarp();
                 if (lane == 0) {
-                    umma::MbarArrive(&ts.bar_empty[buf]);
+                    __threadfence_block();
+                    if ((atomicAdd(&ts.readers[buf], 1u) & 7u) == 7u) {  // every warp has read tile's buffer
+                        __threadfence_block();
+                        if (tile + kEmbedStages < n_tiles) {
+                            const int b = 1 + tile % kEmbedStages;  // tile's MMAs have completed: its stage is free
+                            BulkLoad(page(b), embed + static_cast<std::size_t>(tile + kEmbedStages) * kPageBytes,
+                                     kPageBytes, &ts.bar_load[b]);
+                        }
+                        if (tile + 2 < n_tiles) {
+                            issue(tile + 2);
+                        }
+                    }
                 }
-                ++empty_arrivals[buf];
+                if (tile + 2 < n_tiles) {
+                    load_phase ^= 1u << (1 + (tile + 2) % kEmbedStages);
+                }
             }
+            // every embedding tile has been waited for
+            load_pending &= ~(((1u << kEmbedStages) - 1u) << 1);
             float *cand_v = reinterpret_cast<float *>(smem + kOffCandV);
             int *cand_id = reinterpret_cast<int *>(smem + kOffCandId);
 #pragma unroll
@@ -1044,7 +1037,7 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
                         off = kTblW3;
                     }
                     BulkLoad(buffer(i), ttab + off, bytes, &ts.bar_ring[i % kRing]);
-                    ++ring_issued[i % kRing];
+                    ring_pending |= 1u << (i % kRing);
                 };
                 if (tid == 0) {
                     umma::FenceProxyAsyncShared();
@@ -1117,8 +1110,9 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
                 }
                 for (int i = 0; i < n_tiles; ++i) {
                     const int b = i % kRing;
-                    wait_bar(&ts.bar_ring[b], ring_waited[b] & 1u);
-                    ++ring_waited[b];
+                    wait_bar(&ts.bar_ring[b], (ring_phase >> b) & 1u);
+                    ring_phase ^= 1u << b;
+                    ring_pending &= ~(1u << b);
                     const std::uint8_t *w = buffer(i);
                     if (i < enc_tiles && i < 3) {
                         // encoder hidden rows of this group: EncodeRound's gather chain, ascending feature order
@@ -1610,15 +1604,13 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
         umma::Commit(&ts.bar_drain);
         (void)umma::MbarWait(&ts.bar_drain, 0, 1u << 22);
         for (int b = 0; b < kPages; ++b) {
-            while (load_waited[b] < load_issued[b]) {
-                (void)umma::MbarWait(&ts.bar_load[b], load_waited[b] & 1u, 1u << 22);
-                ++load_waited[b];
+            if ((load_pending >> b) & 1u) {
+                (void)umma::MbarWait(&ts.bar_load[b], (load_phase >> b) & 1u, 1u << 22);
             }
         }
         for (int b = 0; b < kRing; ++b) {
-            while (ring_waited[b] < ring_issued[b]) {
-                (void)umma::MbarWait(&ts.bar_ring[b], ring_waited[b] & 1u, 1u << 22);
-                ++ring_waited[b];
+            if ((ring_pending >> b) & 1u) {
+                (void)umma::MbarWait(&ts.bar_ring[b], (ring_phase >> b) & 1u, 1u << 22);
             }
         }
     }

@@ -90,11 +90,6 @@ __device__ __forceinline__ void Commit(std::uint64_t *mbar) {
                  : "memory");
 }
 
-// One arrival on the mbarrier (release at CTA scope).
-__device__ __forceinline__ void MbarArrive(std::uint64_t *mbar) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(SmemAddress(mbar)) : "memory");
-}
-
 __device__ __forceinline__ void MbarInit(std::uint64_t *mbar, std::uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(SmemAddress(mbar)), "r"(count) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
