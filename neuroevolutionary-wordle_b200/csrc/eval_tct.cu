@@ -204,18 +204,20 @@ __device__ __forceinline__ float Fma16(std::uint32_t a, std::uint32_t b, float c
     return d;
 }
 
-// Approximate score (16-bit operands, FP32 accumulation) of action a for game g: the policy row of the
-// operand tile against the action's row of the embedding table.
-template <bool kFp16>
-__device__ __forceinline__ float ApproxScore(const std::uint8_t *a_tile, int g, const std::uint8_t *embed,
-                                             std::uint32_t a) {
+// Action a's row of the embedding table (64 16-bit values in eight 16-byte pieces of the operand tile layout).
+__device__ __forceinline__ void LoadEmbedRow(const std::uint8_t *embed, std::uint32_t a, uint4 (&e)[8]) {
     const std::uint8_t *erow = embed + static_cast<std::size_t>(a >> 7) * (kTileN * kPolicy * 2) +
                                umma::TileOffset(a & 127u, 0, kPolicy);
-    uint4 e[8];
 #pragma unroll
     for (int kg = 0; kg < 8; ++kg) {
         e[kg] = __ldg(reinterpret_cast<const uint4 *>(erow + kg * 128));
     }
+}
+
+// Approximate score (16-bit operands, FP32 accumulation) of an action for game g: the policy row of the
+// operand tile against the action's embedding row e.
+template <bool kFp16>
+__device__ __forceinline__ float ApproxScore(const std::uint8_t *a_tile, int g, const uint4 (&e)[8]) {
     float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
 #pragma unroll
     for (int kg = 0; kg < 8; ++kg) {
@@ -898,12 +900,13 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
             __syncthreads();
             // re-score each candidate chunk from the 16-bit operands: a warp per chunk (two chunks in flight),
             // top-2 keys by (score, lower action index) from 32-bit warp reductions
-            auto task_bits = [&](std::uint32_t task) {
+            auto task_action = [&](std::uint32_t task) {
+                return (task & 0xFFFFu) * 32u + static_cast<std::uint32_t>(lane);
+            };
+            auto task_bits = [&](std::uint32_t task, const uint4 (&e)[8], std::uint32_t code) {
                 const int g = static_cast<int>(task >> 16);
-                const std::uint32_t a = (task & 0xFFFFu) * 32u + static_cast<std::uint32_t>(lane);
-                const bool valid = a < p.action_count;
-                const std::uint32_t code = valid ? __ldg(p.codes + a) : 0u;
-                const float s = ApproxScore<kFp16>(page(0), g, embed, valid ? a : 0u);
+                const bool valid = task_action(task) < p.action_count;
+                const float s = ApproxScore<kFp16>(page(0), g, e);
                 bool masked = !valid;
                 for (int u = 0; u < t; ++u) {
                     masked |= cs.guess[u][g] == code;
@@ -933,8 +936,19 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
                 const int k1 = k0 + kWarps;
                 const std::uint32_t task0 = tasks[k0];
                 const std::uint32_t task1 = k1 < total ? tasks[k1] : task0;
-                const std::uint32_t ob0 = task_bits(task0);
-                const std::uint32_t ob1 = task_bits(task1);
+                // both chunks' embedding rows and codes are in flight before either dot product
+                const std::uint32_t a0 = task_action(task0);
+                const std::uint32_t a1 = task_action(task1);
+                const bool v0 = a0 < p.action_count;
+                const bool v1 = a1 < p.action_count;
+                uint4 e0[8];
+                uint4 e1[8];
+                LoadEmbedRow(embed, v0 ? a0 : 0u, e0);
+                LoadEmbedRow(embed, v1 ? a1 : 0u, e1);
+                const std::uint32_t code0 = v0 ? __ldg(p.codes + a0) : 0u;
+                const std::uint32_t code1 = v1 ? __ldg(p.codes + a1) : 0u;
+                const std::uint32_t ob0 = task_bits(task0, e0, code0);
+                const std::uint32_t ob1 = task_bits(task1, e1, code1);
                 store_top2(k0, task0, ob0);
                 if (k1 < total) {
                     store_top2(k1, task1, ob1);
