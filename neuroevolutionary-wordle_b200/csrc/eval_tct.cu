@@ -750,9 +750,13 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
                 umma::FenceBeforeSync();
                 __syncwarp();
                 if (lane == 0) {
-                    __threadfence_block();
-                    if ((atomicAdd(&ts.readers[buf], 1u) & 7u) == 7u) {  // every warp has read tile's buffer
-                        __threadfence_block();
+                    // one acquire-release add: releases this warp's reads, and the last reader acquires the others'
+                    std::uint32_t prior = 0;
+                    asm volatile("atom.acq_rel.cta.shared::cta.add.u32 %0, [%1], %2;"
+                                 : "=r"(prior)
+                                 : "r"(umma::SmemAddress(&ts.readers[buf])), "r"(1u)
+                                 : "memory");
+                    if ((prior & 7u) == 7u) {  // every warp has read tile's buffer
                         if (tile + kEmbedStages < n_tiles) {
                             const int b = 1 + tile % kEmbedStages;  // tile's MMAs have completed: its stage is free
                             BulkLoad(page(b), embed + static_cast<std::size_t>(tile + kEmbedStages) * kPageBytes,
