@@ -1560,10 +1560,14 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
                 const int chunks_per_row = static_cast<int>((p.action_count + 31) / 32);
                 for (int f = 0; f < nb; ++f) {
                     if (fb_full[f]) {
+                        // each lane keeps its best key over the warp's chunks; one fold per warp and row
+                        unsigned long long key = 0;
                         for (int c = warp; c < chunks_per_row; c += kEvalThreads / 32) {
-                            RescoreChunk(p, cs, fb_key + f, xp + f * kPolicy, 1, tail, ts.fallback_games[b0 + f], c,
-                                         t);
+                            const unsigned long long k =
+                                ChunkKey(p, cs, xp + f * kPolicy, 1, tail, ts.fallback_games[b0 + f], c, t);
+                            key = k > key ? k : key;
                         }
+                        FoldKeys(fb_key + f, key);
                     }
                 }
                 __syncthreads();

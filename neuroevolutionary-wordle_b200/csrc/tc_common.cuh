@@ -85,31 +85,41 @@ __device__ __forceinline__ float ExactScore(const EvalParams &p, const float *pv
     return s;
 }
 
+// Exact key of this lane's action in 32-action chunk `chunk` for game g, whose policy vector is pv[k * ld]: the
+// packed (score, action) key, or 0 for a guessed word (word equality) or an action past the end. The score is
+// formed before the mask is known, so the action's code and its embedding values are loaded together.
+__device__ __forceinline__ unsigned long long ChunkKey(const EvalParams &p, const ChunkState &cs, const float *pv,
+                                                       int ld, const __half *tail, int g, int chunk, int turns) {
+    const std::uint32_t a = static_cast<std::uint32_t>(chunk) * 32u + (threadIdx.x & 31);
+    if (a >= p.action_count) {
+        return 0;
+    }
+    const std::uint32_t code = p.codes[a];
+    const float s = ExactScore(p, pv, ld, tail, a);
+    bool masked = false;
+    for (int u = 0; u < turns; ++u) {
+        masked |= cs.guess[u][g] == code;
+    }
+    return masked ? 0ull : PackKey(s, a);
+}
+
+// Folds a warp's keys (the masked argmax) into *best_key.
+__device__ __forceinline__ void FoldKeys(unsigned long long *best_key, unsigned long long key) {
+    for (int off = 16; off > 0; off >>= 1) {
+        const unsigned long long other = __shfl_xor_sync(0xffffffffu, key, off);
+        key = other > key ? other : key;
+    }
+    if ((threadIdx.x & 31) == 0 && key != 0) {
+        atomicMax(best_key, key);
+    }
+}
+
 // Warp-cooperative exact re-scoring of 32-action chunk `chunk` for game g, whose policy vector is
 // pv[k * ld]; folds the masked argmax (guessed words excluded by word equality) into *best_key.
 __device__ __forceinline__ void RescoreChunk(const EvalParams &p, const ChunkState &cs, unsigned long long *best_key,
                                              const float *pv, int ld, const __half *tail, int g, int chunk,
                                              int turns) {
-    const int lane = threadIdx.x & 31;
-    const std::uint32_t a = static_cast<std::uint32_t>(chunk) * 32u + lane;
-    unsigned long long key = 0;
-    if (a < p.action_count) {
-        const std::uint32_t code = p.codes[a];
-        bool masked = false;
-        for (int u = 0; u < turns; ++u) {
-            masked |= cs.guess[u][g] == code;
-        }
-        if (!masked) {
-            key = PackKey(ExactScore(p, pv, ld, tail, a), a);
-        }
-    }
-    for (int off = 16; off > 0; off >>= 1) {
-        const unsigned long long other = __shfl_xor_sync(0xffffffffu, key, off);
-        key = other > key ? other : key;
-    }
-    if (lane == 0 && key != 0) {
-        atomicMax(best_key, key);
-    }
+    FoldKeys(best_key, ChunkKey(p, cs, pv, ld, tail, g, chunk, turns));
 }
 
 }  // namespace tcx
