@@ -78,10 +78,11 @@ __device__ std::uint32_t DrawIndex(Stream &s, std::uint32_t n) {
     return curand(&state) % n;
 }
 
+// A queued hit in one word: the value index in the low 32 bits; in the high 32 bits the draw position of its
+// normal pair, with bit 31 set when the hit takes the pair's second value. A child's draw positions stay below
+// 2^31 (LaunchBreed checks the genome size), so a position fits in 31 bits.
 struct EventList {
-    std::uint32_t value[kEventCapacity];
-    unsigned long long pair[kEventCapacity];
-    std::uint8_t second[kEventCapacity];
+    unsigned long long packed[kEventCapacity];
 };
 
 __device__ __forceinline__ void ApplyNormal(__half *values, std::uint32_t v, const Stream &s, unsigned long long pair,
@@ -100,7 +101,9 @@ __device__ __forceinline__ void FlushEvents(__half *values, const Stream &s, flo
                                             int lane) {
     __syncwarp();
     for (int e = lane; e < n_events; e += 32) {
-        ApplyNormal(values, ev.value[e], s, ev.pair[e], ev.second[e] != 0, sigma);
+        const unsigned long long w = ev.packed[e];
+        const std::uint32_t hi = static_cast<std::uint32_t>(w >> 32);
+        ApplyNormal(values, static_cast<std::uint32_t>(w), s, hi & 0x7FFFFFFFu, (hi >> 31) != 0u, sigma);
     }
     __syncwarp();
     n_events = 0;
@@ -141,6 +144,9 @@ __device__ void MutateRun(__half *values, std::uint32_t count, Stream &s, float 
     }
     std::uint32_t v = 0;
     int n_events = 0;
+    // the cached pair's position with bit 31 set: the high word of the next cached hit's event
+    std::uint32_t cached_word = static_cast<std::uint32_t>(s.cached_pair) | 0x80000000u;
+    bool cached = s.cached;
     while (v < count) {
         const unsigned long long window = s.position & ~3ull;
         int r = static_cast<int>(s.position - window);
@@ -176,15 +182,13 @@ __device__ void MutateRun(__half *values, std::uint32_t count, Stream &s, float 
             }
             // value v is hit at draw position window + r
             if (with_normals) {
-                const bool cached = s.cached;
-                const unsigned long long fresh_pair = window + static_cast<unsigned>(r) + 1;
-                ev.value[n_events] = v;  // every lane stores the same values
-                ev.pair[n_events] = cached ? s.cached_pair : fresh_pair;
-                ev.second[n_events] = cached ? 1 : 0;
+                const std::uint32_t fresh = static_cast<std::uint32_t>(window) + static_cast<std::uint32_t>(r) + 1u;
+                // every lane stores the same word
+                ev.packed[n_events] = (static_cast<unsigned long long>(cached ? cached_word : fresh) << 32) | v;
                 ++n_events;
-                s.cached_pair = cached ? s.cached_pair : fresh_pair;
-                s.cached = !cached;
-                r += cached ? 1 : 3;
+                cached_word = cached ? cached_word : (fresh | 0x80000000u);
+                cached = !cached;
+                r += cached ? 3 : 1;  // (toggled) a fresh pair takes two more positions
             } else {
                 r += 1;
             }
@@ -198,6 +202,8 @@ __device__ void MutateRun(__half *values, std::uint32_t count, Stream &s, float 
     if (n_events > 0) {
         FlushEvents(values, s, sigma, ev, n_events, lane);
     }
+    s.cached = cached;
+    s.cached_pair = cached_word & 0x7FFFFFFFu;
 }
 
 __device__ void CopyRegion(std::uint8_t *__restrict__ dst, const std::uint8_t *__restrict__ src, std::size_t bytes,
@@ -350,6 +356,12 @@ __global__ void __launch_bounds__(kWarps * 32) BreedKernel(const BreedParams p) 
 cudaError_t LaunchBreed(const BreedParams &params, cudaStream_t stream, int warps_per_cta) {
     if (params.child_count == 0) {
         return cudaSuccess;
+    }
+    // a child's draw positions: at most three per genome value plus the crossover draws, below 2^31
+    const unsigned long long values =
+        static_cast<unsigned long long>(kPolicyHalfs) + static_cast<unsigned long long>(kTailDim) * params.action_count;
+    if (3ull * values + 64ull >= (1ull << 31)) {
+        return cudaErrorInvalidValue;
     }
     switch (warps_per_cta) {
         case 4:
