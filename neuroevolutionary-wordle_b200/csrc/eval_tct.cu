@@ -353,7 +353,8 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
     const std::uint32_t tmem = ts.tmem_base;
 
     auto wait_bar = [&](std::uint64_t *bar, std::uint32_t parity) {
-        if (*reinterpret_cast<volatile int *>(&ts.failed) != 0) {
+        // a completed phase is taken at once; the failure flag is read only for a phase still open
+        if (umma::MbarTest(bar, parity) || *reinterpret_cast<volatile int *>(&ts.failed) != 0) {
             return;
         }
         if (!umma::MbarWait(bar, parity, kWaitLimit)) {

@@ -95,23 +95,26 @@ __device__ __forceinline__ void MbarInit(std::uint64_t *mbar, std::uint32_t coun
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 
+// Whether the mbarrier phase with the given parity has completed (non-blocking).
+__device__ __forceinline__ bool MbarTest(std::uint64_t *mbar, std::uint32_t parity) {
+    std::uint32_t done = 0;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(SmemAddress(mbar)), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+
 // Waits for the mbarrier phase with the given parity; gives up after `limit` polls and returns false.
 // A phase that has completed already is seen by the non-blocking test_wait; the potentially blocking try_wait
 // took hundreds of cycles to report such a phase on B200, so it is used only while the phase is still open.
 __device__ __forceinline__ bool MbarWait(std::uint64_t *mbar, std::uint32_t parity, std::uint32_t limit) {
-    const std::uint32_t addr = SmemAddress(mbar);
-    {
-        std::uint32_t done = 0;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\tmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}\n"
-            : "=r"(done)
-            : "r"(addr), "r"(parity)
-            : "memory");
-        if (done) {
-            return true;
-        }
+    if (MbarTest(mbar, parity)) {
+        return true;
     }
+    const std::uint32_t addr = SmemAddress(mbar);
     for (std::uint32_t i = 0; i < limit; ++i) {
         std::uint32_t done = 0;
         asm volatile(
