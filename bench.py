@@ -5,15 +5,22 @@ secrets per cell drawn from a 2,315-word secret subset (3 episodes per secret), 
 reference crossover temperatures, mutation p = 0.05, sigma = 0.02. Genomes are the reference's FP16
 layout (bootstrap He-normal weights, N(0, 0.05) tails).
 
-The headline form (default --form tc-trunk-fp16) runs encoder, trunk and scoring on tcgen05 with FP16
-operands and a top-2 margin guard (--tau, default 1e-3 x the score scale) that sends uncertain game steps
-through the exact FP32 path. The plain FP32 form is timed on the same workload in the same process and
-reported beside it ("plain_fp32"), with the guess agreement and fitness delta of the headline form against it over the
-whole population ("agreement_with_plain"). --form fp32 benchmarks the plain form alone.
+The headline form (default --form tc-fp16) gives the reference's results bit for bit: encoder, trunk and policy
+are the reference's FP32 chains, 16-bit tensor-core scores only screen the actions, and every guess is the exact
+FP32 argmax (the chunks a certified error bound cannot rule out are re-scored in FP32). Its line carries the
+device-resident value, the same metric end to end through the public API with host buffers ("e2e"), the
+evaluation kernel's roofline, and the reference's CPU path timed on the generation just measured
+("cpu_baseline"). "other_forms" times the plain FP32 form (no tensor cores at all) and the 16-bit tensor-core
+trunk forms (FP16 and BF16 operands, top-2 margin guard with exact FP32 fallback: narrower than the reference,
+reported with their guess agreement against the plain form, "agreement_with_plain"). "reference_gpu" times the
+reference's own CUDA evaluation (compiled for sm_100a from its sources) on a 256-individual slice of the workload
+on the same GPU, beside this library's forms on the same slice.
 
-On the full workload at N=1 the line also carries "surrogate_vs_plain": the plain FP32 form evolves 50
-generations and its held-out mean solve rate becomes the target; the learned-surrogate method then evolves
-from the same start until it reaches that rate, and the two wall times are reported (--no-surrogate skips it).
+On the full workload at N=1 the line also carries "surrogate_vs_plain" (--no-surrogate skips it).
+
+--gpus N (N > 1) starts N ranks on this node (or runs under torch.distributed.run) and splits the one population
+into N row bands, one per GPU: evaluation per band, fitness all-gather, halo genome exchange with the neighbour
+bands, breeding per band (strong scaling: the total work is the same as at N = 1).
 
 Prints one JSON line (rank 0). `--impl reference` times the reference's own CPU path (its host-callable
 model, scoring and Wordle code composed into its episode loop, built in oracle/_ref) on a bounded sample
@@ -38,8 +45,9 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 MEASURED = ROOT / "MEASURED_PEAKS.json"
-TRAFFIC = ROOT / "profiles" / "eval_fp32_traffic.json"
-TRAFFIC_TCT = ROOT / "profiles" / "eval_tct_traffic.json"
+TRAFFIC_FILES = {"fp32": ROOT / "profiles" / "eval_fp32_traffic.json",
+                 "tc-fp16": ROOT / "profiles" / "eval_tc_traffic.json",
+                 "tc-trunk-fp16": ROOT / "profiles" / "eval_tct_traffic.json"}
 KERNELS_PER_GENERATION = 7  # prepare, evaluate, finalize, summarize, select, plan slots, breed
 FORMS = {"fp32": 0, "tc-bf16": 1, "tc-fp16": 2, "tc-trunk-bf16": 3, "tc-trunk-fp16": 4}
 FORM_NAMES = {"fp32": "plain fp32", "tc-bf16": "tensor-core bf16 scoring, exact fp32 re-scoring",
@@ -47,9 +55,21 @@ FORM_NAMES = {"fp32": "plain fp32", "tc-bf16": "tensor-core bf16 scoring, exact 
               "tc-trunk-bf16": "tensor-core bf16 encoder+trunk+scoring, margin guard tau with exact fp32 fallback",
               "tc-trunk-fp16": "tensor-core fp16 encoder+trunk+scoring, margin guard tau with exact fp32 fallback"}
 EXTRA_KERNELS = {"fp32": 0, "tc-bf16": 1, "tc-fp16": 1, "tc-trunk-bf16": 2, "tc-trunk-fp16": 2}
+# What each form's results are, against the reference's FP32 arithmetic.
+PRECISION = {
+    "fp32": "reference: every policy value, score and guess is the reference's FP32 chain, bit for bit",
+    "tc-bf16": "reference: FP32 policy chains bit for bit; 16-bit tensor-core scores only screen actions and every "
+               "guess is the exact FP32 argmax (certified error bound), so guesses, turns, scores and fitness are "
+               "the reference's bit for bit",
+    "tc-fp16": "reference: FP32 policy chains bit for bit; 16-bit tensor-core scores only screen actions and every "
+               "guess is the exact FP32 argmax (certified error bound), so guesses, turns, scores and fitness are "
+               "the reference's bit for bit",
+    "tc-trunk-bf16": "narrower: 16-bit tensor-core policy; steps under the margin guard re-run in exact FP32",
+    "tc-trunk-fp16": "narrower: 16-bit tensor-core policy; steps under the margin guard re-run in exact FP32",
+}
 DTYPES = {"fp32": "fp32 (fp16-stored genomes)",
-          "tc-bf16": "bf16 tensor-core scores, fp32 trunk and exact fp32 re-scoring",
-          "tc-fp16": "fp16 tensor-core scores, fp32 trunk and exact fp32 re-scoring",
+          "tc-bf16": "fp32 (exact): fp32 trunk and decisions, bf16 tensor-core scores screen the actions",
+          "tc-fp16": "fp32 (exact): fp32 trunk and decisions, fp16 tensor-core scores screen the actions",
           "tc-trunk-bf16": "bf16 tensor-core operands, fp32 accumulation; exact fp32 path for guarded steps",
           "tc-trunk-fp16": "fp16 tensor-core operands, fp32 accumulation; exact fp32 path for guarded steps"}
 
@@ -339,122 +359,336 @@ def surrogate_vs_plain(nwg, wl, torch, generations: int, min_generations: int = 
     }
 
 
+def kernel_launches(form: str) -> int:
+    return KERNELS_PER_GENERATION + EXTRA_KERNELS[form]
+
+
+def roofline(form: str, steps: float, encoded: float, action_count: int, kernel_ms: float, pk: dict,
+             fp32_peak: float, traffic) -> dict:
+    """The evaluation kernel against its bound. The per-step work is SURVEY 8(d)'s 2 * (E_new + 123,136 + 64 A)
+    FLOP: the encoder and trunk share (2 * (9,472 per encoded turn + 123,136 per step)) runs as FP32 FFMA chains in
+    the plain and exact forms, the scoring share (2 * 64 A per step) on CUDA cores (plain) or on tensor cores (the
+    other forms). The bound is the pipe whose share takes longest at its measured peak."""
+    flops = algorithmic_flops(int(steps), int(encoded), action_count)
+    trunk = 2.0 * (9472.0 * encoded + 123136.0 * steps)
+    scoring = flops - trunk
+    t = kernel_ms * 1e-3
+    kernel = {"fp32": "EvalFp32Kernel", "tc-bf16": "EvalTcKernel<bf16>", "tc-fp16": "EvalTcKernel<fp16>",
+              "tc-trunk-bf16": "EvalTctKernel<bf16>", "tc-trunk-fp16": "EvalTctKernel<fp16>"}[form]
+    common = {"kernel": kernel, "kernel_ms_per_launch": kernel_ms, "algorithmic_flop_per_launch": flops,
+              "game_steps_per_launch": steps, "traffic": traffic,
+              "fp32_peak_tflops": fp32_peak, "fp32_peak_source": pk["fp32_source"],
+              "tensor_peak_tflops": pk["bf16_tflops"], "tensor_peak_source": f"dense bf16 burst ({pk['source']})"}
+    if form == "fp32":
+        achieved = flops / t / 1e12
+        return {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                "frac": achieved / fp32_peak, **common}
+    if form in ("tc-bf16", "tc-fp16"):
+        # FP32 chains for encoder and trunk; tensor-core scores with exact FP32 re-scores of the candidate chunks
+        achieved = trunk / t / 1e12
+        return {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                "frac": achieved / fp32_peak, "fp32_pipe_flop_per_launch": trunk,
+                "tensor_flop_per_launch": scoring,
+                "min_ms_at_peaks": 1e3 * (trunk / (fp32_peak * 1e12) + scoring / (pk["bf16_tflops"] * 1e12)),
+                **common}
+    achieved = flops / t / 1e12
+    return {"bound": "tensor", "achieved": achieved, "peak": pk["bf16_tflops"], "unit": "TFLOP/s",
+            "frac": achieved / pk["bf16_tflops"], "fp16 operands": "run at the bf16 rate", **common}
+
+
+def form_line(rt, torch, stream, world, local, form, tau, steps, gen, counts, cfg, sample_clocks=False):
+    """Times `steps` generations of `form` after one untimed generation at that form."""
+    rt.set_form(FORMS[form])
+    if form.startswith("tc-trunk"):
+        rt.set_margin_guard(tau)
+    rt.advance(seed=1000 + gen, counts=counts, config=cfg)
+    gen += 1
+    agg, gen = time_generations(rt, torch, stream, world, local, steps, gen, counts, cfg, sample_clocks)
+    return agg, gen
+
+
+def e2e_line(rt, torch, stream, world, offsets, words, counts, cfg, gen, iterations):
+    """The metric through the public API with host buffers: every step uploads its cell lists from pinned host
+    memory (nwg_set_cell_words), advances one generation and reads the summary back."""
+    pinned_offsets = torch.from_numpy(offsets).pin_memory().numpy()
+    pinned_words = torch.from_numpy(words).pin_memory().numpy()
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    steps = 0
+    barrier(world)
+    torch.cuda.synchronize()
+    start.record(stream)
+    for _ in range(iterations):
+        rt.set_cell_words(pinned_offsets, pinned_words)
+        rt.advance(seed=1000 + gen, counts=counts, config=cfg)
+        steps += rt.stats().game_steps
+        _ = rt.summary().best_fitness
+        gen += 1
+    end.record(stream)
+    torch.cuda.synchronize()
+    ms = max_over_ranks(start.elapsed_time(end), world)
+    total = sum_over_ranks(float(steps), world)
+    return {"value": total / (ms * 1e-3), "unit": "game-steps/s",
+            "h2d_bytes_per_step": int(offsets.nbytes + words.nbytes + 120), "d2h_bytes_per_step": 4 + 48 + 24,
+            "steps": iterations, "ms_per_step": ms / iterations}, gen
+
+
+def cpu_model() -> str:
+    try:
+        for line in subprocess.run(["lscpu"], capture_output=True, text=True, timeout=10).stdout.splitlines():
+            if line.startswith("Model name:"):
+                return line.split(":", 1)[1].strip()
+    except (OSError, subprocess.SubprocessError):
+        pass
+    return "unknown"
+
+
+def cpu_baseline_on(rt, catalog, offsets, words, action_count, label):
+    """The reference's CPU path (oracle/_ref/libref_host.so, every host thread) on genomes of the runtime's current
+    generation with their own cells."""
+    threads = os.cpu_count() or 1
+    sample = min(len(rt.current_generation()["slots"]), max(2, threads))
+    gen = rt.current_generation()
+    genomes = np.stack([rt.download_slot(int(gen["slots"][i])).view(np.uint16) for i in range(sample)])
+    res = cpu_reference_rate(catalog, offsets, words, genomes, action_count, sample, threads)
+    if res is None:
+        return None
+    rate, dt, steps = res
+    return {"value": rate, "unit": "game-steps/s", "cores": threads, "cpu": cpu_model(), "kind": "reference",
+            "sample": f"{label}: evaluation of {sample} individuals (generation {gen['generation_index']}) with "
+                      f"their own cells, {steps} game steps in {dt:.1f} s on {threads} threads"}
+
+
+def reference_gpu(nwg, torch, wl, catalog, population=256, columns=16, repeats=3):
+    """The reference's own CUDA evaluation on this B200: oracle/_ref/libref_ckpt.so (slab_runtime.cu compiled for
+    sm_100a) runs TryEvaluateCurrentGenerationFitnessOnDevice (slab_runtime.cu:1086; warp scorer above 128
+    actions, slab_runtime.cu:452-549) through its own API on a bootstrapped slice of the workload: `population`
+    individuals at the full action space, each playing the 3 x 256 episodes of a 256-word foundation shard. This
+    library evaluates the same genomes (its bootstrap is the reference's, bit for bit) and the same shard with the
+    plain form and the exact tensor-core-screened form; their fitness must equal the reference's."""
+    import ctypes as C
+
+    from oracle import pyoracle as O
+
+    L = O.ref_ckpt()
+    if L is None:
+        return {"unavailable": "oracle/_ref/libref_ckpt.so was not built"}
+    capi = nwg.capi
+    counts = capi.word_counts(training=wl.secrets_per_cell, action_space=wl.action_count)
+    stride = capi.genome_stride_bytes(wl.action_count)
+    rc = capi.RuntimeConfig()
+    rc.genotype_slab_byte_budget_bytes = 2 * population * stride
+    rc.generation_byte_budget_bytes = population * stride
+    rc.action_count, rc.population_size_ceiling, rc.grid_column_count = wl.action_count, population, columns
+    ms = np.zeros(repeats, np.float64)
+    ref_fit = np.zeros(population, np.float32)
+    letters = np.ascontiguousarray(catalog, np.uint8)
+    seed = 11
+    if L.refckpt_time_evaluation(C.addressof(rc), letters.ctypes.data, len(letters), population, seed, 0,
+                                 C.addressof(counts), repeats, ms.ctypes.data, ref_fit.ctypes.data) != 1:
+        return {"unavailable": "the reference runtime failed on the slice"}
+    nwg.capi.upload_catalog(catalog)
+    rt = nwg.Runtime(wl.action_count, population, columns, stream=torch.cuda.current_stream().cuda_stream)
+    rt.bootstrap(population, seed=seed)
+    ours = {}
+    for form in ("fp32", "tc-fp16"):
+        rt.set_form(FORMS[form])
+        rt.evaluate(counts)  # warm-up (and the tables of the tensor-core form)
+        times = []
+        for _ in range(repeats):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            rt.evaluate(counts)
+            times.append(1e3 * (time.perf_counter() - t0))
+        st = rt.stats()
+        fit = rt.current_generation()["fitness"]
+        ours[form] = {"ms": statistics.median(times), "game_steps": int(st.game_steps),
+                      "fitness_equals_reference": bool(np.array_equal(fit.view(np.uint32), ref_fit.view(np.uint32)))}
+    rt.close()
+    steps = ours["fp32"]["game_steps"]
+    ref_ms = float(np.median(ms[1:])) if repeats > 1 else float(ms[0])
+    return {"value": steps / (ref_ms * 1e-3), "unit": "game-steps/s", "ms_per_evaluation": ref_ms,
+            "ms_all_calls": [round(float(x), 2) for x in ms],
+            "slice": f"{population} individuals ({population // columns}x{columns}) x {wl.action_count} actions, "
+                     f"foundation shard of {wl.secrets_per_cell} words (768 episodes each), {steps} game steps",
+            "what": "the reference's TryEvaluateCurrentGenerationFitnessOnDevice (slab_runtime.cu:1086) compiled for "
+                    "sm_100a from its sources, host clock around each call (each synchronises)",
+            "ours_same_slice": {f: {"value": o["game_steps"] / (o["ms"] * 1e-3), "ms_per_evaluation": o["ms"],
+                                    "fitness_equals_reference": o["fitness_equals_reference"],
+                                    "speedup_over_reference_gpu": ref_ms / o["ms"]} for f, o in ours.items()}}
+
+
+def run_bands(args, nwg, torch, wl, rank, world, local) -> None:
+    """N > 1: one population split by grid rows, one band per rank (nwg_set_band): fitness all-gathered, halo genomes
+    exchanged with the neighbour bands, every band breeding its own rows. Total work is fixed (strong scaling)."""
+    bands = importlib.import_module("neuroevolutionary-wordle_b200.bands")
+    catalog = wl.catalog()
+    offsets, words = wl.cell_lists()
+    nwg.capi.upload_catalog(catalog)
+    layout = bands.band_layout(wl.population // wl.columns, wl.columns, world, rank, wl.radius)
+    band = bands.BandRuntime(layout, wl.action_count)
+    band.rt.set_form(FORMS[args.form])
+    if args.form.startswith("tc-trunk"):
+        band.rt.set_margin_guard(args.tau)
+    band.bootstrap(0)
+    band.set_cell_words(offsets, words)
+    counts = nwg.capi.word_counts(training=wl.action_count, action_space=wl.action_count)
+    cfg = nwg.capi.assembly_config(radius=wl.radius, p=wl.mutation_probability, sigma=wl.mutation_sigma)
+    stream = torch.cuda.current_stream()
+    gen = 0
+    for _ in range(args.warmup):
+        band.advance(1000 + gen, counts, cfg)
+        gen += 1
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    steps = 0
+    kernel_ms = []
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.__enter__()
+    start.record(stream)
+    for _ in range(args.steps):
+        band.advance(1000 + gen, counts, cfg)
+        st = band.rt.stats()
+        steps += st.game_steps
+        kernel_ms.append(st.eval_kernel_ms)
+        gen += 1
+    end.record(stream)
+    torch.cuda.synchronize()
+    clocks.__exit__(None, None, None)
+    barrier(world)
+    ms = max_over_ranks(start.elapsed_time(end), world)
+    total = sum_over_ranks(float(steps), world)
+    # end to end: host cell lists uploaded every step, the band summary read back
+    pinned_offsets = torch.from_numpy(offsets).pin_memory().numpy()
+    pinned_words = torch.from_numpy(words).pin_memory().numpy()
+    iters = max(1, min(args.steps, 3))
+    e_steps = 0
+    barrier(world)
+    torch.cuda.synchronize()
+    start.record(stream)
+    for _ in range(iters):
+        band.set_cell_words(pinned_offsets, pinned_words)
+        band.advance(1000 + gen, counts, cfg)
+        e_steps += band.rt.stats().game_steps
+        _ = band.rt.summary().best_fitness
+        gen += 1
+    end.record(stream)
+    torch.cuda.synchronize()
+    e_ms = max_over_ranks(start.elapsed_time(end), world)
+    e_total = sum_over_ranks(float(e_steps), world)
+    mean, var = band.fitness_moments()  # whole grid, FP64 (one all-reduce of three sums)
+    band_bytes = (layout.cells + 1) * 4 + int(offsets[layout.first_cell + layout.cells] - offsets[layout.first_cell]) * 4
+    if rank == 0:
+        print(json.dumps({
+            "metric": "game-steps/s", "value": total / (ms * 1e-3), "unit": "game-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": DTYPES[args.form], "data": "synthetic",
+            "impl": "ours", "generations_per_s": args.steps / (ms * 1e-3),
+            "config": {"workload": wl.name, "population": wl.population,
+                       "grid": f"{wl.population // wl.columns}x{wl.columns}", "action_count": wl.action_count,
+                       "secrets_per_cell": wl.secrets_per_cell, "form": FORM_NAMES[args.form],
+                       "parallelism": f"row bands: {world} bands of {layout.rows} rows, halo {layout.halo} row(s); "
+                                      "fitness all-gather + halo genome exchange (NCCL) per generation",
+                       "l2": "inputs larger than L2"},
+            "e2e": {"value": e_total / (e_ms * 1e-3), "unit": "game-steps/s", "h2d_bytes_per_step": band_bytes + 120,
+                    "d2h_bytes_per_step": 76},
+            "gpu_launches": (kernel_launches(args.form) + 3) * args.steps,
+            "eval_kernel_ms_rank0": sum(kernel_ms) / len(kernel_ms),
+            "last_evaluation_fp64": {"fitness_mean": mean, "fitness_variance": var},
+            "clocks": clocks.summary(),
+        }), flush=True)
+    band.close()
+
+
 def run_ours(args) -> None:
     import torch
 
     rank, world, local = dist_setup(args.gpus)
     nwg = importlib.import_module("neuroevolutionary-wordle_b200")
     wl = {"full": nwg.workload.FULL, "medium": nwg.workload.MEDIUM, "small": nwg.workload.SMALL}[args.workload]
+    if world > 1:
+        run_bands(args, nwg, torch, wl, rank, world, local)
+        return
     catalog = wl.catalog()
     offsets, words = wl.cell_lists()
     nwg.capi.upload_catalog(catalog)
     stream = torch.cuda.current_stream()
+    pk = peaks()
+    fp32_peak = nwg.capi.measure_fp32_peak(stream.cuda_stream)
+    pk["fp32_source"] = "measured live by nwg_measure_fp32_peak (independent FFMA chains on every SM)"
     rt = nwg.Runtime(wl.action_count, wl.population, wl.columns, stream=stream.cuda_stream)
     rt.set_cell_words(offsets, words)
-    trunk_form = args.form.startswith("tc-trunk")
-    rt.set_form(FORMS[args.form])
-    if trunk_form:
-        rt.set_margin_guard(args.tau)
-    rt.bootstrap(wl.population, seed=0 + rank)
+    rt.bootstrap(wl.population, seed=0)
     counts = nwg.capi.word_counts(training=wl.action_count, action_space=wl.action_count)
     cfg = nwg.capi.assembly_config(radius=wl.radius, p=wl.mutation_probability, sigma=wl.mutation_sigma)
-
-    # CPU baseline sample: the reference CPU path on the first genomes of generation 0 (rank 0, N=1 only).
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        threads = os.cpu_count() or 1
-        sample = min(wl.population, max(2, threads))
-        genomes = np.stack([rt.download_slot(i).view(np.uint16) for i in range(sample)])
-        res = cpu_reference_rate(catalog, offsets, words, genomes, wl.action_count, sample, threads)
-        if res is not None:
-            rate, dt, steps = res
-            cpu = {"value": rate, "unit": "game-steps/s", "cores": threads, "kind": "reference",
-                   "sample": f"generation-0 evaluation of {sample} of {wl.population} individuals "
-                             f"({steps} game steps, {dt:.1f} s) with {threads} threads"}
-
+    form = args.form
+    rt.set_form(FORMS[form])
+    if form.startswith("tc-trunk"):
+        rt.set_margin_guard(args.tau)
     gen = 0
     for _ in range(args.warmup):
         rt.advance(seed=1000 + gen, counts=counts, config=cfg)
         gen += 1
 
-    # ---- device-resident timed region ----
+    # ---- the headline form, device-resident ----
     agg, gen = time_generations(rt, torch, stream, world, local, args.steps, gen, counts, cfg, sample_clocks=True)
     ms = agg["ms"]
     steps = agg["steps"]
-    total_steps = sum_over_ranks(float(steps), world)
+    value = steps / (ms * 1e-3)
+    traffic_file = TRAFFIC_FILES.get(form)
+    traffic = json.loads(traffic_file.read_text()).get("bytes_per_launch") if traffic_file and traffic_file.exists() \
+        else None
+    kernel_mean_ms = sum(agg["kernel_ms"]) / len(agg["kernel_ms"])
+    line_roofline = roofline(form, steps / args.steps, agg["encoded"] / args.steps, wl.action_count, kernel_mean_ms,
+                             pk, fp32_peak, traffic)
 
-    # ---- end-to-end through the public API with host buffers ----
-    pinned_offsets = torch.from_numpy(offsets).pin_memory().numpy()
-    pinned_words = torch.from_numpy(words).pin_memory().numpy()
-    e2e_start = torch.cuda.Event(enable_timing=True)
-    e2e_end = torch.cuda.Event(enable_timing=True)
-    e2e_steps = 0
-    e2e_iters = max(1, min(args.steps, 3))
-    barrier(world)
-    torch.cuda.synchronize()
-    e2e_start.record(stream)
-    for _ in range(e2e_iters):
-        rt.set_cell_words(pinned_offsets, pinned_words)
-        rt.advance(seed=1000 + gen, counts=counts, config=cfg)
-        e2e_steps += rt.stats().game_steps
-        _ = rt.summary().best_fitness
-        gen += 1
-    e2e_end.record(stream)
-    torch.cuda.synchronize()
-    e2e_ms = max_over_ranks(e2e_start.elapsed_time(e2e_end), world)
-    e2e_total = sum_over_ranks(float(e2e_steps), world)
+    # ---- the headline form end to end through the public API ----
+    e2e, gen = e2e_line(rt, torch, stream, world, offsets, words, counts, cfg, gen, max(1, min(args.steps, 3)))
 
-    # ---- the plain FP32 form on the same workload, and the trunk form's agreement with it ----
-    plain = None
-    agree = None
-    if args.form != "fp32" and not args.no_plain:
-        if rank == 0 and trunk_form:
-            agree = agreement_sample(rt, torch, counts, FORMS[args.form], args.tau, 3 * wl.secrets_per_cell)
-        rt.set_form(0)
-        for _ in range(1):
-            rt.advance(seed=1000 + gen, counts=counts, config=cfg)
-            gen += 1
-        pagg, gen = time_generations(rt, torch, stream, world, local, args.steps, gen, counts, cfg)
-        plain_value = sum_over_ranks(float(pagg["steps"]), world) / (pagg["ms"] * 1e-3)
-        plain = {"value": plain_value, "unit": "game-steps/s", "ms_per_step": pagg["ms"] / args.steps,
-                 "eval_kernel_ms": sum(pagg["kernel_ms"]) / len(pagg["kernel_ms"]),
-                 "speedup_of_this_form": (total_steps / (ms * 1e-3)) / plain_value,
-                 "note": "plain FP32 form, same workload and process, after this form's timed generations"}
+    # ---- the CPU baseline on the generation just timed ----
+    cpu = None if args.no_cpu_baseline else cpu_baseline_on(rt, catalog, offsets, words, wl.action_count,
+                                                             "the timed run's latest generation")
 
-    if rank != 0:
-        rt.close()
-        return
+    others = {}
+    agreement = {}
+    if not args.no_plain:
+        for other in [f for f in ("fp32", "tc-trunk-fp16", "tc-trunk-bf16") if f != form]:
+            oagg, gen = form_line(rt, torch, stream, world, local, other, args.tau, args.steps, gen, counts, cfg)
+            o_kernel = sum(oagg["kernel_ms"]) / len(oagg["kernel_ms"])
+            o_value = oagg["steps"] / (oagg["ms"] * 1e-3)
+            entry = {"value": o_value, "unit": "game-steps/s", "ms_per_step": oagg["ms"] / args.steps,
+                     "generations_per_s": args.steps / (oagg["ms"] * 1e-3), "dtype": DTYPES[other],
+                     "form": FORM_NAMES[other],
+                     "roofline": roofline(other, oagg["steps"] / args.steps, oagg["encoded"] / args.steps,
+                                          wl.action_count, o_kernel, pk, fp32_peak,
+                                          (json.loads(TRAFFIC_FILES[other].read_text()).get("bytes_per_launch")
+                                           if other in TRAFFIC_FILES and TRAFFIC_FILES[other].exists() else None))}
+            if other.startswith("tc-trunk"):
+                entry["margin_tau"] = args.tau
+                entry["rescoring"] = {"candidate_chunks_per_step": oagg["candidates"] / max(oagg["steps"], 1),
+                                      "fallback_fraction": oagg["fallbacks"] / max(oagg["steps"], 1)}
+                if other == "tc-trunk-fp16":
+                    entry["e2e"], gen = e2e_line(rt, torch, stream, world, offsets, words, counts, cfg, gen,
+                                                 max(1, min(args.steps, 3)))
+            others[other] = entry
+        plain_value = others["fp32"]["value"] if "fp32" in others else value
+        for name, entry in others.items():
+            entry["speedup_over_plain_fp32"] = entry["value"] / plain_value
+        # guess agreement of the 16-bit trunk forms and of the headline with the plain form, whole population
+        for f in [x for x in (form, "tc-trunk-fp16", "tc-trunk-bf16") if x != "fp32"]:
+            agreement[f] = agreement_sample(rt, torch, counts, FORMS[f], args.tau, 3 * wl.secrets_per_cell)
+
+    ref_gpu = None
+    if not args.no_reference_gpu and args.workload == "full":
+        ref_gpu = reference_gpu(nwg, torch, wl, catalog)
+        nwg.capi.upload_catalog(catalog)
     race = None
-    if world == 1 and not args.no_surrogate and args.workload == "full":
+    if not args.no_surrogate and args.workload == "full":
         rt.close()
         rt = None
         race = surrogate_vs_plain(nwg, wl, torch, args.surrogate_generations)
-    pk = peaks()
-    mean_steps = steps / args.steps
-    mean_encoded = agg["encoded"] / args.steps
-    kernel_mean_ms = sum(agg["kernel_ms"]) / len(agg["kernel_ms"])
-    flops = algorithmic_flops(int(mean_steps), int(mean_encoded), wl.action_count)
-    achieved_tflops = flops / (kernel_mean_ms * 1e-3) / 1e12
-    fp32_peak = 148 * 128 * 2 * pk["sm_max_mhz"] * 1e6 / 1e12
-    traffic_file = TRAFFIC_TCT if trunk_form else TRAFFIC
-    traffic = None
-    if traffic_file.exists() and (trunk_form or args.form == "fp32"):
-        traffic = json.loads(traffic_file.read_text()).get("bytes_per_launch")
-    if trunk_form or args.form in ("tc-bf16", "tc-fp16"):
-        kernel = "EvalTctKernel" if trunk_form else "EvalTcKernel"
-        roofline = {"kernel": kernel, "bound": "tensor", "achieved": achieved_tflops, "peak": pk["bf16_tflops"],
-                    "unit": "TFLOP/s", "frac": achieved_tflops / pk["bf16_tflops"], "traffic": traffic,
-                    "peak_source": f"dense bf16 burst ({pk['source']}); fp16 operands run at the same rate",
-                    "frac_of_fp32_peak": achieved_tflops / fp32_peak}
-    else:
-        roofline = {"kernel": "EvalFp32Kernel", "bound": "fp32", "achieved": achieved_tflops, "peak": fp32_peak,
-                    "unit": "TFLOP/s", "frac": achieved_tflops / fp32_peak, "traffic": traffic,
-                    "peak_source": f"148 SMs x 128 FFMA/clk x 2 x {pk['sm_max_mhz']:.0f} MHz "
-                                   f"(sm_max_mhz {pk['source']})",
-                    "frac_of_bf16_tensor_peak": achieved_tflops / pk["bf16_tflops"]}
-    roofline.update({"kernel_ms_per_launch": kernel_mean_ms, "algorithmic_flop_per_launch": flops,
-                     "game_steps_per_launch": mean_steps})
-    value = total_steps / (ms * 1e-3)
     line = {
         "metric": "game-steps/s",
         "value": value,
@@ -466,7 +700,8 @@ def run_ours(args) -> None:
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": DTYPES[args.form],
+        "dtype": DTYPES[form],
+        "precision": PRECISION[form],
         "data": "synthetic",
         "impl": "ours",
         "generations_per_s": args.steps / (ms * 1e-3),
@@ -474,22 +709,21 @@ def run_ours(args) -> None:
                    f"{wl.columns}", "action_count": wl.action_count, "secrets_per_cell": wl.secrets_per_cell,
                    "secret_subset": wl.secret_subset, "episodes_per_secret": 3, "selection_radius": wl.radius,
                    "mutation_probability": wl.mutation_probability, "mutation_sigma": wl.mutation_sigma,
-                   "form": FORM_NAMES[args.form], "margin_tau": args.tau if trunk_form else None,
-                   "parallelism": f"{world} independent populations (one per GPU)",
+                   "form": FORM_NAMES[form], "margin_tau": args.tau if form.startswith("tc-trunk") else None,
+                   "parallelism": "one GPU, the whole population",
                    "l2": "inputs larger than L2 (genome slab "
                          f"{wl.population * nwg.capi.genome_stride_bytes(wl.action_count) / 1e9:.2f} GB)"},
-        "roofline": roofline,
+        "roofline": line_roofline,
         "cpu_baseline": cpu,
-        "e2e": {"value": e2e_total / (e2e_ms * 1e-3), "unit": "game-steps/s",
-                "h2d_bytes_per_step": int(offsets.nbytes + words.nbytes + 120),
-                "d2h_bytes_per_step": 4 + 48 + 24},
-        "gpu_launches": (KERNELS_PER_GENERATION + EXTRA_KERNELS[args.form]) * args.steps,
+        "e2e": e2e,
+        "gpu_launches": kernel_launches(form) * args.steps,
         "rescoring": {"chunks_per_step": agg["rescored"] / max(steps, 1),
                       "full_rescore_fraction": agg["full"] / max(steps, 1),
                       "candidate_chunks_per_step": agg["candidates"] / max(steps, 1),
                       "fallback_fraction": agg["fallbacks"] / max(steps, 1)},
-        "plain_fp32": plain,
-        "agreement_with_plain": agree,
+        "other_forms": others or None,
+        "agreement_with_plain": agreement or None,
+        "reference_gpu": ref_gpu,
         "surrogate_vs_plain": race,
         "clocks": agg["clocks"],
     }
@@ -631,10 +865,30 @@ def run_reference(args) -> None:
         "config": {"workload": wl.name, "population": wl.population, "action_count": wl.action_count,
                    "secrets_per_cell": wl.secrets_per_cell, "form": "reference CPU path",
                    "sample_per_step": f"evaluation of {sample} individuals"},
-        "cpu_baseline": {"value": value, "unit": "game-steps/s", "cores": threads, "kind": "reference",
+        "cpu_baseline": {"value": value, "unit": "game-steps/s", "cores": threads, "cpu": cpu_model(),
+                         "kind": "reference",
                          "sample": f"{sample} individuals per step, {steps_total} game steps timed"},
         "e2e": {"value": value, "unit": "game-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
+
+
+def launch_ranks(args) -> None:
+    """`--gpus N` outside a launcher: start N ranks (one process per GPU) under torch.distributed.run on this node
+    and exit with their status. Under a launcher whose world size differs from N, refuse."""
+    world = int(os.environ.get("WORLD_SIZE", "0"))
+    if world == args.gpus or (world == 0 and args.gpus == 1):
+        return
+    if world != 0 or args.gpus < 1:
+        print(json.dumps({"error": f"--gpus {args.gpus} but the launcher started {world} rank(s)"}), file=sys.stderr)
+        sys.exit(2)
+    import socket
+
+    with socket.socket() as sock:
+        sock.bind(("127.0.0.1", 0))
+        port = sock.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), str(Path(__file__).resolve()), *sys.argv[1:]]
+    sys.exit(subprocess.call(cmd))
 
 
 def main() -> None:
@@ -646,15 +900,21 @@ def main() -> None:
     ap.add_argument("--workload", choices=["full", "medium", "small", "growth"], default="full",
                     help="growth: the batching form (16,384 individuals, uneven shards, widening action space)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--form", choices=sorted(FORMS), default="tc-trunk-fp16")
-    ap.add_argument("--no-plain", action="store_true", help="skip the plain FP32 comparison and the agreement sample")
+    ap.add_argument("--form", choices=sorted(FORMS), default="tc-fp16",
+                    help="headline form (default: FP32 trunk and decisions, tensor-core screening; results "
+                         "bit-identical to the reference's)")
+    ap.add_argument("--no-plain", action="store_true", help="skip the other forms and the agreement samples")
     ap.add_argument("--tau", type=float, default=1e-3, help="margin guard of the tensor-core trunk forms (1e-3 x the score scale)")
     ap.add_argument("--no-surrogate", action="store_true", help="skip the surrogate-vs-plain race")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip timing the reference's own CUDA evaluation on a slice of the workload")
     ap.add_argument("--surrogate-generations", type=int, default=50)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
-    elif args.workload == "growth":
+        return
+    launch_ranks(args)
+    if args.workload == "growth":
         run_growth(args)
     else:
         run_ours(args)

@@ -214,6 +214,13 @@ int nwg_set_evaluation_form(nwg_runtime *runtime, int form);
  * back); a huge tau sends every step through the exact path. Negative or non-finite tau is rejected. */
 int nwg_set_margin_guard(nwg_runtime *runtime, float tau);
 
+/* Poll limit of every bounded mbarrier wait in the tensor-core evaluation kernels (default 2^26; no counterpart in
+ * the reference, whose kernels have no such waits). A wait that reaches it gives up: the evaluation stops issuing
+ * copies and tensor-core work, waits (bounded) for what is in flight, releases tensor memory and returns
+ * NWG_TIMEOUT, the sticky-first-failure convention of slab_runtime.cu:288-290; the runtime stays usable. A limit
+ * of 0 gives up at the first wait whose phase has not completed yet, which is how the tests exercise that path. */
+int nwg_set_wait_limit(nwg_runtime *runtime, uint32_t polls);
+
 /* TryBootstrapRandomCurrentGenerationOnDevice (slab_runtime.hpp:123-124). */
 int nwg_bootstrap(nwg_runtime *runtime, size_t generation_size, uint32_t generation_seed, size_t generation_index);
 
@@ -665,10 +672,45 @@ int nwg_breed_device(const void *parent_slab, size_t parent_pitch, const uint32_
 int nwg_bootstrap_device(void *slab, size_t pitch, size_t population, size_t generation_index, uint32_t seed,
                          size_t action_count, void *cuda_stream);
 
+/* FP32 fused multiply-add throughput of the current device in TFLOP/s, measured by a short kernel of independent
+ * FMA chains on every SM (no counterpart in the reference): the roofline denominator of the FP32 evaluation forms.
+ * Allocates a few bytes, synchronises the stream. */
+int nwg_measure_fp32_peak(double *tflops_out, void *cuda_stream);
+
+/* ---- Row bands: one population split by grid rows across ranks (no counterpart in the reference, which runs on
+ * one GPU). The split follows the path's own dependencies: evaluation is per individual; selection reads the
+ * fitness of the Moore neighbourhood (selection_ops.cuh:218-263, spatial/grid.hpp:181-218), so a band selects over
+ * the whole grid's fitness, gathered by the caller; breeding reads the two parents' genomes
+ * (genome_ops.cuh:386-407), which for children on a band's edge lie up to `radius` rows into the neighbouring
+ * band, so each band holds `halo_rows` rows above and below it, copied in by the caller. Children keep their
+ * whole-grid indices in every Philox stream, so the bands together produce exactly the children of a single
+ * runtime holding the whole grid.
+ *
+ * nwg_set_band: this runtime holds rows [band_row_first, band_row_first + rows) of a grid of global_rows rows
+ * (rows = population_size_ceiling / grid_column_count); the top 2 * halo_rows * columns slots of its slab hold the
+ * halo (create it with room for two band generations plus those slots). global_rows = 0 returns to a whole
+ * population. The whole-grid paths (nwg_prepare_generation, nwg_advance, nwg_advance_graphed) return
+ * NWG_UNSUPPORTED in band mode; nwg_bootstrap of a band (its full size) draws its rows' organisms of the whole
+ * grid's generation. Per generation:
+ *   nwg_evaluate (the band's own cells, set by nwg_set_cell_words in band order);
+ *   nwg_device_generation -> the band's fitness and has-fitness device arrays, gathered by the caller into the
+ *     whole grid's arrays (band k at offset k * band cells);
+ *   nwg_band_prepare: selection for the band's children over the whole grid (radius <= halo_rows, <= 2);
+ *   nwg_band_copy_rows: band rows [band_row, band_row + rows) into a device buffer (the halo a neighbour needs);
+ *   nwg_band_install_halo: the rows above (global rows first - halo .. first - 1) and below (first + rows ..),
+ *     halo_rows * columns genomes each at src_pitch, from device buffers;
+ *   nwg_assemble_prepared: breed the band's children and make them the current generation. */
+int nwg_set_band(nwg_runtime *runtime, size_t global_rows, size_t band_row_first, size_t halo_rows);
+int nwg_device_generation(const nwg_runtime *runtime, void **fitness, void **has_fitness, size_t *count);
+int nwg_band_prepare(nwg_runtime *runtime, uint32_t generation_seed, const nwg_generation_assembly_config *config,
+                     const float *fitness_all, const uint8_t *has_fitness_all);
+int nwg_band_copy_rows(nwg_runtime *runtime, size_t band_row, size_t rows, void *dst, size_t dst_pitch);
+int nwg_band_install_halo(nwg_runtime *runtime, const void *above, const void *below, size_t src_pitch);
+
 /* Fitness evaluation that allocates no device memory. No counterpart in the reference.
- * For callers that cannot call cudaMalloc: work being captured into a CUDA graph (an allocation would
- * break the capture), embedders whose device memory belongs to another allocator or pool, and processes
- * that keep a fixed device-memory footprint after start-up. Every pointer is a device pointer the caller
+ * For callers that cannot call cudaMalloc: embedders whose device memory belongs to another allocator or
+ * pool, and processes that keep a fixed device-memory footprint after start-up (a late allocation can fail
+ * or stall the device). Every pointer is a device pointer the caller
  * owns: the slab (individual i's genome image at slab + slot_indices[i] * slot_pitch), the catalog as
  * rows of 5 letter indices, the per-cell word lists in CSR form (catalog indices), and the outputs
  * fitness[population] and, when not NULL, counters[3] (game steps, encoded turns, episodes). The
@@ -677,8 +719,10 @@ int nwg_bootstrap_device(void *slab, size_t pitch, size_t population, size_t gen
  * exits; it limits population to 4,096 and the catalog to 4,739 words (NWG_UNSUPPORTED beyond). All
  * calls share that array and it keeps the last call's contents, so calls that overlap on the GPU (other
  * streams or host threads) race and must be serialised by the caller. The first call on each device
- * resolves the array's device address; make that first call before any stream capture. The call
- * synchronises its stream and returns the evaluation status. */
+ * resolves the array's device address (cudaGetSymbolAddress with that device current). A cell whose
+ * offsets decrease, or whose list is empty or longer than 2^20 words, gives NWG_INVALID_TRAINING_SHARD
+ * without a read of its words. population 0 gives NWG_INVALID_RUNTIME_CONFIG. The call synchronises its
+ * stream and returns the evaluation status. */
 int nwg_evaluate_noalloc(const void *slab, size_t slot_pitch, const uint32_t *slot_indices, size_t population,
                          size_t grid_column_count, size_t action_count, const uint8_t *catalog_letters,
                          size_t catalog_count, const uint32_t *cell_offsets, const uint32_t *cell_words,

@@ -211,6 +211,8 @@ EXPORTS = [
     "nwg_read_solve_rates", "nwg_read_score_table", "nwg_mlp_create", "nwg_mlp_destroy", "nwg_mlp_set_stream", "nwg_mlp_parameter_count",
     "nwg_mlp_parameters", "nwg_mlp_forward", "nwg_mlp_gradients", "nwg_mlp_train_step", "nwg_bf16_gemm_nt",
     "nwg_descriptors", "nwg_surrogate_create", "nwg_surrogate_destroy", "nwg_surrogate_advance",
+    "nwg_set_band", "nwg_device_generation", "nwg_band_prepare", "nwg_band_copy_rows", "nwg_band_install_halo",
+    "nwg_measure_fp32_peak", "nwg_set_wait_limit",
 ]
 
 
@@ -310,7 +312,21 @@ def lib() -> C.CDLL:
     L.nwg_breed_device.argtypes = [_vp, _sz, _vp, _vp, _sz, _vp, _sz, _sz, C.c_uint32, _sz,
                                    C.POINTER(BreedingConfig), C.POINTER(MutationConfig), _vp]
     L.nwg_bootstrap_device.argtypes = [_vp, _sz, _sz, _sz, C.c_uint32, _sz, _vp]
+    L.nwg_set_band.argtypes = [_vp, _sz, _sz, _sz]
+    L.nwg_device_generation.argtypes = [_vp, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_sz)]
+    L.nwg_band_prepare.argtypes = [_vp, C.c_uint32, C.POINTER(AssemblyConfig), _vp, _vp]
+    L.nwg_band_copy_rows.argtypes = [_vp, _sz, _sz, _vp, _sz]
+    L.nwg_band_install_halo.argtypes = [_vp, _vp, _vp, _sz]
+    L.nwg_measure_fp32_peak.argtypes = [C.POINTER(C.c_double), _vp]
+    L.nwg_set_wait_limit.argtypes = [_vp, C.c_uint32]
     return L
+
+
+def measure_fp32_peak(stream: int | None = None) -> float:
+    """FP32 FMA throughput of the current device (TFLOP/s), measured by the library's peak kernel."""
+    v = C.c_double()
+    check(lib().nwg_measure_fp32_peak(C.byref(v), stream), "nwg_measure_fp32_peak")
+    return v.value
 
 
 def status_string(status: int) -> str:
@@ -378,11 +394,12 @@ class Runtime:
     """One device GA runtime (DeviceSlabGARuntimeBuffers of the reference)."""
 
     def __init__(self, action_count: int, population: int, columns: int, slab_generations: float = 2.0,
-                 stream: int | None = None):
+                 stream: int | None = None, slab_slots: int | None = None):
         stride = genome_stride_bytes(action_count)
         cfg = RuntimeConfig()
         cfg.generation_byte_budget_bytes = population * stride
-        cfg.genotype_slab_byte_budget_bytes = int(slab_generations * population) * stride
+        slots = slab_slots if slab_slots is not None else int(slab_generations * population)
+        cfg.genotype_slab_byte_budget_bytes = slots * stride
         cfg.host_spillover_byte_budget_bytes = 0
         cfg.action_count = action_count
         cfg.population_size_ceiling = population
@@ -423,6 +440,12 @@ class Runtime:
 
     def set_margin_guard(self, tau: float) -> None:
         check(lib().nwg_set_margin_guard(self.handle, tau), "nwg_set_margin_guard")
+
+    DEFAULT_WAIT_LIMIT = 1 << 26
+
+    def set_wait_limit(self, polls: int) -> None:
+        """Poll limit of the tensor-core kernels' bounded waits (NWG_TIMEOUT when one gives up)."""
+        check(lib().nwg_set_wait_limit(self.handle, polls), "nwg_set_wait_limit")
 
     def bootstrap(self, size: int, seed: int, generation_index: int = 0) -> None:
         check(lib().nwg_bootstrap(self.handle, size, seed, generation_index), "nwg_bootstrap")
@@ -632,6 +655,26 @@ class Runtime:
         pitch = _sz()
         check(lib().nwg_device_slab(self.handle, C.byref(ptr), C.byref(pitch)), "nwg_device_slab")
         return ptr.value, pitch.value
+
+    # ---- row bands (nwg_set_band): one population split by grid rows across ranks ----
+    def set_band(self, global_rows: int, band_row_first: int, halo_rows: int) -> None:
+        check(lib().nwg_set_band(self.handle, global_rows, band_row_first, halo_rows), "nwg_set_band")
+
+    def device_generation(self):
+        """(fitness device pointer, has-fitness device pointer, count) of the current generation."""
+        f, h, n = _vp(), _vp(), _sz()
+        check(lib().nwg_device_generation(self.handle, C.byref(f), C.byref(h), C.byref(n)), "nwg_device_generation")
+        return f.value, h.value, n.value
+
+    def band_prepare(self, seed: int, config: AssemblyConfig | None, fitness_all: int, has_all: int) -> None:
+        check(lib().nwg_band_prepare(self.handle, seed, C.byref(config) if config else None, fitness_all, has_all),
+              "nwg_band_prepare")
+
+    def band_copy_rows(self, band_row: int, rows: int, dst: int, dst_pitch: int) -> None:
+        check(lib().nwg_band_copy_rows(self.handle, band_row, rows, dst, dst_pitch), "nwg_band_copy_rows")
+
+    def band_install_halo(self, above: int, below: int, src_pitch: int) -> None:
+        check(lib().nwg_band_install_halo(self.handle, above, below, src_pitch), "nwg_band_install_halo")
 
 
 class Checkpoint:

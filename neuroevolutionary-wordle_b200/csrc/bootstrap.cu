@@ -30,11 +30,15 @@ __constant__ LayerSpan kLayers[5] = {
     {kTrW3, kTrB3, kHidden1, kPolicy},
 };
 
+// Organism i of this launch is organism organism_first + i of a population of stream_population (a row band of a
+// larger grid draws the streams of its own rows).
 __global__ void __launch_bounds__(kBootstrapThreads) BootstrapKernel(std::uint8_t *slab, std::size_t pitch,
                                                                      const std::uint32_t *slots,
                                                                      std::uint32_t population,
                                                                      std::uint64_t generation_index,
-                                                                     std::uint32_t seed, std::uint32_t action_count) {
+                                                                     std::uint32_t seed, std::uint32_t action_count,
+                                                                     std::uint32_t organism_first,
+                                                                     std::uint32_t stream_population) {
     const std::uint32_t organism = blockIdx.x;
     if (organism >= population) {
         return;
@@ -42,7 +46,9 @@ __global__ void __launch_bounds__(kBootstrapThreads) BootstrapKernel(std::uint8_
     const std::uint32_t slot = slots != nullptr ? slots[organism] : organism;
     __half *genome = reinterpret_cast<__half *>(slab + static_cast<std::size_t>(slot) * pitch);
     const std::uint64_t stream =
-        ((generation_index * static_cast<std::uint64_t>(population) + organism) * kBootstrapThreads) + threadIdx.x;
+        ((generation_index * static_cast<std::uint64_t>(stream_population) + organism_first + organism) *
+         kBootstrapThreads) +
+        threadIdx.x;
     curandStatePhilox4_32_10_t state;
     curand_init(static_cast<unsigned long long>(seed), stream, 0ULL, &state);
     for (int l = 0; l < 5; ++l) {
@@ -67,12 +73,17 @@ __global__ void __launch_bounds__(kBootstrapThreads) BootstrapKernel(std::uint8_
 
 cudaError_t LaunchBootstrap(std::uint8_t *slab, std::size_t pitch, const std::uint32_t *slots,
                             std::uint32_t population, std::uint64_t generation_index, std::uint32_t seed,
-                            std::uint32_t action_count, cudaStream_t stream) {
+                            std::uint32_t action_count, cudaStream_t stream, std::uint32_t organism_first,
+                            std::uint32_t stream_population) {
     if (population == 0) {
         return cudaSuccess;
     }
+    if (stream_population == 0) {
+        stream_population = population;
+    }
     BootstrapKernel<<<population, kBootstrapThreads, 0, stream>>>(slab, pitch, slots, population, generation_index,
-                                                                   seed, action_count);
+                                                                   seed, action_count, organism_first,
+                                                                   stream_population);
     return cudaGetLastError();
 }
 

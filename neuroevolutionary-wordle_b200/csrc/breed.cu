@@ -254,7 +254,7 @@ __global__ void __launch_bounds__(kWarps * 32) BreedKernel(const BreedParams p) 
 
     Stream s;
     s.seed = p.generation_seed;
-    s.subsequence = static_cast<std::uint32_t>(child + p.generation_index * 4099u);
+    s.subsequence = static_cast<std::uint32_t>(p.child_first + child + p.generation_index * 4099u);
     s.position = 0;
     s.cached = false;
     s.cached_pair = 0;

@@ -81,6 +81,7 @@ struct nwg_runtime {
     std::size_t last_table_pitch = 0;  // of the tables the last tensor-core evaluation built (0: none)
     std::uint8_t *trunk_tables = nullptr;
     float margin_tau = 1.0e-3f;
+    std::uint32_t wait_limit = kDefaultWaitLimit;  // bounded mbarrier waits of the tensor-core kernels
     // a generation prepared for assembly (evaluated and planned; nwg_prepare_generation / checkpoint restore)
     bool prepared = false;
     std::uint32_t prepared_seed = 0;
@@ -118,6 +119,13 @@ struct nwg_runtime {
     std::size_t last_eval_population = 0;
     std::size_t last_action_count = 0;
     std::size_t last_eval_generation = 0;
+    // row band of a population split across ranks (nwg_set_band): this runtime holds rows
+    // [band_row_first, band_row_first + band rows) of a grid of band_global_rows rows; the halo rows above and below
+    // live in the top band_reserved_slots slots, which children never take
+    bool band = false;
+    std::size_t band_global_rows = 0, band_row_first = 0, band_halo_rows = 0, band_reserved_slots = 0;
+    std::uint32_t *band_parent_table = nullptr;  // [global population]: parent index -> slot (0xFFFFFFFF: absent)
+    bool band_halo_ready = false;                // the halo of the current generation is installed
 };
 
 namespace {
@@ -322,7 +330,7 @@ bool BuildHintGroup(std::uint32_t word, HintGroup &g) {
 __global__ void PlanChildSlotsKernel(const std::uint32_t *pairs, std::uint32_t child_count,
                                      const std::uint32_t *parent_slots, std::uint32_t parent_count,
                                      std::uint8_t *used, std::uint32_t slot_count, std::uint32_t *child_slots,
-                                     int *status) {
+                                     int *status, std::uint32_t parent_slot_limit) {
     __shared__ std::uint32_t partial[1024];
     __shared__ std::uint32_t base;
     const std::uint32_t t = threadIdx.x;
@@ -333,12 +341,19 @@ __global__ void PlanChildSlotsKernel(const std::uint32_t *pairs, std::uint32_t c
     for (std::uint32_t c = t; c < child_count; c += blockDim.x) {
         const std::uint32_t a = pairs[2 * c];
         const std::uint32_t b = pairs[2 * c + 1];
-        if (a >= parent_count || b >= parent_count || parent_slots[a] >= slot_count || parent_slots[b] >= slot_count) {
+        // parents held in slots at or above slot_count (a band's halo rows) are valid up to parent_slot_limit and
+        // are never candidates for a child's slot
+        if (a >= parent_count || b >= parent_count || parent_slots[a] >= parent_slot_limit ||
+            parent_slots[b] >= parent_slot_limit) {
             SetStatus(status, kInvalidParentIndex);
             continue;
         }
-        used[parent_slots[a]] = 1;
-        used[parent_slots[b]] = 1;
+        if (parent_slots[a] < slot_count) {
+            used[parent_slots[a]] = 1;
+        }
+        if (parent_slots[b] < slot_count) {
+            used[parent_slots[b]] = 1;
+        }
     }
     if (t == 0) {
         base = 0;
@@ -384,6 +399,43 @@ __global__ void CopySlotsKernel(const std::uint8_t *src, std::size_t src_pitch, 
     }
 }
 
+// Copies `n` genomes (`bytes` per genome, a multiple of 16) from slots src_slots[i] to dst + i * dst_pitch.
+__global__ void GatherSlotsKernel(const std::uint8_t *src, std::size_t src_pitch, const std::uint32_t *src_slots,
+                                  std::uint8_t *dst, std::size_t dst_pitch, std::size_t bytes, std::uint32_t n) {
+    const std::size_t vectors = bytes / 16;
+    for (std::uint32_t i = blockIdx.x; i < n; i += gridDim.x) {
+        const uint4 *s = reinterpret_cast<const uint4 *>(src + static_cast<std::size_t>(src_slots[i]) * src_pitch);
+        uint4 *d = reinterpret_cast<uint4 *>(dst + static_cast<std::size_t>(i) * dst_pitch);
+        for (std::size_t v = threadIdx.x; v < vectors; v += blockDim.x) {
+            d[v] = s[v];
+        }
+    }
+}
+
+// The band's parent table over the whole grid: its own rows at their slots, the halo rows above (global rows
+// first - halo .. first - 1, toroidal) and below (first + band .. first + band + halo - 1) at the reserved slots
+// from reserved_base on, every other cell absent.
+__global__ void BandParentTableKernel(std::uint32_t *table, std::uint32_t global_rows, std::uint32_t cols,
+                                      std::uint32_t first_row, std::uint32_t band_rows, std::uint32_t halo_rows,
+                                      const std::uint32_t *band_slots, std::uint32_t reserved_base) {
+    const std::uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= global_rows * cols) {
+        return;
+    }
+    const std::uint32_t row = g / cols;
+    const std::uint32_t col = g - row * cols;
+    const std::uint32_t offset = (row + global_rows - first_row) % global_rows;  // rows after the band's first row
+    std::uint32_t slot = 0xFFFFFFFFu;
+    if (offset < band_rows) {
+        slot = band_slots[offset * cols + col];
+    } else if (offset < band_rows + halo_rows) {  // below the band
+        slot = reserved_base + (halo_rows + offset - band_rows) * cols + col;
+    } else if (offset >= global_rows - halo_rows) {  // above the band
+        slot = reserved_base + (offset - (global_rows - halo_rows)) * cols + col;
+    }
+    table[g] = slot;
+}
+
 void FreeRuntime(nwg_runtime *rt) {
     if (rt == nullptr) {
         return;
@@ -393,7 +445,7 @@ void FreeRuntime(nwg_runtime *rt) {
                            rt->slot_used,  rt->status,       rt->summary,     rt->shards,      rt->cell_offsets,
                            rt->cell_words, rt->local_words,  rt->chunk_start, rt->score_sum,   rt->steps,
                            rt->won_sum,
-                           rt->scratch,    rt->tc_tables,    rt->trunk_tables};
+                           rt->scratch,    rt->tc_tables,    rt->trunk_tables, rt->band_parent_table};
     for (void *p : device_ptrs) {
         if (p != nullptr) {
             cudaFree(p);
@@ -534,7 +586,7 @@ int EvaluateImpl(nwg_runtime *rt, const nwg_runtime_word_counts *counts, const n
                                        rt->stream));
         NWG_TRY(RecordEvent(rt->eval_begin, rt->stream));
         NWG_TRY(LaunchEvalTct(p, rt->tc_tables, TcTablePitch(static_cast<std::uint32_t>(selectable)), rt->trunk_tables,
-                              rt->margin_tau, fp16, rt->steps + 5, EvalGrid(rt), rt->stream));
+                              rt->margin_tau, fp16, rt->steps + 5, EvalGrid(rt), rt->stream, rt->wait_limit));
         NWG_TRY(RecordEvent(rt->eval_end, rt->stream));
     } else {
         const bool fp16 = rt->form == NWG_FORM_TC_FP16;
@@ -547,7 +599,7 @@ int EvaluateImpl(nwg_runtime *rt, const nwg_runtime_word_counts *counts, const n
                                     rt->tc_tables, fp16, rt->stream));
         NWG_TRY(RecordEvent(rt->eval_begin, rt->stream));
         NWG_TRY(LaunchEvalTc(p, rt->tc_tables, TcTablePitch(static_cast<std::uint32_t>(selectable)), kappa, fp16,
-                             rt->steps + 3, EvalGrid(rt), rt->stream));
+                             rt->steps + 3, EvalGrid(rt), rt->stream, rt->wait_limit));
         NWG_TRY(RecordEvent(rt->eval_end, rt->stream));
     }
     NWG_TRY(LaunchFinalizeFitness(rt->score_sum, rt->local_words, population, rt->cur_fitness, rt->cur_eval,
@@ -1127,6 +1179,14 @@ int nwg_set_evaluation_form(nwg_runtime *rt, int form) {
     return kOk;
 }
 
+int nwg_set_wait_limit(nwg_runtime *rt, uint32_t polls) {
+    if (rt == nullptr) {
+        return kInvalidRuntimeConfig;
+    }
+    rt->wait_limit = polls;
+    return kOk;
+}
+
 int nwg_set_margin_guard(nwg_runtime *rt, float tau) {
     if (rt == nullptr || !(tau >= 0.0f) || !(tau <= 3.0e38f)) {
         return kInvalidRuntimeConfig;
@@ -1144,6 +1204,14 @@ int nwg_bootstrap(nwg_runtime *rt, size_t generation_size, uint32_t generation_s
         generation_size % rt->grid_column_count != 0) {
         return kInvalidGeneration;
     }
+    // a band bootstraps its own rows of the whole grid's generation 0 (their organisms' random streams)
+    if (rt->band && generation_size != rt->max_generation_size) {
+        return kInvalidGeneration;
+    }
+    const std::uint32_t organism_first =
+        rt->band ? static_cast<std::uint32_t>(rt->band_row_first * rt->grid_column_count) : 0u;
+    const std::uint32_t stream_population =
+        rt->band ? static_cast<std::uint32_t>(rt->band_global_rows * rt->grid_column_count) : 0u;
     std::vector<std::uint32_t> slots(generation_size);
     for (std::size_t i = 0; i < generation_size; ++i) {
         slots[i] = static_cast<std::uint32_t>(i);
@@ -1157,7 +1225,7 @@ int nwg_bootstrap(nwg_runtime *rt, size_t generation_size, uint32_t generation_s
     NWG_TRY(cudaMemsetAsync(rt->summary, 0, sizeof(SummaryDevice), rt->stream));
     NWG_TRY(LaunchBootstrap(rt->slab, rt->pitch, rt->cur_slots, static_cast<std::uint32_t>(generation_size),
                             generation_index, generation_seed, static_cast<std::uint32_t>(rt->action_count),
-                            rt->stream));
+                            rt->stream, organism_first, stream_population));
     const int st = Sync(rt);
     if (st != kOk) {
         rt->cur_gen_size = 0;
@@ -1165,6 +1233,7 @@ int nwg_bootstrap(nwg_runtime *rt, size_t generation_size, uint32_t generation_s
     }
     rt->cur_gen_index = generation_index;
     rt->cur_gen_size = generation_size;
+    rt->band_halo_ready = false;
     rt->released_parents = false;
     rt->next_gen_index = 0;
     rt->next_gen_size = 0;
@@ -1323,6 +1392,9 @@ int nwg_prepare_generation(nwg_runtime *rt, uint32_t generation_seed, const nwg_
     if (rt == nullptr || counts == nullptr) {
         return kInvalidRuntimeConfig;
     }
+    if (rt->band) {
+        return kUnsupported;  // a band selects over the whole grid's fitness: nwg_band_prepare
+    }
     rt->prepared = false;
     nwg_generation_assembly_config cfg{};
     cfg.parent_selection.cellular_breeding_radius = 2;  // selection.hpp:13-18, spatial/grid.hpp:11
@@ -1422,12 +1494,19 @@ int nwg_prepare_generation(nwg_runtime *rt, uint32_t generation_seed, const nwg_
 namespace {
 
 // The device work of assembling planned children without injection: slot plan, breeding, cleared next arrays.
+// In band mode the parents are named by their index in the whole grid and found through the band's parent table
+// (the band's own slots and its halo slots), the children's streams are their whole-grid indices, and the halo
+// slots are never given to a child.
 cudaError_t AssembleLaunch(nwg_runtime *rt, std::uint32_t generation_seed, const nwg_generation_assembly_config &cfg,
                            std::size_t next_size) {
-    PlanChildSlotsKernel<<<1, 1024, 0, rt->stream>>>(rt->pairs, static_cast<std::uint32_t>(next_size), rt->cur_slots,
-                                                     static_cast<std::uint32_t>(rt->cur_gen_size), rt->slot_used,
-                                                     static_cast<std::uint32_t>(rt->slot_count), rt->next_slots,
-                                                     rt->status);
+    const std::uint32_t *parent_slots = rt->band ? rt->band_parent_table : rt->cur_slots;
+    const std::size_t parent_count =
+        rt->band ? rt->band_global_rows * rt->grid_column_count : rt->cur_gen_size;
+    const std::size_t assignable = rt->slot_count - rt->band_reserved_slots;
+    PlanChildSlotsKernel<<<1, 1024, 0, rt->stream>>>(rt->pairs, static_cast<std::uint32_t>(next_size), parent_slots,
+                                                     static_cast<std::uint32_t>(parent_count), rt->slot_used,
+                                                     static_cast<std::uint32_t>(assignable), rt->next_slots,
+                                                     rt->status, static_cast<std::uint32_t>(rt->slot_count));
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
         return e;
@@ -1435,10 +1514,11 @@ cudaError_t AssembleLaunch(nwg_runtime *rt, std::uint32_t generation_seed, const
     BreedParams bp{};
     bp.parent_slab = rt->slab;
     bp.parent_pitch = rt->pitch;
-    bp.parent_slots = rt->cur_slots;
+    bp.parent_slots = parent_slots;
     bp.child_slab = rt->slab;
     bp.child_pitch = rt->pitch;
     bp.child_slots = rt->next_slots;
+    bp.child_first = rt->band ? static_cast<std::uint32_t>(rt->band_row_first * rt->grid_column_count) : 0u;
     bp.pairs = rt->pairs;
     bp.child_count = static_cast<std::uint32_t>(next_size);
     bp.action_count = static_cast<std::uint32_t>(rt->action_count);
@@ -1493,6 +1573,9 @@ int nwg_assemble_prepared(nwg_runtime *rt) {
     if (!rt->prepared) {
         return SetHostStatus(rt, kInvalidAssemblyPlan);
     }
+    if (rt->band && !rt->band_halo_ready) {
+        return SetHostStatus(rt, kInvalidAssemblyPlan);  // the halo rows of this generation are not installed
+    }
     rt->prepared = false;
     const std::uint32_t generation_seed = rt->prepared_seed;
     const nwg_generation_assembly_config cfg = rt->prepared_config;
@@ -1537,6 +1620,9 @@ int nwg_advance_graphed(nwg_runtime *rt, uint32_t generation_seed, const nwg_run
     }
     if (pending != nullptr && pending->enabled) {
         return nwg_advance(rt, generation_seed, counts, config, pending, nullptr, nullptr, nullptr, nullptr, nullptr);
+    }
+    if (rt->band) {
+        return kUnsupported;
     }
     if (rt->breed_begin == nullptr) {
         NWG_TRY(cudaEventCreate(&rt->breed_begin));
@@ -1702,6 +1788,7 @@ int nwg_swap_generations(nwg_runtime *rt) {
     std::swap(rt->cur_gen_size, rt->next_gen_size);
     rt->prepared = false;
     rt->released_parents = false;
+    rt->band_halo_ready = false;
     return kOk;
 }
 
@@ -1818,6 +1905,7 @@ int nwg_upload_current_generation(nwg_runtime *rt, const uint32_t *slot_indices,
     rt->cur_gen_index = generation_index;
     rt->prepared = false;
     rt->released_parents = false;
+    rt->band_halo_ready = false;
     return kOk;
 }
 
@@ -1842,6 +1930,157 @@ int nwg_device_slab(const nwg_runtime *rt, void **slab_out, size_t *pitch_out) {
     }
     *slab_out = rt->slab;
     *pitch_out = rt->pitch;
+    return kOk;
+}
+
+int nwg_set_band(nwg_runtime *rt, size_t global_rows, size_t band_row_first, size_t halo_rows) {
+    if (rt == nullptr) {
+        return kInvalidRuntimeConfig;
+    }
+    if (global_rows == 0) {  // back to a whole population
+        rt->band = false;
+        rt->band_global_rows = rt->band_row_first = rt->band_halo_rows = rt->band_reserved_slots = 0;
+        rt->band_halo_ready = false;
+        return kOk;
+    }
+    const std::size_t cols = rt->grid_column_count;
+    const std::size_t band_rows = rt->max_generation_size / cols;
+    const std::size_t reserved = 2 * halo_rows * cols;
+    // the halo rows must be other rows than the band's (and than each other's), and the slab must hold the band's
+    // parents, its children and the halo
+    if (band_rows == 0 || halo_rows == 0 || band_row_first >= global_rows || global_rows < band_rows + 2 * halo_rows ||
+        global_rows * cols > 0xFFFFFFFFull || rt->slot_count < 2 * rt->max_generation_size + reserved) {
+        return kInvalidRuntimeConfig;
+    }
+    if (rt->band_parent_table == nullptr || rt->band_global_rows * cols < global_rows * cols) {
+        if (rt->band_parent_table != nullptr) {
+            cudaFree(rt->band_parent_table);
+            rt->band_parent_table = nullptr;
+        }
+        NWG_TRY(cudaMalloc(&rt->band_parent_table, global_rows * cols * sizeof(std::uint32_t)));
+    }
+    rt->band = true;
+    rt->band_global_rows = global_rows;
+    rt->band_row_first = band_row_first;
+    rt->band_halo_rows = halo_rows;
+    rt->band_reserved_slots = reserved;
+    rt->band_halo_ready = false;
+    rt->prepared = false;
+    return kOk;
+}
+
+int nwg_device_generation(const nwg_runtime *rt, void **fitness, void **has_fitness, size_t *count) {
+    if (rt == nullptr || fitness == nullptr || has_fitness == nullptr || count == nullptr) {
+        return kInvalidRuntimeConfig;
+    }
+    *fitness = rt->cur_fitness;
+    *has_fitness = rt->cur_has;
+    *count = rt->cur_gen_size;
+    return kOk;
+}
+
+int nwg_band_copy_rows(nwg_runtime *rt, size_t band_row, size_t rows, void *dst, size_t dst_pitch) {
+    if (rt == nullptr || dst == nullptr || rt->released_parents) {
+        return kInvalidRuntimeConfig;
+    }
+    const std::size_t cols = rt->grid_column_count;
+    const std::size_t bytes = (rt->stride + 15) / 16 * 16;
+    if (rows == 0 || (band_row + rows) * cols > rt->cur_gen_size || dst_pitch < bytes || dst_pitch % 16 != 0 ||
+        reinterpret_cast<std::uintptr_t>(dst) % 16 != 0) {
+        return kInvalidRuntimeConfig;
+    }
+    const std::uint32_t n = static_cast<std::uint32_t>(rows * cols);
+    GatherSlotsKernel<<<n < 1024 ? n : 1024, 256, 0, rt->stream>>>(rt->slab, rt->pitch, rt->cur_slots + band_row * cols,
+                                                                   static_cast<std::uint8_t *>(dst), dst_pitch, bytes,
+                                                                   n);
+    NWG_TRY(cudaGetLastError());
+    return Sync(rt);
+}
+
+int nwg_band_install_halo(nwg_runtime *rt, const void *above, const void *below, size_t src_pitch) {
+    if (rt == nullptr || !rt->band || above == nullptr || below == nullptr || src_pitch < rt->stride ||
+        rt->released_parents) {
+        return kInvalidRuntimeConfig;
+    }
+    const std::size_t cols = rt->grid_column_count;
+    const std::size_t band_rows = rt->cur_gen_size / cols;
+    const std::size_t halo_cells = rt->band_halo_rows * cols;
+    const std::size_t reserved_base = rt->slot_count - rt->band_reserved_slots;
+    if (band_rows * cols != rt->cur_gen_size || band_rows + 2 * rt->band_halo_rows > rt->band_global_rows) {
+        return kInvalidGeneration;
+    }
+    std::uint8_t *base = rt->slab + reserved_base * rt->pitch;
+    NWG_TRY(cudaMemcpy2DAsync(base, rt->pitch, above, src_pitch, rt->stride, halo_cells, cudaMemcpyDeviceToDevice,
+                              rt->stream));
+    NWG_TRY(cudaMemcpy2DAsync(base + halo_cells * rt->pitch, rt->pitch, below, src_pitch, rt->stride, halo_cells,
+                              cudaMemcpyDeviceToDevice, rt->stream));
+    const std::uint32_t cells = static_cast<std::uint32_t>(rt->band_global_rows * cols);
+    BandParentTableKernel<<<(cells + 255) / 256, 256, 0, rt->stream>>>(
+        rt->band_parent_table, static_cast<std::uint32_t>(rt->band_global_rows), static_cast<std::uint32_t>(cols),
+        static_cast<std::uint32_t>(rt->band_row_first), static_cast<std::uint32_t>(band_rows),
+        static_cast<std::uint32_t>(rt->band_halo_rows), rt->cur_slots, static_cast<std::uint32_t>(reserved_base));
+    NWG_TRY(cudaGetLastError());
+    const int st = Sync(rt);
+    rt->band_halo_ready = st == kOk;
+    return st;
+}
+
+int nwg_band_prepare(nwg_runtime *rt, uint32_t generation_seed, const nwg_generation_assembly_config *config,
+                     const float *fitness_all, const uint8_t *has_fitness_all) {
+    if (rt == nullptr || !rt->band || fitness_all == nullptr || has_fitness_all == nullptr) {
+        return kInvalidRuntimeConfig;
+    }
+    rt->prepared = false;
+    nwg_generation_assembly_config cfg{};
+    cfg.parent_selection.cellular_breeding_radius = 2;  // selection.hpp:13-18, spatial/grid.hpp:11
+    cfg.parent_selection.rank_exponent = 0.5f;
+    cfg.breeding = {0.02f, 0.01f, 0.005f};
+    cfg.mutation = {0.0001f, 0.02f, 0.0f};
+    if (config != nullptr) {
+        cfg = *config;
+    }
+    const auto in01 = [](float v) { return v >= 0.0f && v <= 1.0f; };
+    // the band's children reach rows up to the radius away: the halo must cover them (radius <= 2 keeps the
+    // Moore-list selection, which the halo bounds; the whole-grid scan above that is not split)
+    const bool valid = cfg.parent_selection.cellular_breeding_radius > 0 &&
+                       cfg.parent_selection.cellular_breeding_radius <= rt->band_halo_rows &&
+                       cfg.parent_selection.cellular_breeding_radius <= 2 &&
+                       cfg.parent_selection.rank_exponent >= 0.0f && cfg.parent_selection.rank_exponent <= 4.0f &&
+                       in01(cfg.breeding.crossover_temperature_level1) &&
+                       in01(cfg.breeding.crossover_temperature_level2) &&
+                       in01(cfg.breeding.crossover_temperature_level3) && in01(cfg.mutation.mutation_probability) &&
+                       cfg.mutation.mutation_sigma >= 0.0f &&
+                       in01(cfg.mutation.output_tail_row_scale_mutation_probability);
+    if (!valid) {
+        return SetHostStatus(rt, kInvalidAssemblyConfig);
+    }
+    if (rt->cur_gen_size == 0 || rt->cur_gen_size % rt->grid_column_count != 0 || rt->released_parents) {
+        return SetHostStatus(rt, kInvalidGeneration);
+    }
+    SelectParams sp{};
+    sp.fitness = fitness_all;
+    sp.has_fitness = has_fitness_all;
+    sp.rows = static_cast<std::uint32_t>(rt->band_global_rows);
+    sp.cols = static_cast<std::uint32_t>(rt->grid_column_count);
+    sp.child_count = static_cast<std::uint32_t>(rt->cur_gen_size);
+    sp.child_first = static_cast<std::uint32_t>(rt->band_row_first * rt->grid_column_count);
+    sp.generation_index = rt->cur_gen_index;
+    sp.radius = cfg.parent_selection.cellular_breeding_radius;
+    sp.rank_exponent = cfg.parent_selection.rank_exponent;
+    sp.planning_seed = generation_seed ^ 0xA341316Cu;  // slab_runtime.cu:1443
+    sp.pairs = rt->pairs;
+    sp.status = rt->status;
+    NWG_TRY(LaunchSelect(sp, rt->stream));
+    const int st = Sync(rt);
+    if (st != kOk) {
+        return st;
+    }
+    rt->planned_children = rt->cur_gen_size;
+    rt->prepared = true;
+    rt->prepared_seed = generation_seed;
+    rt->prepared_config = cfg;
+    rt->prepared_injection = nwg_pending_injection{};
+    rt->prepared_next_action_count = rt->action_count;
     return kOk;
 }
 

@@ -42,12 +42,19 @@ __global__ void EvalPrepareKernel(WordSource src, std::uint32_t population, std:
     const std::uint32_t end = min(population, begin + per);
     std::uint32_t sum = 0;
     for (std::uint32_t i = begin; i < end; ++i) {
-        const std::uint32_t w = CountWords(src, i);
+        std::uint32_t w = 0;
+        // explicit lists: a decreasing pair of offsets would read as a huge count; such a cell, an empty one and
+        // one longer than kMaxCellWords are refused and get no chunks, so no kernel reads past its list
+        const bool ordered = src.mode != 0 || src.cell_offsets[i + 1] >= src.cell_offsets[i];
+        if (ordered) {
+            w = CountWords(src, i);
+        }
+        if (!ordered || w == 0 || w > kMaxCellWords) {
+            SetStatus(status, kInvalidTrainingShard);
+            w = 0;
+        }
         local_words[i] = w;
         score_sum[i] = 0;
-        if (w == 0) {
-            SetStatus(status, kInvalidTrainingShard);
-        }
         sum += ChunksForWords(w);
     }
     partial[t] = sum;

@@ -1,11 +1,17 @@
 // Fitness evaluation for callers that cannot allocate device memory.
 //
-// Some callers cannot call cudaMalloc: code running while a stream is being captured into a CUDA graph
-// (an allocation would break the capture), embedders whose device memory is owned by another allocator
-// or pool, and processes that must keep a fixed device-memory footprint after start-up. They can hand
-// this entry point device buffers they already own; everything else the evaluation needs (the per-CTA
-// layer-1 accumulators, the per-cell word counts and chunk offsets, the catalog tables, the score sums
-// and the status word) lives in one fixed array of this file, g_noalloc_scratch.
+// Some callers cannot call cudaMalloc: embedders whose device memory is owned by another allocator or
+// pool (a second allocator would fragment it or exceed its accounting), and processes that must keep a
+// fixed device-memory footprint after start-up (an allocation in the middle of a run can fail or stall
+// the device). They can hand this entry point device buffers they already own; everything else the
+// evaluation needs (the per-CTA layer-1 accumulators, the per-cell word counts and chunk offsets, the
+// catalog tables, the score sums and the status word) lives in one fixed array of this file,
+// g_noalloc_scratch.
+//
+// The word lists are the caller's device buffers and are not read on the host: a cell whose offsets
+// decrease, or whose list is empty or longer than 2^20 words, is refused on the device
+// (NWG_INVALID_TRAINING_SHARD) and none of its words is read. The call ends with a read of the status
+// word and a synchronisation of the caller's stream.
 //
 // The array is a file-scope __device__ variable, so every GPU that loads the library holds it until
 // the process exits. Host code cannot use the symbol as a device address: on first use on each device
@@ -107,12 +113,12 @@ extern "C" int nwg_evaluate_noalloc(const void *slab, size_t slot_pitch, const u
                                     const uint32_t *cell_offsets, const uint32_t *cell_words, float *fitness,
                                     uint64_t *counters, void *cuda_stream) {
     if (slab == nullptr || slot_indices == nullptr || catalog_letters == nullptr || cell_offsets == nullptr ||
-        cell_words == nullptr || fitness == nullptr || grid_column_count == 0 ||
+        cell_words == nullptr || fitness == nullptr || grid_column_count == 0 || population == 0 ||
         population % grid_column_count != 0 || slot_pitch % 16 != 0 ||
         slot_pitch < GenomeStrideBytes(action_count) || action_count == 0 || action_count > catalog_count) {
         return kInvalidRuntimeConfig;
     }
-    if (population == 0 || population > kNoAllocMaxPopulation || catalog_count > kNoAllocMaxCatalog) {
+    if (population > kNoAllocMaxPopulation || catalog_count > kNoAllocMaxCatalog) {
         return kUnsupported;  // beyond the fixed scratch array
     }
     unsigned char *scratch = nullptr;

@@ -29,7 +29,7 @@ using namespace tcx;
 
 constexpr int kTileN = 128;                  // actions per MMA tile
 constexpr std::uint32_t kTmemColumns = 256;  // two 128-column FP32 accumulators
-constexpr std::uint32_t kWaitLimit = 1u << 26;
+constexpr std::uint32_t kDrainLimit = 1u << 22;  // polls of each wind-down wait after a failure
 constexpr int kTileBytes = kTileN * kPolicy * 2;  // 16 KB of 16-bit embeddings per tile
 constexpr int kMaxTasks = 2048;
 
@@ -52,6 +52,8 @@ static_assert((kOffKeys * 4) % 8 == 0, "64-bit keys need 8-byte alignment");
 struct TcState {
     std::uint64_t mbar_load[kStages];
     std::uint64_t mbar_mma[2];
+    std::uint64_t mbar_drain;            // wind-down after a failure: thread 0's MMAs have completed
+    unsigned int loads_issued[kStages];  // bulk copies issued on each stage barrier (one per phase)
     int task_count;
     int full_count;
     std::uint32_t tmem_base;
@@ -65,11 +67,17 @@ struct TcParams {
     float kappa;
     int fp16_operands;
     unsigned long long *tc_counters;  // [0] re-scored chunks, [1] games re-scored over every action
+    std::uint32_t wait_limit;         // polls of a bounded mbarrier wait before it gives up (NWG_TIMEOUT)
 };
 
+// Failure protocol: a wait that gives up (q.wait_limit polls, or earlier once another thread has recorded a failure)
+// marks its thread dead (`alive`) and the CTA failed; a dead thread issues nothing and no copy or MMA is issued once
+// the CTA has failed, so every barrier phase still gets exactly one copy or commit, and the kernel's wind-down waits
+// for the copies issued on each barrier (counted) and for thread 0's MMAs.
 template <bool kFp16>
 __device__ void ScoreTensorCores(const TcParams &q, ChunkState &cs, TcState &ts, const __half *gh, float *arena,
-                                 int t, std::uint32_t (&load_uses)[kStages], std::uint32_t (&mma_uses)[2]) {
+                                 int t, std::uint32_t (&load_uses)[kStages], std::uint32_t (&mma_uses)[2],
+                                 bool &alive) {
     const EvalParams &p = q.base;
     const int tid = threadIdx.x;
     const int warp = tid >> 5;
@@ -113,8 +121,31 @@ __device__ void ScoreTensorCores(const TcParams &q, ChunkState &cs, TcState &ts,
                                       : umma::InstrDescBf16(128, kTileN);
     const std::uint64_t a_desc0 = umma::SmemDescriptor(umma::SmemAddress(a_tile), 128, 1024);
     const std::uint32_t b_addr0 = umma::SmemAddress(b_tile);
+    auto failed_now = [&]() { return *reinterpret_cast<volatile int *>(&ts.failed) != 0; };
+    auto can_issue = [&]() { return alive && !failed_now(); };
+    auto wait_bar = [&](std::uint64_t *bar, std::uint32_t parity) -> bool {
+        if (alive && umma::MbarTest(bar, parity)) {
+            return true;
+        }
+        if (alive && !failed_now() && umma::MbarWaitOrStop(bar, parity, q.wait_limit, &ts.failed)) {
+            return true;
+        }
+        *reinterpret_cast<volatile int *>(&ts.failed) = 1;
+        alive = false;
+        return false;
+    };
+    auto issue_load = [&](int stage, int tile) {  // thread 0
+        if (can_issue()) {
+            BulkLoad(b_tile + stage * kTileBytes, embed + static_cast<std::size_t>(tile) * kTileBytes, kTileBytes,
+                     &ts.mbar_load[stage]);
+            atomicAdd(&ts.loads_issued[stage], 1u);
+        }
+    };
     // accumulator buffer: tile & 1; embedding stage: tile % kStages
     auto issue_mma = [&](int tile) {
+        if (!can_issue()) {
+            return;
+        }
         const int acc = tile & 1;
         const int stage = tile % kStages;
         const std::uint32_t d = ts.tmem_base + static_cast<std::uint32_t>(acc * kTileN);
@@ -126,21 +157,20 @@ __device__ void ScoreTensorCores(const TcParams &q, ChunkState &cs, TcState &ts,
         }
         umma::Commit(&ts.mbar_mma[acc]);
     };
-    auto wait_load = [&](int tile) {
+    auto wait_load = [&](int tile) -> bool {
         const int stage = tile % kStages;
-        if (!umma::MbarWait(&ts.mbar_load[stage], load_uses[stage] & 1u, kWaitLimit)) {
-            ts.failed = 1;
-        }
+        const bool ok = wait_bar(&ts.mbar_load[stage], load_uses[stage] & 1u);
         load_uses[stage] += 1;
+        return ok;
     };
     if (tid == 0) {
         for (int tile = 0; tile < kStages && tile < n_tiles; ++tile) {
-            BulkLoad(b_tile + tile * kTileBytes, embed + static_cast<std::size_t>(tile) * kTileBytes, kTileBytes,
-                     &ts.mbar_load[tile]);
+            issue_load(tile, tile);
         }
-        wait_load(0);
-        umma::FenceAfterSync();
-        issue_mma(0);
+        if (wait_load(0)) {
+            umma::FenceAfterSync();
+            issue_mma(0);
+        }
     }
 
     const int quadrant = warp & 3;
@@ -155,21 +185,16 @@ __device__ void ScoreTensorCores(const TcParams &q, ChunkState &cs, TcState &ts,
     }
     for (int tile = 0; tile < n_tiles; ++tile) {
         const int buf = tile & 1;
-        if (tid == 0 && tile + 1 < n_tiles) {
-            wait_load(tile + 1);
+        if (tid == 0 && tile + 1 < n_tiles && wait_load(tile + 1)) {
             umma::FenceAfterSync();
             issue_mma(tile + 1);
         }
-        if (!umma::MbarWait(&ts.mbar_mma[buf], mma_uses[buf] & 1u, kWaitLimit)) {
-            ts.failed = 1;
-        }
+        const bool mma_done = wait_bar(&ts.mbar_mma[buf], mma_uses[buf] & 1u);
         mma_uses[buf] += 1;
         umma::FenceAfterSync();
-        if (tid == 0 && tile + kStages < n_tiles) {
+        if (tid == 0 && tile + kStages < n_tiles && mma_done) {
             // tile's MMA has completed, so its embedding stage is free for tile + kStages
-            const int stage = tile % kStages;
-            BulkLoad(b_tile + stage * kTileBytes, embed + static_cast<std::size_t>(tile + kStages) * kTileBytes,
-                     kTileBytes, &ts.mbar_load[stage]);
+            issue_load(tile % kStages, tile + kStages);
         }
         const bool last = tile + 1 == n_tiles;
 #pragma unroll
@@ -349,6 +374,7 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTcKernel(const TcParams q
     unsigned long long episodes = 0;
     std::uint32_t load_uses[kStages] = {0, 0, 0};
     std::uint32_t mma_uses[2] = {0, 0};
+    bool alive = true;
     const std::uint32_t total_chunks = p.chunk_start[p.population];
 
     if (tid < 32) {
@@ -360,6 +386,10 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTcKernel(const TcParams q
         }
         for (int b = 0; b < 2; ++b) {
             umma::MbarInit(&ts.mbar_mma[b], 1);
+        }
+        umma::MbarInit(&ts.mbar_drain, 1);
+        for (int b = 0; b < kStages; ++b) {
+            ts.loads_issued[b] = 0;
         }
         ts.failed = 0;
     }
@@ -389,7 +419,7 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTcKernel(const TcParams q
                 encoded += tid == 0 ? static_cast<unsigned long long>(cs.active) : 0ull;
             }
             TrunkForward(p, cs, gh, arena, scratch, t, step, ind);
-            ScoreTensorCores<kFp16>(q, cs, ts, gh, arena, t, load_uses, mma_uses);
+            ScoreTensorCores<kFp16>(q, cs, ts, gh, arena, t, load_uses, mma_uses, alive);
             if (ts.failed) {
                 break;
             }
@@ -398,11 +428,19 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTcKernel(const TcParams q
         FinishChunk(p, cs, ind, episodes);
     }
     FlushCounters(p, decisions, encoded, episodes);
+    __syncthreads();
     if (tid == 0 && ts.failed) {
         SetStatus(p.status, kTimeout);
-        // let any tensor-core work still in flight finish before the columns are released (bounded)
-        (void)umma::MbarWait(&ts.mbar_mma[0], mma_uses[0] & 1u, 1u << 20);
-        (void)umma::MbarWait(&ts.mbar_mma[1], mma_uses[1] & 1u, 1u << 20);
+        // thread 0's MMAs (a commit tracks all of its earlier tensor-core operations), then the last copy issued on
+        // each stage barrier (the n-th copy completes phase n - 1), before the columns and the CTA are released
+        umma::Commit(&ts.mbar_drain);
+        (void)umma::MbarWait(&ts.mbar_drain, 0, kDrainLimit);
+        for (int b = 0; b < kStages; ++b) {
+            const unsigned int n = ts.loads_issued[b];
+            if (n != 0) {
+                (void)umma::MbarWait(&ts.mbar_load[b], (n - 1u) & 1u, kDrainLimit);
+            }
+        }
     }
     umma::FenceBeforeSync();
     __syncthreads();
@@ -541,7 +579,8 @@ cudaError_t LaunchBuildTcTables(const std::uint8_t *slab, std::size_t pitch, con
 }
 
 cudaError_t LaunchEvalTc(const EvalParams &params, const std::uint8_t *tables, std::size_t table_pitch, float kappa,
-                         bool fp16, unsigned long long *tc_counters, int cta_count, cudaStream_t stream) {
+                         bool fp16, unsigned long long *tc_counters, int cta_count, cudaStream_t stream,
+                         std::uint32_t wait_limit) {
     const int arena_bytes = kArenaFloats * static_cast<int>(sizeof(float));
     static std::atomic<unsigned long long> configured[2]{{0}, {0}};
     if (const cudaError_t e = fp16 ? RaiseSharedLimit(EvalTcKernel<true>, arena_bytes, configured[1])
@@ -559,6 +598,7 @@ cudaError_t LaunchEvalTc(const EvalParams &params, const std::uint8_t *tables, s
     q.kappa = kappa;
     q.fp16_operands = fp16 ? 1 : 0;
     q.tc_counters = tc_counters;
+    q.wait_limit = wait_limit;
     if (fp16) {
         EvalTcKernel<true><<<cta_count, kEvalThreads, arena_bytes, stream>>>(q);
     } else {

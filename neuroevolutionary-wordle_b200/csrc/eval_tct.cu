@@ -40,7 +40,7 @@ constexpr int kSmemBytes = kPages * kPageBytes;
 constexpr int kTileN = 128;
 constexpr int kEmbedStages = 5;  // scoring stages live in pages 1..5
 constexpr std::uint32_t kTmemColumns = 256;
-constexpr std::uint32_t kWaitLimit = 1u << 26;
+constexpr std::uint32_t kDrainLimit = 1u << 22;  // polls of each wind-down wait after a failure
 constexpr int kKe1 = 160;  // encoder input features (145) padded to a multiple of 16
 constexpr int kFallbackBatch = 8;
 
@@ -104,8 +104,10 @@ struct TctState {
     std::uint64_t bar_free[2];       // trunk operand stages released by completed MMAs
     std::uint64_t bar_mma;           // a trunk phase's MMAs have completed
     std::uint64_t bar_acc[2];        // scoring accumulator buffers: MMAs completed
-    std::uint64_t bar_drain;
+    std::uint64_t bar_drain[kEvalThreads / 32];  // wind-down after a failure: each warp's MMAs have completed
     std::uint64_t bar_ring[kRing];   // exact-path weight tiles (FP16 form)
+    unsigned int loads_issued[kPages];  // bulk copies issued on each page barrier (one per phase)
+    unsigned int ring_issued[kRing];
     std::uint32_t tmem_base;
     int failed;
     int n_fallback;
@@ -132,6 +134,7 @@ struct TctParams {
     std::size_t trunk_pitch;
     float tau;
     unsigned long long *counters;  // [0] candidate chunks, [1] fallback steps, [2] exact chunks, [3] exact rows
+    std::uint32_t wait_limit;      // polls of a bounded mbarrier wait before it gives up (NWG_TIMEOUT)
 };
 
 template <bool kFp16>
@@ -311,11 +314,9 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
     unsigned long long decisions = 0, encoded = 0, episodes = 0;
     unsigned long long cand_chunks = 0, fallback_steps = 0, exact_chunks = 0, exact_rows = 0;
     // Barrier bookkeeping as one bit per barrier in registers (each barrier has at most one copy or commit
-    // outstanding): the parity of the next wait, and for the copies whether one is in flight.
-    // thread 0 only: page loads, their flight bits, exact-path ring tiles in flight, stage commits mod 2
+    // outstanding): the parity of the next wait.
+    // thread 0 only: page loads, stage commits mod 2
     std::uint32_t load_phase = 0;
-    std::uint32_t load_pending = 0;
-    std::uint32_t ring_pending = 0;
     std::uint32_t free_parity = 0;
     // every thread: ring waits, phase commits, accumulator waits
     std::uint32_t ring_phase = 0;
@@ -341,9 +342,15 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
         umma::MbarInit(&ts.bar_acc[1], 1);
         ts.readers[0] = 0;
         ts.readers[1] = 0;
-        umma::MbarInit(&ts.bar_drain, 1);
+        for (int w = 0; w < kEvalThreads / 32; ++w) {
+            umma::MbarInit(&ts.bar_drain[w], 1);
+        }
         for (int b = 0; b < kRing; ++b) {
             umma::MbarInit(&ts.bar_ring[b], 1);
+            ts.ring_issued[b] = 0;
+        }
+        for (int b = 0; b < kPages; ++b) {
+            ts.loads_issued[b] = 0;
         }
         ts.failed = 0;
     }
@@ -352,33 +359,50 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
     umma::FenceAfterSync();
     const std::uint32_t tmem = ts.tmem_base;
 
-    auto wait_bar = [&](std::uint64_t *bar, std::uint32_t parity) {
+    // Failure protocol. A wait that gives up (q.wait_limit polls, or earlier once another thread has recorded a
+    // failure) marks its thread dead and the CTA failed. From then on the thread issues nothing, and no thread issues
+    // anything once it sees the CTA failed: every copy or MMA that is issued follows successful waits of its own
+    // thread, so each barrier phase still gets exactly one copy or commit. Threads keep their uniform control flow
+    // (results are discarded) until the chunk's next uniform check; the wind-down then waits for the copies issued
+    // on each barrier (counted) and for every warp's MMAs before tensor memory is released.
+    bool alive = true;
+    auto failed_now = [&]() { return *reinterpret_cast<volatile int *>(&ts.failed) != 0; };
+    auto can_issue = [&]() { return alive && !failed_now(); };
+    auto wait_bar = [&](std::uint64_t *bar, std::uint32_t parity) -> bool {
         // a completed phase is taken at once; the failure flag is read only for a phase still open
-        if (umma::MbarTest(bar, parity) || *reinterpret_cast<volatile int *>(&ts.failed) != 0) {
-            return;
+        if (alive && umma::MbarTest(bar, parity)) {
+            return true;
         }
-        if (!umma::MbarWait(bar, parity, kWaitLimit)) {
-            ts.failed = 1;
+        if (alive && !failed_now() && umma::MbarWaitOrStop(bar, parity, q.wait_limit, &ts.failed)) {
+            return true;
+        }
+        *reinterpret_cast<volatile int *>(&ts.failed) = 1;
+        alive = false;
+        return false;
+    };
+    auto issue_load = [&](int b, void *dst, const void *src, std::uint32_t bytes) {  // any issuing thread
+        if (can_issue()) {
+            BulkLoad(dst, src, bytes, &ts.bar_load[b]);
+            atomicAdd(&ts.loads_issued[b], 1u);
         }
     };
     // thread 0 only
-    auto load = [&](int b, void *dst, const void *src, std::uint32_t bytes) {
-        BulkLoad(dst, src, bytes, &ts.bar_load[b]);
-        load_pending |= 1u << b;
-    };
-    auto wait_load = [&](int b) {
-        wait_bar(&ts.bar_load[b], (load_phase >> b) & 1u);
+    auto load = [&](int b, void *dst, const void *src, std::uint32_t bytes) { issue_load(b, dst, src, bytes); };
+    auto wait_load = [&](int b) -> bool {
+        const bool ok = wait_bar(&ts.bar_load[b], (load_phase >> b) & 1u);
         load_phase ^= 1u << b;
-        load_pending &= ~(1u << b);
+        return ok;
     };
     auto commit_free = [&](int s) {
-        umma::Commit(&ts.bar_free[s]);
+        if (can_issue()) {
+            umma::Commit(&ts.bar_free[s]);
+        }
         free_parity ^= 1u << s;
     };
-    auto wait_free = [&](int s) { wait_bar(&ts.bar_free[s], ((free_parity >> s) & 1u) ^ 1u); };
+    auto wait_free = [&](int s) { return wait_bar(&ts.bar_free[s], ((free_parity >> s) & 1u) ^ 1u); };
     // every thread (uniform control flow)
     auto commit_mma = [&]() {
-        if (tid == 0) {
+        if (tid == 0 && can_issue()) {
             umma::Commit(&ts.bar_mma);
         }
         ++mma_commits;
@@ -458,8 +482,7 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
                 *reinterpret_cast<std::uint16_t *>(onehot + umma::TileOffset(g, feature, kKe1)) = One16<kFp16>();
             }
             phase_sync();
-            if (tid == 0) {
-                wait_load(2);
+            if (tid == 0 && wait_load(2) && can_issue()) {
                 umma::FenceAfterSync();
                 MmaK(tmem, onehot, kKe1, we1, kKe1, kKe1 / 16, idesc128, false);
             }
@@ -480,8 +503,7 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
                 }
             }
             phase_sync();
-            if (tid == 0) {
-                wait_load(5);
+            if (tid == 0 && wait_load(5) && can_issue()) {
                 umma::FenceAfterSync();
                 MmaK(tmem + 128, a_h, kEncoderHidden, page(5), kEncoderHidden, kEncoderHidden / 16, idesc64, false);
             }
@@ -554,13 +576,15 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
                         const int st = i & 1;
                         const int enc_b = st == 0 ? 2 : 5;
                         const int w_b = st == 0 ? 3 : 0;
-                        wait_load(w_b);
+                        bool ok = wait_load(w_b);
                         if (i > 0) {
-                            wait_load(enc_b);
+                            ok = wait_load(enc_b) && ok;
                         }
-                        umma::FenceAfterSync();
-                        MmaK(tmem, page(enc_b), kEncoderOut, page(w_b), kEncoderOut, kEncoderOut / 16, idesc256,
-                             i > 0);
+                        if (ok && can_issue()) {
+                            umma::FenceAfterSync();
+                            MmaK(tmem, page(enc_b), kEncoderOut, page(w_b), kEncoderOut, kEncoderOut / 16, idesc256,
+                                 i > 0);
+                        }
                         commit_free(st);
                         if (i + 2 < t) {
                             wait_free(st);
@@ -592,7 +616,9 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
             // layer 2: A (h0) from tensor memory, 16 K-steps per half of the outputs
             if (tid == 0) {
                 for (int kc = 0; kc < 4; ++kc) {
-                    wait_load(kc);
+                    if (!wait_load(kc) || !can_issue()) {
+                        continue;
+                    }
                     umma::FenceAfterSync();
                     const std::uint32_t b_addr = umma::SmemAddress(page(kc));
 #pragma unroll
@@ -636,8 +662,7 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
             }
             phase_sync();
             // layer 3
-            if (tid == 0) {
-                wait_load(4);
+            if (tid == 0 && wait_load(4) && can_issue()) {
                 umma::FenceAfterSync();
                 MmaK(tmem + 128, page(0), kHidden1, page(4), kHidden1, kHidden1 / 16, idesc64, false);
             }
@@ -706,11 +731,12 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
             auto issue = [&](int tile) {  // one thread
                 const int acc = tile & 1;
                 const int b = 1 + tile % kEmbedStages;
-                wait_bar(&ts.bar_load[b], (load_phase >> b) & 1u);
-                umma::FenceAfterSync();
-                MmaK(tmem + static_cast<std::uint32_t>(acc * kTileN), a_tile, kPolicy, page(b), kPolicy, kPolicy / 16,
-                     idesc128, false);
-                umma::Commit(&ts.bar_acc[acc]);
+                if (wait_bar(&ts.bar_load[b], (load_phase >> b) & 1u) && can_issue()) {
+                    umma::FenceAfterSync();
+                    MmaK(tmem + static_cast<std::uint32_t>(acc * kTileN), a_tile, kPolicy, page(b), kPolicy,
+                         kPolicy / 16, idesc128, false);
+                    umma::Commit(&ts.bar_acc[acc]);
+                }
             };
             for (int k = 0; k < 2 && k < n_tiles; ++k) {
                 if (tid == 0) {
@@ -760,8 +786,8 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
                     if ((prior & 7u) == 7u) {  // every warp has read tile's buffer
                         if (tile + kEmbedStages < n_tiles) {
                             const int b = 1 + tile % kEmbedStages;  // tile's MMAs have completed: its stage is free
-                            BulkLoad(page(b), embed + static_cast<std::size_t>(tile + kEmbedStages) * kPageBytes,
-                                     kPageBytes, &ts.bar_load[b]);
+                            issue_load(b, page(b), embed + static_cast<std::size_t>(tile + kEmbedStages) * kPageBytes,
+                                       kPageBytes);
                         }
                         if (tile + 2 < n_tiles) {
                             issue(tile + 2);
@@ -772,8 +798,6 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
                     load_phase ^= 1u << (1 + (tile + 2) % kEmbedStages);
                 }
             }
-            // every embedding tile has been waited for
-            load_pending &= ~(((1u << kEmbedStages) - 1u) << 1);
             float *cand_v = reinterpret_cast<float *>(smem + kOffCandV);
             int *cand_id = reinterpret_cast<int *>(smem + kOffCandId);
 #pragma unroll
@@ -1055,8 +1079,10 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
                     } else {
                         off = kTblW3;
                     }
-                    BulkLoad(buffer(i), ttab + off, bytes, &ts.bar_ring[i % kRing]);
-                    ring_pending |= 1u << (i % kRing);
+                    if (can_issue()) {
+                        BulkLoad(buffer(i), ttab + off, bytes, &ts.bar_ring[i % kRing]);
+                        atomicAdd(&ts.ring_issued[i % kRing], 1u);
+                    }
                 };
                 if (tid == 0) {
                     umma::FenceProxyAsyncShared();
@@ -1131,7 +1157,6 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
                     const int b = i % kRing;
                     wait_bar(&ts.bar_ring[b], (ring_phase >> b) & 1u);
                     ring_phase ^= 1u << b;
-                    ring_pending &= ~(1u << b);
                     const std::uint8_t *w = buffer(i);
                     if (i < enc_tiles && i < 3) {
                         // encoder hidden rows of this group: EncodeRound's gather chain, ascending feature order
@@ -1608,6 +1633,9 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
             decide(t);
             if (ts.n_fallback > 0) {
                 exact_fallback(t, step);
+                if (__syncthreads_or(failed_now())) {  // a ring wait gave up: no guess from this step
+                    break;
+                }
             }
             AppendGuesses(p, cs, step, decisions);
         }
@@ -1621,19 +1649,28 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
         atomicAdd(q.counters + 3, exact_rows);
     }
     __syncthreads();
-    if (tid == 0 && ts.failed) {
-        SetStatus(p.status, kTimeout);
-        // let tensor-core work and bulk copies still in flight finish before the CTA releases its resources
-        umma::Commit(&ts.bar_drain);
-        (void)umma::MbarWait(&ts.bar_drain, 0, 1u << 22);
-        for (int b = 0; b < kPages; ++b) {
-            if ((load_pending >> b) & 1u) {
-                (void)umma::MbarWait(&ts.bar_load[b], (load_phase >> b) & 1u, 1u << 22);
-            }
+    if (ts.failed) {  // read after the barrier: uniform
+        if (tid == 0) {
+            SetStatus(p.status, kTimeout);
         }
-        for (int b = 0; b < kRing; ++b) {
-            if ((ring_pending >> b) & 1u) {
-                (void)umma::MbarWait(&ts.bar_ring[b], (ring_phase >> b) & 1u, 1u << 22);
+        // every warp's MMAs (a commit tracks all of its thread's earlier tensor-core operations; lane 0 of each warp
+        // is the only issuer in it), then the last copy issued on each barrier (the n-th copy completes phase n - 1)
+        if (lane == 0) {
+            umma::Commit(&ts.bar_drain[warp]);
+            (void)umma::MbarWait(&ts.bar_drain[warp], 0, kDrainLimit);
+        }
+        if (tid == 0) {
+            for (int b = 0; b < kPages; ++b) {
+                const unsigned int n = ts.loads_issued[b];
+                if (n != 0) {
+                    (void)umma::MbarWait(&ts.bar_load[b], (n - 1u) & 1u, kDrainLimit);
+                }
+            }
+            for (int b = 0; b < kRing; ++b) {
+                const unsigned int n = ts.ring_issued[b];
+                if (n != 0) {
+                    (void)umma::MbarWait(&ts.bar_ring[b], (n - 1u) & 1u, kDrainLimit);
+                }
             }
         }
     }
@@ -1702,7 +1739,7 @@ cudaError_t LaunchBuildTrunkTables(const std::uint8_t *slab, std::size_t pitch, 
 
 cudaError_t LaunchEvalTct(const EvalParams &params, const std::uint8_t *embed_tables, std::size_t embed_pitch,
                           const std::uint8_t *trunk_tables, float tau, bool fp16, unsigned long long *counters,
-                          int cta_count, cudaStream_t stream) {
+                          int cta_count, cudaStream_t stream, std::uint32_t wait_limit) {
     static std::atomic<unsigned long long> configured[2]{{0}, {0}};
     if (const cudaError_t e = fp16 ? RaiseSharedLimit(EvalTctKernel<true>, kSmemBytes, configured[1])
                                    : RaiseSharedLimit(EvalTctKernel<false>, kSmemBytes, configured[0]);
@@ -1720,6 +1757,7 @@ cudaError_t LaunchEvalTct(const EvalParams &params, const std::uint8_t *embed_ta
     q.trunk_pitch = kTrunkTableBytes;
     q.tau = tau;
     q.counters = counters;
+    q.wait_limit = wait_limit;
     if (fp16) {
         EvalTctKernel<true><<<cta_count, kEvalThreads, kSmemBytes, stream>>>(q);
     } else {

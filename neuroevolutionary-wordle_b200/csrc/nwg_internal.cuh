@@ -55,6 +55,8 @@ struct WordSource {
 // ---- fitness evaluation (plain FP32 form) ----
 constexpr int kEvalThreads = 256;
 constexpr int kChunkGames = 128;
+// Longest word list a cell may have (2^20 words: three chunk counts per cell stay far from 32-bit overflow).
+constexpr std::uint32_t kMaxCellWords = 1u << 20;
 
 struct EvalParams {
     const std::uint8_t *slab;
@@ -97,8 +99,11 @@ std::size_t TcTablePitch(std::uint32_t action_count);
 cudaError_t LaunchBuildTcTables(const std::uint8_t *slab, std::size_t pitch, const std::uint32_t *slots,
                                 std::uint32_t population, const float *fixed_t, std::uint32_t action_pad,
                                 std::uint32_t action_count, std::uint8_t *tables, bool fp16, cudaStream_t stream);
+// Polls of a bounded mbarrier wait in the tensor-core evaluation kernels before it gives up with NWG_TIMEOUT.
+constexpr std::uint32_t kDefaultWaitLimit = 1u << 26;
 cudaError_t LaunchEvalTc(const EvalParams &params, const std::uint8_t *tables, std::size_t table_pitch, float kappa,
-                         bool fp16, unsigned long long *tc_counters, int cta_count, cudaStream_t stream);
+                         bool fp16, unsigned long long *tc_counters, int cta_count, cudaStream_t stream,
+                         std::uint32_t wait_limit = kDefaultWaitLimit);
 
 // ---- fitness evaluation, tensor-core trunk form ----
 std::size_t TrunkTablePitch();
@@ -106,7 +111,7 @@ cudaError_t LaunchBuildTrunkTables(const std::uint8_t *slab, std::size_t pitch, 
                                    std::uint32_t population, std::uint8_t *tables, bool fp16, cudaStream_t stream);
 cudaError_t LaunchEvalTct(const EvalParams &params, const std::uint8_t *embed_tables, std::size_t embed_pitch,
                           const std::uint8_t *trunk_tables, float tau, bool fp16, unsigned long long *counters,
-                          int cta_count, cudaStream_t stream);
+                          int cta_count, cudaStream_t stream, std::uint32_t wait_limit = kDefaultWaitLimit);
 
 struct SummaryDevice {
     float best_fitness;
@@ -134,6 +139,7 @@ struct SelectParams {
     std::uint32_t planning_seed;
     std::uint32_t *pairs;  // [child_count * 2]
     int *status;
+    std::uint32_t child_first;  // global index of child 0 (a band of a larger grid; 0 for a whole population)
 };
 cudaError_t LaunchSelect(const SelectParams &params, cudaStream_t stream);
 
@@ -153,6 +159,7 @@ struct BreedParams {
     float crossover_l1, crossover_l2, crossover_l3;
     float mutation_probability, mutation_sigma, row_scale_probability;
     int *status;
+    std::uint32_t child_first;  // global index of child 0: its Philox subsequence (0 for a whole population)
 };
 cudaError_t LaunchBreed(const BreedParams &params, cudaStream_t stream, int warps_per_cta = 8);
 
@@ -164,9 +171,12 @@ cudaError_t LaunchInject(std::uint8_t *slab, std::size_t pitch, const std::uint3
                          int *status, cudaStream_t stream);
 
 // ---- bootstrap ----
+// Organism i is organism organism_first + i of a population of stream_population (0: population) in the
+// random-stream map.
 cudaError_t LaunchBootstrap(std::uint8_t *slab, std::size_t pitch, const std::uint32_t *slots,
                             std::uint32_t population, std::uint64_t generation_index, std::uint32_t seed,
-                            std::uint32_t action_count, cudaStream_t stream);
+                            std::uint32_t action_count, cudaStream_t stream, std::uint32_t organism_first = 0,
+                            std::uint32_t stream_population = 0);
 
 // ---- the pre-breeding boundary, for checkpoints (checkpoint.cu) ----
 

@@ -5,7 +5,9 @@
 // Philox stream is (seed ^ 0xA341316C, uint32(child + generation * 8191)) and is consumed in the same
 // order (two 32-bit outputs for the tie-break seed, one uniform for the threshold, per parent). The
 // neighbourhood is the deduplicated Moore list for radius <= 2 (spatial/grid.hpp:181-218) and every cell
-// within the toroidal Chebyshev radius, in index order, above that (selection_ops.cuh:163-216).
+// within the toroidal Chebyshev radius, in index order, above that (selection_ops.cuh:163-216). A row band of a
+// larger grid selects for its own children only (child_first = the band's first cell), over the whole grid's
+// fitness, with the same streams as a single-population run.
 #include <curand_kernel.h>
 
 #include "nwg_internal.cuh"
@@ -154,10 +156,11 @@ __device__ bool SelectFromRadius(const float *f, const std::uint8_t *has, std::u
 }
 
 __global__ void SelectKernel(const SelectParams p) {
-    const std::uint32_t child = blockIdx.x * blockDim.x + threadIdx.x;
-    if (child >= p.child_count) {
+    const std::uint32_t local = blockIdx.x * blockDim.x + threadIdx.x;
+    if (local >= p.child_count) {
         return;
     }
+    const std::uint32_t child = p.child_first + local;  // the child's index in the whole grid
     const std::uint64_t rows = p.rows;
     const std::uint64_t cols = p.cols;
     // the child keeps its (row, column) in the current grid (selection_ops.cuh:233-235)
@@ -203,8 +206,8 @@ __global__ void SelectKernel(const SelectParams p) {
         SetStatus(p.status, kParentSelectionFailed);
         return;
     }
-    p.pairs[2 * child] = static_cast<std::uint32_t>(first);
-    p.pairs[2 * child + 1] = static_cast<std::uint32_t>(second);
+    p.pairs[2 * local] = static_cast<std::uint32_t>(first);
+    p.pairs[2 * local + 1] = static_cast<std::uint32_t>(second);
 }
 
 }  // namespace

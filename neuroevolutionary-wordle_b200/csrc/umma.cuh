@@ -107,6 +107,32 @@ __device__ __forceinline__ bool MbarTest(std::uint64_t *mbar, std::uint32_t pari
     return done != 0;
 }
 
+// Waits for the mbarrier phase with the given parity; gives up after `limit` polls, or as soon as another thread
+// of the CTA has recorded a failure in *failed (checked every 16 polls), and returns false.
+__device__ __forceinline__ bool MbarWaitOrStop(std::uint64_t *mbar, std::uint32_t parity, std::uint32_t limit,
+                                               const int *failed) {
+    if (MbarTest(mbar, parity)) {
+        return true;
+    }
+    const std::uint32_t addr = SmemAddress(mbar);
+    for (std::uint32_t i = 0; i < limit; ++i) {
+        if ((i & 15u) == 0u && *reinterpret_cast<const volatile int *>(failed) != 0) {
+            return false;
+        }
+        std::uint32_t done = 0;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(addr), "r"(parity)
+            : "memory");
+        if (done) {
+            return true;
+        }
+    }
+    return false;
+}
+
 // Waits for the mbarrier phase with the given parity; gives up after `limit` polls and returns false.
 // A phase that has completed already is seen by the non-blocking test_wait; the potentially blocking try_wait
 // took hundreds of cycles to report such a phase on B200, so it is used only while the phase is still open.

@@ -293,6 +293,8 @@ def ref_ckpt() -> C.CDLL | None:
                                           C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_char_p]
     L.refckpt_runtime_evaluate.argtypes = [C.c_void_p, C.c_void_p, _sz, _sz, C.c_uint32, _sz, C.c_void_p, C.c_void_p,
                                            C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.refckpt_time_evaluation.argtypes = [C.c_void_p, C.c_void_p, _sz, _sz, C.c_uint32, _sz, C.c_void_p, _sz,
+                                          C.c_void_p, C.c_void_p]
     L.refart_write.argtypes = [C.c_char_p, C.c_char_p, C.c_void_p, C.c_void_p, _sz, C.c_void_p, C.c_char_p]
     L.refart_read.argtypes = [C.c_char_p, C.c_char_p, C.c_void_p, C.c_void_p, _sz, C.c_void_p, C.POINTER(_sz),
                               C.c_char_p, _sz]
@@ -352,6 +354,8 @@ def ref_dev() -> C.CDLL | None:
     L.refdev_upload_catalog.argtypes = [_u8p, _sz]
     L.refdev_evaluate.argtypes = [C.c_void_p, _sz, _sz, _sz, _sz, C.c_void_p, _sz, _sz, C.c_void_p, C.c_void_p,
                                   C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.refdev_evaluate_csr.argtypes = [C.c_void_p, _sz, C.c_void_p, _sz, _sz, C.c_void_p, C.c_void_p, _sz,
+                                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     L.refdev_select.argtypes = [C.c_void_p, C.c_void_p, _sz, _sz, _sz, _sz, _sz, C.c_float, C.c_uint32, C.c_void_p,
                                 C.c_void_p, C.c_void_p]
     L.refdev_breed.argtypes = [C.c_void_p, _sz, C.c_void_p, _sz, C.c_void_p, _sz, _sz, C.c_uint32, _sz, C.c_float,

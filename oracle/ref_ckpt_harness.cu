@@ -15,6 +15,7 @@
 // Device entry points (drive the reference's whole runtime on the GPU):
 //   refckpt_runtime_capture create, bootstrap, TryCreatePrebreedingCheckpointOnDevice, write
 //   refckpt_runtime_evaluate create, bootstrap, TryEvaluateCurrentGenerationFitnessOnDevice, fitness arrays
+//   refckpt_time_evaluation create, bootstrap, TryEvaluateCurrentGenerationFitnessOnDevice timed per call
 //   refckpt_runtime_resume  read, TryRestorePrebreedingCheckpointToDevice, TryResumeGenerationFromCheckpointOnDevice,
 //                          then the new generation's genomes in individual order
 #include "genetic_algorithm/device/slab_runtime.cu"
@@ -26,6 +27,7 @@
 #include "genetic_algorithm/genetic_convergence.hpp"
 #include "inference/single_model_device_runtime.cu"
 
+#include <chrono>
 #include <cstring>
 #include <random>
 
@@ -377,6 +379,39 @@ int refckpt_runtime_evaluate(const void *config, const std::uint8_t *letters, st
     }
     if (ok) {
         std::memcpy(summary, &s, sizeof(s));
+    }
+    sd::DestroyDeviceSlabGARuntimeBuffers(buffers);
+    return ok ? 1 : 0;
+}
+
+// The reference's evaluation timed through its public API: create, bootstrap, then `repeats` calls of
+// TryEvaluateCurrentGenerationFitnessOnDevice (each synchronises the device before it returns), each timed on the
+// host clock around the call; ms_out[r] is call r's time, then the fitness of the last call.
+int refckpt_time_evaluation(const void *config, const std::uint8_t *letters, std::size_t catalog_count,
+                            std::size_t generation_size, std::uint32_t bootstrap_seed, std::size_t generation_index,
+                            const void *counts, std::size_t repeats, double *ms_out, float *fitness) {
+    tf::TrainingWordCatalog *catalog = new tf::TrainingWordCatalog{};
+    const bool have_catalog =
+        MakeCatalog(letters, catalog_count, *catalog) && tf::UploadTrainingWordCatalogToDeviceConstantMemory(*catalog);
+    delete catalog;
+    if (!have_catalog) {
+        return 0;
+    }
+    sd::DeviceSlabGARuntimeBuffers buffers{};
+    gs::SlabGeneration generation{};
+    bool ok = sd::TryCreateDeviceSlabGARuntimeBuffers(buffers, *static_cast<const sd::DeviceSlabGARuntimeConfig *>(config)) &&
+              sd::TryBootstrapRandomCurrentGenerationOnDevice(buffers, generation_size, bootstrap_seed, generation_index);
+    for (std::size_t r = 0; ok && r < repeats; ++r) {
+        const auto t0 = std::chrono::steady_clock::now();
+        ok = sd::TryEvaluateCurrentGenerationFitnessOnDevice(buffers, *static_cast<const sd::RuntimeWordCounts *>(counts),
+                                                             nullptr) &&
+             cudaDeviceSynchronize() == cudaSuccess;
+        const auto t1 = std::chrono::steady_clock::now();
+        ms_out[r] = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    }
+    ok = ok && sd::TryDownloadCurrentGenerationFromDevice(buffers, generation);
+    for (std::size_t i = 0; ok && i < generation.active_individual_count; ++i) {
+        fitness[i] = generation.fitness[i];
     }
     sd::DestroyDeviceSlabGARuntimeBuffers(buffers);
     return ok ? 1 : 0;

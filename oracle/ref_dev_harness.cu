@@ -7,6 +7,10 @@
 // reference's arithmetic and random streams bit for bit on the same B200:
 //   - refdev_evaluate:  slab_runtime.cu:452-549 (warp per episode) with the guesses
 //                       and policy vectors of every decision recorded;
+//   - refdev_evaluate_csr: the same episode loop over explicit per-individual word
+//                       lists (CSR); only the word lookup of TryInitializeEpisodeGrid
+//                       (evaluation_ops.cuh:203-237) is restated, everything the policy,
+//                       grid and score code does is the reference's own;
 //   - refdev_select:    slab_runtime.cu:633-675 (BuildSlabAssemblyPlanKernel body);
 //   - refdev_breed:     genotype_slab/device_runtime.cu:448-516 (breed + mutate body);
 //   - refdev_bootstrap: genotype_slab/device_runtime.cu:258-314 (initialisation body);
@@ -75,6 +79,98 @@ __global__ void EvaluateKernel(const std::uint8_t *slab, std::size_t pitch, std:
     if (s.status != 0) {
         if (lane == 0) {
             atomicCAS(status, 0, 100 + s.status);
+        }
+        return;
+    }
+    int step = 0;
+    while (!s.grid.IsFinished()) {
+        SelectedAction selected{};
+        const DynamicInferenceStatusCode st = SelectNextGuessFromDynamicGenomeConcurrently<32>(
+            s.grid, tf::DeviceTrainingWordCatalog(), genome, action_count, s.dynamic_policy, selected);
+        if (st != DynamicInferenceStatusCode::kOk) {
+            if (lane == 0) {
+                atomicCAS(status, 0, 200 + static_cast<int>(st));
+            }
+            return;
+        }
+        if (policy_trace != nullptr) {
+            for (int k = lane; k < 64; k += 32) {
+                policy_trace[(slot * 6 + step) * 64 + k] = s.dynamic_policy.model.policy_vector[k];
+            }
+        }
+        if (lane == 0) {
+            choices[slot * 6 + step] = static_cast<int>(selected.action_index);
+            s.status = neuroevolution::wordle::TryAppendGuess(s.grid, selected.word) ? 0 : 2;
+        }
+        __syncwarp();
+        if (s.status != 0) {
+            if (lane == 0) {
+                atomicCAS(status, 0, 300);
+            }
+            return;
+        }
+        ++step;
+    }
+    if (lane == 0) {
+        scores[slot] = ScoreCompletedEpisode(s.grid);
+        turns[slot] = static_cast<int>(s.grid.turn_count);
+    }
+}
+
+// evaluation_ops.cuh:171-237 with the shard walk replaced by a lookup in the individual's own word list:
+// secret = list[e / 3]; variant 1 prefills list[(e/3 + 1) % W], list[(e/3 + 2) % W]; variant 2 the words at
+// +3 and +4. The grid rules (MakeWordleGrid, TryAppendGuess) are the reference's.
+__device__ bool InitializeCsrEpisode(const std::uint32_t *list, std::size_t w, std::size_t episode,
+                                     neuroevolution::wordle::WordleGrid &grid) {
+    const tf::TrainingWordCatalog &catalog = tf::DeviceTrainingWordCatalog();
+    const std::size_t entry = episode / 3;
+    const std::size_t variant = episode % 3;
+    if (w == 0 || list[entry] >= catalog.word_count) {
+        return false;
+    }
+    grid = neuroevolution::wordle::MakeWordleGrid(catalog.words[list[entry]]);
+    if (variant == 0) {
+        return true;
+    }
+    const std::size_t first = variant == 1 ? entry + 1 : entry + 3;
+    const std::uint32_t a = list[first % w];
+    const std::uint32_t b = list[(first + 1) % w];
+    if (a >= catalog.word_count || b >= catalog.word_count) {
+        return false;
+    }
+    return neuroevolution::wordle::TryAppendGuess(grid, catalog.words[a]) &&
+           neuroevolution::wordle::TryAppendGuess(grid, catalog.words[b]);
+}
+
+// One warp per episode (slab_runtime.cu:452-549); individual i's genome at slab + slots[i] * pitch and its
+// words at cell_words[cell_offsets[i] .. cell_offsets[i + 1]).
+__global__ void EvaluateCsrKernel(const std::uint8_t *slab, std::size_t pitch, const std::uint32_t *slots,
+                                  std::size_t population, std::size_t action_count,
+                                  const std::uint32_t *cell_offsets, const std::uint32_t *cell_words,
+                                  std::size_t max_episodes, float *scores, int *turns, int *choices,
+                                  float *policy_trace, int *status) {
+    __shared__ GenomeEvaluationWarpScratch<32> scratch[kWarps];
+    const std::size_t individual = blockIdx.x;
+    const int warp = threadIdx.x / 32;
+    const int lane = threadIdx.x % 32;
+    const std::size_t episode = static_cast<std::size_t>(blockIdx.y) * kWarps + warp;
+    if (individual >= population) {
+        return;
+    }
+    const std::size_t w = cell_offsets[individual + 1] - cell_offsets[individual];
+    if (episode >= 3 * w || episode >= max_episodes) {
+        return;
+    }
+    const std::uint8_t *genome = slab + static_cast<std::size_t>(slots[individual]) * pitch;
+    const std::size_t slot = individual * max_episodes + episode;
+    auto &s = scratch[warp];
+    if (lane == 0) {
+        s.status = InitializeCsrEpisode(cell_words + cell_offsets[individual], w, episode, s.grid) ? 0 : 1;
+    }
+    __syncwarp();
+    if (s.status != 0) {
+        if (lane == 0) {
+            atomicCAS(status, 0, 101);
         }
         return;
     }
@@ -225,6 +321,24 @@ int refdev_evaluate(const void *slab, std::size_t pitch, std::size_t population,
                                                              cudaSuccess;
     cudaFree(shards);
     return ok ? 1 : 0;
+}
+
+// Explicit per-individual word lists; every pointer is a device pointer (policy_trace may be null).
+int refdev_evaluate_csr(const void *slab, std::size_t pitch, const std::uint32_t *slots, std::size_t population,
+                        std::size_t action_count, const std::uint32_t *cell_offsets, const std::uint32_t *cell_words,
+                        std::size_t max_episodes, float *scores, int *turns, int *choices, float *policy_trace,
+                        int *status, void *stream) {
+    if (population == 0 || max_episodes == 0) {
+        return 0;
+    }
+    dim3 grid(static_cast<unsigned>(population), static_cast<unsigned>((max_episodes + kWarps - 1) / kWarps));
+    EvaluateCsrKernel<<<grid, 32 * kWarps, 0, static_cast<cudaStream_t>(stream)>>>(
+        static_cast<const std::uint8_t *>(slab), pitch, slots, population, action_count, cell_offsets, cell_words,
+        max_episodes, scores, turns, choices, policy_trace, status);
+    return cudaGetLastError() == cudaSuccess &&
+                   cudaStreamSynchronize(static_cast<cudaStream_t>(stream)) == cudaSuccess
+               ? 1
+               : 0;
 }
 
 int refdev_select(const float *fitness, const std::uint8_t *has_fitness, std::size_t population,
