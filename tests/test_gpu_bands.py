@@ -48,7 +48,7 @@ def test_two_bands_equal_the_whole_population(rows, cols, radius, halo, form):
         b.rt.set_margin_guard(1e-3)
         b.bootstrap(9)
         b.set_cell_words(offsets, words)
-    assert all(np.array_equal(x, y) for x, y in zip(_images(whole), _images(parts[0]) + _images(parts[1])))
+    assert all(np.array_equal(x, y) for x, y in zip(_images(whole), _images(parts[0].rt) + _images(parts[1].rt)))
 
     for generation in range(3):
         seed = 500 + generation
@@ -76,7 +76,7 @@ def test_two_bands_equal_the_whole_population(rows, cols, radius, halo, form):
             b.rt.assemble()
         plan = np.concatenate([b.rt.assembly_plan() for b in parts])
         assert np.array_equal(plan, whole.assembly_plan()), f"generation {generation}: parent pairs differ"
-        got = _images(parts[0]) + _images(parts[1])
+        got = _images(parts[0].rt) + _images(parts[1].rt)
         for c, (x, y) in enumerate(zip(_images(whole), got)):
             assert np.array_equal(x, y), f"generation {generation}: child {c} differs"
     for b in parts:
