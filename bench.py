@@ -16,7 +16,10 @@ reported with their guess agreement against the plain form, "agreement_with_plai
 reference's own CUDA evaluation (compiled for sm_100a from its sources) on a 256-individual slice of the workload
 on the same GPU, beside this library's forms on the same slice.
 
-On the full workload at N=1 the line also carries "surrogate_vs_plain" (--no-surrogate skips it).
+On the full workload at N=1 the line also carries "batching_form", the widening run of the batching
+configuration (16,384 individuals on 128x128, uneven per-cell lists, the action space widened from 1,024 to 4,739
+words over 50 generations, graphed generations with tuned launch shapes, BF16 trunk form; --no-growth skips it),
+and "surrogate_vs_plain" (--no-surrogate skips it).
 
 --gpus N (N > 1) starts N ranks on this node (or runs under torch.distributed.run) and splits the one population
 into N row bands, one per GPU: evaluation per band, fitness all-gather, halo genome exchange with the neighbour
@@ -684,10 +687,18 @@ def run_ours(args) -> None:
     if not args.no_reference_gpu and args.workload == "full":
         ref_gpu = reference_gpu(nwg, torch, wl, catalog)
         nwg.capi.upload_catalog(catalog)
-    race = None
-    if not args.no_surrogate and args.workload == "full":
+    if rt is not None:
         rt.close()
         rt = None
+    batching = None
+    if not args.no_growth and args.workload == "full":
+        # config 3 names BF16 operands for the batching form
+        batching = growth_run(nwg, torch, "tc-trunk-bf16", args.tau, 0, local)
+        for k in ("total_steps", "total_s"):
+            batching.pop(k)
+        nwg.capi.upload_catalog(catalog)
+    race = None
+    if not args.no_surrogate and args.workload == "full":
         race = surrogate_vs_plain(nwg, wl, torch, args.surrogate_generations)
     line = {
         "metric": "game-steps/s",
@@ -724,6 +735,7 @@ def run_ours(args) -> None:
         "other_forms": others or None,
         "agreement_with_plain": agreement or None,
         "reference_gpu": ref_gpu,
+        "batching_form": batching,
         "surrogate_vs_plain": race,
         "clocks": agg["clocks"],
     }
@@ -732,19 +744,15 @@ def run_ours(args) -> None:
         rt.close()
 
 
-def run_growth(args) -> None:
-    """Batching form with uneven shards: 16,384 individuals on a 128x128 grid, per-cell secret lists of
-    floor(exp(U[ln 32, ln 1024])) words drawn from the first 1,024 catalog words, and the action space widened
-    from 1,024 to 4,739 words in steps of 512 (the last step 131) over 50 generations. Every generation that does
-    not widen runs as one CUDA graph with launch shapes tuned per width (nwg_advance_graphed); a widening
+def growth_run(nwg, torch, form: str, tau: float, rank: int = 0, local: int = 0) -> dict:
+    """Batching form with uneven shards (the widening run): 16,384 individuals on a 128x128 grid, per-cell secret
+    lists of floor(exp(U[ln 32, ln 1024])) words drawn from the first 1,024 catalog words, and the action space
+    widened from 1,024 to 4,739 words in steps of 512 (the last step 131) over 50 generations. Every generation that
+    does not widen runs as one CUDA graph with launch shapes tuned per width (nwg_advance_graphed); a widening
     generation breeds into the wider slab and injects the new rows directly. As in the reference, the generation
     byte budget is fixed at creation (16,384 genomes at 1,024 words), so each widening keeps the whole grid rows
     that still fit; the surviving cells keep their secret lists. Timed on the host with the device synchronised
-    around each generation; game steps are counted on the device."""
-    import torch
-
-    rank, world, local = dist_setup(args.gpus)
-    nwg = importlib.import_module("neuroevolutionary-wordle_b200")
+    around each generation; game steps are counted on the device. Returns this rank's totals and the line fields."""
     W, capi = nwg.workload, nwg.capi
     population, columns, start, final, step, generations = 16384, 128, 1024, 4739, 512, 50
     widths = list(range(start + step, final, step)) + [final]
@@ -761,9 +769,9 @@ def run_growth(args) -> None:
     offsets, words = W.loguniform_cell_lists(population, 32, 1024, subset, rank)
     rt = nwg.Runtime(start, population, columns, stream=torch.cuda.current_stream().cuda_stream)
     rt.set_cell_words(offsets, words)
-    rt.set_form(FORMS[args.form])
-    if args.form.startswith("tc-trunk"):
-        rt.set_margin_guard(args.tau)
+    rt.set_form(FORMS[form])
+    if form.startswith("tc-trunk"):
+        rt.set_margin_guard(tau)
     rt.bootstrap(population, seed=rank)
     cfg = capi.assembly_config(radius=1, p=0.05, sigma=0.02)
     width = start
@@ -797,25 +805,42 @@ def run_growth(args) -> None:
         tuning[w] = {"decided": bool(t.decided), "eval_ctas": t.eval_ctas, "breed_warps": t.breed_warps,
                      "eval_ms": [round(x, 3) for x in t.eval_ms], "breed_ms": [round(x, 3) for x in t.breed_ms]}
     gi = rt.graph_info()
-    value = sum_over_ranks(float(total_steps), world) / max_over_ranks(total_s, world)
+    final_population = len(rt.current_generation()["slots"])
+    rt.close()
+    return {
+        "total_steps": total_steps, "total_s": total_s, "generations": generations,
+        "value": total_steps / total_s, "unit": "game-steps/s", "generations_per_s": generations / total_s,
+        "ms_per_generation": 1e3 * total_s / generations, "dtype": DTYPES[form],
+        "config": {"workload": "p16384_grid128_a1024to4739_loguniform32to1024", "population": population,
+                   "grid": "128x128", "action_width": f"{start} -> {final} in steps of {step}",
+                   "widen_at_generation": widen_at, "secrets_per_cell": "floor(exp(U[ln 32, ln 1024]))",
+                   "secret_words": f"the first {start} catalog words", "form": FORM_NAMES[form],
+                   "margin_tau": tau if form.startswith("tc-trunk") else None,
+                   "timing": "host clock around each generation, device synchronised",
+                   "final_population": final_population, "final_width": width},
+        "per_width": {w: {**r, "game_steps_per_s": r["game_steps"] / r["seconds"]} for w, r in per_width.items()},
+        "launch_tuning": tuning,
+        "graphs": {"launches": gi.launches, "instantiations": gi.instantiations, "updates": gi.updates},
+        "clocks": clocks.summary(),
+    }
+
+
+def run_growth(args) -> None:
+    """The widening run alone (growth_run), one JSON line; every rank runs its own 16,384-individual grid."""
+    import torch
+
+    rank, world, local = dist_setup(args.gpus)
+    nwg = importlib.import_module("neuroevolutionary-wordle_b200")
+    r = growth_run(nwg, torch, args.form, args.tau, rank, local)
+    value = sum_over_ranks(float(r["total_steps"]), world) / max_over_ranks(r["total_s"], world)
     if rank == 0:
         print(json.dumps({
-            "metric": "game-steps/s", "value": value, "unit": "game-steps/s", "n_gpus": world, "steps": generations,
-            "warmup": 0, "ms_per_step": 1e3 * total_s / generations, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": DTYPES[args.form], "data": "synthetic", "impl": "ours",
-            "generations_per_s": generations / total_s,
-            "config": {"workload": "p16384_grid128_a1024to4739_loguniform32to1024", "population": population,
-                       "grid": "128x128", "action_width": f"{start} -> {final} in steps of {step}",
-                       "widen_at_generation": widen_at, "secrets_per_cell": "floor(exp(U[ln 32, ln 1024]))",
-                       "secret_words": f"the first {start} catalog words", "form": FORM_NAMES[args.form],
-                       "margin_tau": args.tau, "timing": "host clock around each generation, device synchronised",
-                       "final_population": len(rt.current_generation()["slots"]), "final_width": width},
-            "per_width": {w: {**r, "game_steps_per_s": r["game_steps"] / r["seconds"]} for w, r in per_width.items()},
-            "launch_tuning": tuning,
-            "graphs": {"launches": gi.launches, "instantiations": gi.instantiations, "updates": gi.updates},
-            "clocks": clocks.summary(),
+            "metric": "game-steps/s", "value": value, "unit": "game-steps/s", "n_gpus": world,
+            "steps": r["generations"], "warmup": 0, "ms_per_step": r["ms_per_generation"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": r["dtype"], "data": "synthetic", "impl": "ours",
+            "generations_per_s": r["generations_per_s"], "config": r["config"], "per_width": r["per_width"],
+            "launch_tuning": r["launch_tuning"], "graphs": r["graphs"], "clocks": r["clocks"],
         }), flush=True)
-    rt.close()
 
 
 def run_reference(args) -> None:
@@ -909,6 +934,8 @@ def main() -> None:
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="skip timing the reference's own CUDA evaluation on a slice of the workload")
     ap.add_argument("--surrogate-generations", type=int, default=50)
+    ap.add_argument("--no-growth", action="store_true",
+                    help="skip the widening run (16,384 individuals, 1,024 -> 4,739 words) in the full line")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

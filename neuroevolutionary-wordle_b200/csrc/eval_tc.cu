@@ -52,8 +52,9 @@ static_assert((kOffKeys * 4) % 8 == 0, "64-bit keys need 8-byte alignment");
 struct TcState {
     std::uint64_t mbar_load[kStages];
     std::uint64_t mbar_mma[2];
-    std::uint64_t mbar_drain;            // wind-down after a failure: thread 0's MMAs have completed
+    std::uint64_t mbar_drain[kEvalThreads / 32];  // wind-down after a failure: each warp's MMAs have completed
     unsigned int loads_issued[kStages];  // bulk copies issued on each stage barrier (one per phase)
+    std::uint32_t readers[2];            // warps that have read each accumulator buffer (8 per tile)
     int task_count;
     int full_count;
     std::uint32_t tmem_base;
@@ -75,9 +76,9 @@ struct TcParams {
 // the CTA has failed, so every barrier phase still gets exactly one copy or commit, and the kernel's wind-down waits
 // for the copies issued on each barrier (counted) and for thread 0's MMAs.
 template <bool kFp16>
-__device__ void ScoreTensorCores(const TcParams &q, ChunkState &cs, TcState &ts, const __half *gh, float *arena,
-                                 int t, std::uint32_t (&load_uses)[kStages], std::uint32_t (&mma_uses)[2],
-                                 bool &alive) {
+__device__ __forceinline__ void ScoreTensorCores(const TcParams &q, ChunkState &cs, TcState &ts, const __half *gh,
+                                                 float *arena, int t, std::uint32_t &load_phase,
+                                                 std::uint32_t &acc_phase, bool &alive) {
     const EvalParams &p = q.base;
     const int tid = threadIdx.x;
     const int warp = tid >> 5;
@@ -96,6 +97,62 @@ __device__ void ScoreTensorCores(const TcParams &q, ChunkState &cs, TcState &ts,
     const float *emax = reinterpret_cast<const float *>(table);
     const std::uint8_t *embed = table + 256;
     const int n_tiles = static_cast<int>((p.action_count + kTileN - 1) / kTileN);
+
+    const std::uint32_t idesc = kFp16 ? (umma::InstrDescBf16(128, kTileN) & ~((7u << 7) | (7u << 10)))
+                                      : umma::InstrDescBf16(128, kTileN);
+    const std::uint64_t a_desc0 = umma::SmemDescriptor(umma::SmemAddress(a_tile), 128, 1024);
+    const std::uint32_t b_addr0 = umma::SmemAddress(b_tile);
+    auto failed_now = [&]() { return *reinterpret_cast<volatile int *>(&ts.failed) != 0; };
+    auto can_issue = [&]() { return alive && !failed_now(); };
+    auto wait_bar = [&](std::uint64_t *bar, std::uint32_t parity) -> bool {
+        if (alive && umma::MbarTest(bar, parity)) {
+            return true;
+        }
+        if (alive && !failed_now() && umma::MbarWaitOrStop(bar, parity, q.wait_limit, &ts.failed)) {
+            return true;
+        }
+        *reinterpret_cast<volatile int *>(&ts.failed) = 1;
+        alive = false;
+        return false;
+    };
+    auto issue_load = [&](int stage, int tile) {  // the issuing thread
+        if (can_issue()) {
+            BulkLoad(b_tile + stage * kTileBytes, embed + static_cast<std::size_t>(tile) * kTileBytes, kTileBytes,
+                     &ts.mbar_load[stage]);
+            atomicAdd(&ts.loads_issued[stage], 1u);
+        }
+    };
+    // accumulator buffer: tile & 1; embedding stage: tile % kStages
+    auto issue_mma = [&](int tile) {  // the issuing thread, once tile's stage has landed
+        if (!can_issue()) {
+            return;
+        }
+        const int acc = tile & 1;
+        const int stage = tile % kStages;
+        const std::uint32_t d = ts.tmem_base + static_cast<std::uint32_t>(acc * kTileN);
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            const std::uint64_t ad = a_desc0 + static_cast<std::uint64_t>((s * 256) >> 4);
+            const std::uint64_t bd = umma::SmemDescriptor(b_addr0 + stage * kTileBytes + s * 256, 128, 1024);
+            umma::Mma(d, ad, bd, idesc, s > 0);
+        }
+        umma::Commit(&ts.mbar_mma[acc]);
+    };
+    auto wait_stage_and_issue = [&](int tile) {
+        const int stage = tile % kStages;
+        if (wait_bar(&ts.mbar_load[stage], (load_phase >> stage) & 1u)) {
+            umma::FenceAfterSync();
+            issue_mma(tile);
+        }
+    };
+    // The first embedding tiles stream in while the 16-bit policy operand is built: the stages are free (the trunk's
+    // last reads of this memory ended before its final barrier).
+    if (tid == 0) {
+        umma::FenceProxyAsyncShared();
+        for (int tile = 0; tile < kStages && tile < n_tiles; ++tile) {
+            issue_load(tile, tile);
+        }
+    }
 
     // 16-bit policy operand, K-major tile [128 games][64]
     for (int idx = tid; idx < kChunkGames * kPolicy; idx += kEvalThreads) {
@@ -117,62 +174,16 @@ __device__ void ScoreTensorCores(const TcParams &q, ChunkState &cs, TcState &ts,
     umma::FenceProxyAsyncShared();
     __syncthreads();
 
-    const std::uint32_t idesc = kFp16 ? (umma::InstrDescBf16(128, kTileN) & ~((7u << 7) | (7u << 10)))
-                                      : umma::InstrDescBf16(128, kTileN);
-    const std::uint64_t a_desc0 = umma::SmemDescriptor(umma::SmemAddress(a_tile), 128, 1024);
-    const std::uint32_t b_addr0 = umma::SmemAddress(b_tile);
-    auto failed_now = [&]() { return *reinterpret_cast<volatile int *>(&ts.failed) != 0; };
-    auto can_issue = [&]() { return alive && !failed_now(); };
-    auto wait_bar = [&](std::uint64_t *bar, std::uint32_t parity) -> bool {
-        if (alive && umma::MbarTest(bar, parity)) {
-            return true;
+    // No block barrier inside the tile loop. Thread 0 issues tiles 0 and 1; after that, the last warp to read tile
+    // k's accumulator buffer (an arrival counter per buffer) refills tile k's embedding stage with tile k + kStages
+    // and issues tile k + 2 into the buffer it has just released, while the other warps read the other buffer. The
+    // stage parities advance alike in every thread, tile by tile.
+    for (int tile = 0; tile < 2 && tile < n_tiles; ++tile) {
+        if (tid == 0) {
+            wait_stage_and_issue(tile);
         }
-        if (alive && !failed_now() && umma::MbarWaitOrStop(bar, parity, q.wait_limit, &ts.failed)) {
-            return true;
-        }
-        *reinterpret_cast<volatile int *>(&ts.failed) = 1;
-        alive = false;
-        return false;
-    };
-    auto issue_load = [&](int stage, int tile) {  // thread 0
-        if (can_issue()) {
-            BulkLoad(b_tile + stage * kTileBytes, embed + static_cast<std::size_t>(tile) * kTileBytes, kTileBytes,
-                     &ts.mbar_load[stage]);
-            atomicAdd(&ts.loads_issued[stage], 1u);
-        }
-    };
-    // accumulator buffer: tile & 1; embedding stage: tile % kStages
-    auto issue_mma = [&](int tile) {
-        if (!can_issue()) {
-            return;
-        }
-        const int acc = tile & 1;
-        const int stage = tile % kStages;
-        const std::uint32_t d = ts.tmem_base + static_cast<std::uint32_t>(acc * kTileN);
-#pragma unroll
-        for (int s = 0; s < 4; ++s) {
-            const std::uint64_t ad = a_desc0 + static_cast<std::uint64_t>((s * 256) >> 4);
-            const std::uint64_t bd = umma::SmemDescriptor(b_addr0 + stage * kTileBytes + s * 256, 128, 1024);
-            umma::Mma(d, ad, bd, idesc, s > 0);
-        }
-        umma::Commit(&ts.mbar_mma[acc]);
-    };
-    auto wait_load = [&](int tile) -> bool {
-        const int stage = tile % kStages;
-        const bool ok = wait_bar(&ts.mbar_load[stage], load_uses[stage] & 1u);
-        load_uses[stage] += 1;
-        return ok;
-    };
-    if (tid == 0) {
-        for (int tile = 0; tile < kStages && tile < n_tiles; ++tile) {
-            issue_load(tile, tile);
-        }
-        if (wait_load(0)) {
-            umma::FenceAfterSync();
-            issue_mma(0);
-        }
+        load_phase ^= 1u << (tile % kStages);
     }
-
     const int quadrant = warp & 3;
     const int half = warp >> 2;
     const int row = quadrant * 32 + lane;
@@ -185,44 +196,49 @@ __device__ void ScoreTensorCores(const TcParams &q, ChunkState &cs, TcState &ts,
     }
     for (int tile = 0; tile < n_tiles; ++tile) {
         const int buf = tile & 1;
-        if (tid == 0 && tile + 1 < n_tiles && wait_load(tile + 1)) {
-            umma::FenceAfterSync();
-            issue_mma(tile + 1);
-        }
-        const bool mma_done = wait_bar(&ts.mbar_mma[buf], mma_uses[buf] & 1u);
-        mma_uses[buf] += 1;
+        const bool acc_ok = wait_bar(&ts.mbar_mma[buf], (acc_phase >> buf) & 1u);
+        acc_phase ^= 1u << buf;
         umma::FenceAfterSync();
-        if (tid == 0 && tile + kStages < n_tiles && mma_done) {
-            // tile's MMA has completed, so its embedding stage is free for tile + kStages
-            issue_load(tile % kStages, tile + kStages);
-        }
-        const bool last = tile + 1 == n_tiles;
-#pragma unroll
-        for (int c = 0; c < 2; ++c) {
-            const int col0 = half * 64 + c * 32;
-            float v[32];
-            umma::Load32(ts.tmem_base + static_cast<std::uint32_t>(buf * kTileN + col0) +
+        __syncwarp();
+        {
+            float v[64];
+            umma::Load64(ts.tmem_base + static_cast<std::uint32_t>(buf * kTileN + half * 64) +
                              (static_cast<std::uint32_t>(quadrant * 32) << 16),
                          v);
-            if (last) {
+            if (tile + 1 == n_tiles) {
 #pragma unroll
-                for (int j = 0; j < 32; ++j) {
-                    if (static_cast<std::uint32_t>(tile * kTileN + col0 + j) >= p.action_count) {
+                for (int j = 0; j < 64; ++j) {
+                    if (static_cast<std::uint32_t>(tile * kTileN + half * 64 + j) >= p.action_count) {
                         v[j] = -INFINITY;
                     }
                 }
             }
-#pragma unroll
-            for (int w = 16; w > 0; w >>= 1) {
-#pragma unroll
-                for (int j = 0; j < w; ++j) {
-                    v[j] = fmaxf(v[j], v[j + w]);
-                }
-            }
-            InsertTop4(tv, ti, v[0], tile * 4 + half * 2 + c);
+            const float m0 = Max32(v, 0);
+            const float m1 = Max32(v, 32);
+            InsertTop4(tv, ti, m0, tile * 4 + half * 2);
+            InsertTop4(tv, ti, m1, tile * 4 + half * 2 + 1);
         }
         umma::FenceBeforeSync();
-        __syncthreads();
+        __syncwarp();
+        if (lane == 0) {
+            // one acquire-release add: releases this warp's reads, and the last reader acquires the others'
+            std::uint32_t prior = 0;
+            asm volatile("atom.acq_rel.cta.shared::cta.add.u32 %0, [%1], %2;"
+                         : "=r"(prior)
+                         : "r"(umma::SmemAddress(&ts.readers[buf])), "r"(1u)
+                         : "memory");
+            if ((prior & 7u) == 7u && acc_ok) {  // every warp has read tile's buffer; tile's MMAs have completed
+                if (tile + kStages < n_tiles) {
+                    issue_load(tile % kStages, tile + kStages);
+                }
+                if (tile + 2 < n_tiles) {
+                    wait_stage_and_issue(tile + 2);
+                }
+            }
+        }
+        if (tile + 2 < n_tiles) {
+            load_phase ^= 1u << ((tile + 2) % kStages);
+        }
     }
 #pragma unroll
     for (int j = 0; j < kTopK; ++j) {
@@ -320,10 +336,30 @@ __device__ void ScoreTensorCores(const TcParams &q, ChunkState &cs, TcState &ts,
     const __half *tail = reinterpret_cast<const __half *>(reinterpret_cast<const std::uint8_t *>(gh) + kTailOffsetBytes);
     const int tasks = ts.task_count < kMaxTasks ? ts.task_count : kMaxTasks;
     const int first_full = ts.full_count;
-    for (int k = warp; k < tasks; k += kEvalThreads / 32) {
-        const std::uint32_t task = task_list[k];
-        const int tg = static_cast<int>(task >> 16);
-        RescoreChunk(p, cs, best_key + tg, pv + tg, kLd, tail, tg, static_cast<int>(task & 0xFFFFu), turns_now);
+    constexpr int kWarps = kEvalThreads / 32;
+    if constexpr (kFp16) {
+        // the FP16 table holds every embedding value exactly: two tasks per warp in flight
+        for (int k0 = warp; k0 < tasks; k0 += 2 * kWarps) {
+            const int k1 = k0 + kWarps;
+            const std::uint32_t task0 = task_list[k0];
+            const std::uint32_t task1 = k1 < tasks ? task_list[k1] : task0;
+            const int g0 = static_cast<int>(task0 >> 16);
+            const int g1 = static_cast<int>(task1 >> 16);
+            unsigned long long key0 = 0;
+            unsigned long long key1 = 0;
+            ChunkKeyPairFp16(p, cs, embed, pv + g0, g0, static_cast<int>(task0 & 0xFFFFu), pv + g1, g1,
+                             static_cast<int>(task1 & 0xFFFFu), kLd, turns_now, key0, key1);
+            FoldKeys(best_key + g0, key0);
+            if (k1 < tasks) {
+                FoldKeys(best_key + g1, key1);
+            }
+        }
+    } else {
+        for (int k = warp; k < tasks; k += kWarps) {
+            const std::uint32_t task = task_list[k];
+            const int tg = static_cast<int>(task >> 16);
+            RescoreChunk(p, cs, best_key + tg, pv + tg, kLd, tail, tg, static_cast<int>(task & 0xFFFFu), turns_now);
+        }
     }
     __syncthreads();
     // a game whose exact best stays below top - eps, or whose task list overflowed, is re-scored in full
@@ -345,8 +381,23 @@ __device__ void ScoreTensorCores(const TcParams &q, ChunkState &cs, TcState &ts,
     const int chunks_per_row = static_cast<int>((p.action_count + 31) / 32);
     for (int i = 0; i < full_count; ++i) {
         const int g = full_rows[i];
-        for (int chunk = warp; chunk < chunks_per_row; chunk += kEvalThreads / 32) {
-            RescoreChunk(p, cs, best_key + g, pv + g, kLd, tail, g, chunk, turns_now);
+        if constexpr (kFp16) {
+            // each lane keeps its best key over the warp's chunks, two chunks in flight; one fold per warp
+            unsigned long long best = 0;
+            for (int c0 = warp; c0 < chunks_per_row; c0 += 2 * kWarps) {
+                const int c1 = c0 + kWarps;
+                unsigned long long key0 = 0;
+                unsigned long long key1 = 0;
+                ChunkKeyPairFp16(p, cs, embed, pv + g, g, c0, pv + g, g, c1 < chunks_per_row ? c1 : c0, kLd,
+                                 turns_now, key0, key1);
+                best = key0 > best ? key0 : best;
+                best = c1 < chunks_per_row && key1 > best ? key1 : best;
+            }
+            FoldKeys(best_key + g, best);
+        } else {
+            for (int chunk = warp; chunk < chunks_per_row; chunk += kWarps) {
+                RescoreChunk(p, cs, best_key + g, pv + g, kLd, tail, g, chunk, turns_now);
+            }
         }
     }
     __syncthreads();
@@ -372,8 +423,10 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTcKernel(const TcParams q
     unsigned long long decisions = 0;
     unsigned long long encoded = 0;
     unsigned long long episodes = 0;
-    std::uint32_t load_uses[kStages] = {0, 0, 0};
-    std::uint32_t mma_uses[2] = {0, 0};
+    // parity of the next wait on each stage barrier (bit per stage) and accumulator barrier (bit per buffer); every
+    // thread advances them alike, tile by tile
+    std::uint32_t load_phase = 0;
+    std::uint32_t acc_phase = 0;
     bool alive = true;
     const std::uint32_t total_chunks = p.chunk_start[p.population];
 
@@ -387,10 +440,14 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTcKernel(const TcParams q
         for (int b = 0; b < 2; ++b) {
             umma::MbarInit(&ts.mbar_mma[b], 1);
         }
-        umma::MbarInit(&ts.mbar_drain, 1);
+        for (int w = 0; w < kEvalThreads / 32; ++w) {
+            umma::MbarInit(&ts.mbar_drain[w], 1);
+        }
         for (int b = 0; b < kStages; ++b) {
             ts.loads_issued[b] = 0;
         }
+        ts.readers[0] = 0;
+        ts.readers[1] = 0;
         ts.failed = 0;
     }
     umma::FenceBeforeSync();
@@ -419,7 +476,7 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTcKernel(const TcParams q
                 encoded += tid == 0 ? static_cast<unsigned long long>(cs.active) : 0ull;
             }
             TrunkForward(p, cs, gh, arena, scratch, t, step, ind);
-            ScoreTensorCores<kFp16>(q, cs, ts, gh, arena, t, load_uses, mma_uses, alive);
+            ScoreTensorCores<kFp16>(q, cs, ts, gh, arena, t, load_phase, acc_phase, alive);
             if (ts.failed) {
                 break;
             }
@@ -429,16 +486,22 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTcKernel(const TcParams q
     }
     FlushCounters(p, decisions, encoded, episodes);
     __syncthreads();
-    if (tid == 0 && ts.failed) {
-        SetStatus(p.status, kTimeout);
-        // thread 0's MMAs (a commit tracks all of its earlier tensor-core operations), then the last copy issued on
-        // each stage barrier (the n-th copy completes phase n - 1), before the columns and the CTA are released
-        umma::Commit(&ts.mbar_drain);
-        (void)umma::MbarWait(&ts.mbar_drain, 0, kDrainLimit);
-        for (int b = 0; b < kStages; ++b) {
-            const unsigned int n = ts.loads_issued[b];
-            if (n != 0) {
-                (void)umma::MbarWait(&ts.mbar_load[b], (n - 1u) & 1u, kDrainLimit);
+    if (ts.failed) {  // read after the barrier: uniform
+        // every warp's MMAs (a commit tracks all of its thread's earlier tensor-core operations; lane 0 of each warp
+        // is the only issuer in it), then the last copy issued on each stage barrier (the n-th copy completes phase
+        // n - 1), before the columns and the CTA are released
+        const int warp = tid >> 5;
+        if ((tid & 31) == 0) {
+            umma::Commit(&ts.mbar_drain[warp]);
+            (void)umma::MbarWait(&ts.mbar_drain[warp], 0, kDrainLimit);
+        }
+        if (tid == 0) {
+            SetStatus(p.status, kTimeout);
+            for (int b = 0; b < kStages; ++b) {
+                const unsigned int n = ts.loads_issued[b];
+                if (n != 0) {
+                    (void)umma::MbarWait(&ts.mbar_load[b], (n - 1u) & 1u, kDrainLimit);
+                }
             }
         }
     }

@@ -207,16 +207,6 @@ __device__ __forceinline__ float Fma16(std::uint32_t a, std::uint32_t b, float c
     return d;
 }
 
-// Action a's row of the embedding table (64 16-bit values in eight 16-byte pieces of the operand tile layout).
-__device__ __forceinline__ void LoadEmbedRow(const std::uint8_t *embed, std::uint32_t a, uint4 (&e)[8]) {
-    const std::uint8_t *erow = embed + static_cast<std::size_t>(a >> 7) * (kTileN * kPolicy * 2) +
-                               umma::TileOffset(a & 127u, 0, kPolicy);
-#pragma unroll
-    for (int kg = 0; kg < 8; ++kg) {
-        e[kg] = __ldg(reinterpret_cast<const uint4 *>(erow + kg * 128));
-    }
-}
-
 // Approximate score (16-bit operands, FP32 accumulation) of an action for game g: the policy row of the
 // operand tile against the action's embedding row e.
 template <bool kFp16>
@@ -236,29 +226,6 @@ __device__ __forceinline__ float ApproxScore(const std::uint8_t *a_tile, int g, 
         }
     }
     return (acc[0] + acc[1]) + (acc[2] + acc[3]);
-}
-
-// Three-input maximum (one sm_100 instruction).
-__device__ __forceinline__ float Max3(float a, float b, float c) {
-    float d;
-    asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
-    return d;
-}
-
-// Maximum of v[base .. base + 31] in 16 three-input steps.
-__device__ __forceinline__ float Max32(const float (&v)[64], int base) {
-    float m[12];
-#pragma unroll
-    for (int j = 0; j < 10; ++j) {
-        m[j] = Max3(v[base + 3 * j], v[base + 3 * j + 1], v[base + 3 * j + 2]);
-    }
-    m[10] = v[base + 30];
-    m[11] = v[base + 31];
-    const float a = Max3(m[0], m[1], m[2]);
-    const float b = Max3(m[3], m[4], m[5]);
-    const float c = Max3(m[6], m[7], m[8]);
-    const float d = Max3(m[9], m[10], m[11]);
-    return fmaxf(Max3(a, b, c), d);
 }
 
 // Copies `rows` rows of `cols` (a multiple of 32) 16-bit values, source row stride src_ld, destination row
@@ -1570,10 +1537,32 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
                 }
                 __syncthreads();
                 const int n_tasks = *fb_count;
-                for (int k = warp; k < n_tasks; k += kEvalThreads / 32) {
-                    const int f = static_cast<int>(fb_tasks[k] >> 16);
-                    RescoreChunk(p, cs, fb_key + f, xp + f * kPolicy, 1, tail, ts.fallback_games[b0 + f],
-                                 static_cast<int>(fb_tasks[k] & 0xFFFFu), t);
+                constexpr int kWarps = kEvalThreads / 32;
+                if constexpr (kFp16) {
+                    // the FP16 table holds every embedding value exactly: two tasks per warp in flight
+                    for (int k0 = warp; k0 < n_tasks; k0 += 2 * kWarps) {
+                        const int k1 = k0 + kWarps;
+                        const std::uint32_t task0 = fb_tasks[k0];
+                        const std::uint32_t task1 = k1 < n_tasks ? fb_tasks[k1] : task0;
+                        const int f0 = static_cast<int>(task0 >> 16);
+                        const int f1 = static_cast<int>(task1 >> 16);
+                        unsigned long long key0 = 0;
+                        unsigned long long key1 = 0;
+                        ChunkKeyPairFp16(p, cs, embed, xp + f0 * kPolicy, ts.fallback_games[b0 + f0],
+                                         static_cast<int>(task0 & 0xFFFFu), xp + f1 * kPolicy,
+                                         ts.fallback_games[b0 + f1], static_cast<int>(task1 & 0xFFFFu), 1, t, key0,
+                                         key1);
+                        FoldKeys(fb_key + f0, key0);
+                        if (k1 < n_tasks) {
+                            FoldKeys(fb_key + f1, key1);
+                        }
+                    }
+                } else {
+                    for (int k = warp; k < n_tasks; k += kWarps) {
+                        const int f = static_cast<int>(fb_tasks[k] >> 16);
+                        RescoreChunk(p, cs, fb_key + f, xp + f * kPolicy, 1, tail, ts.fallback_games[b0 + f],
+                                     static_cast<int>(fb_tasks[k] & 0xFFFFu), t);
+                    }
                 }
                 __syncthreads();
                 if (tid < nb && !fb_full[tid]) {
@@ -1588,10 +1577,22 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
                     if (fb_full[f]) {
                         // each lane keeps its best key over the warp's chunks; one fold per warp and row
                         unsigned long long key = 0;
-                        for (int c = warp; c < chunks_per_row; c += kEvalThreads / 32) {
-                            const unsigned long long k =
-                                ChunkKey(p, cs, xp + f * kPolicy, 1, tail, ts.fallback_games[b0 + f], c, t);
-                            key = k > key ? k : key;
+                        const int g = ts.fallback_games[b0 + f];
+                        if constexpr (kFp16) {
+                            for (int c0 = warp; c0 < chunks_per_row; c0 += 2 * kWarps) {
+                                const int c1 = c0 + kWarps;
+                                unsigned long long key0 = 0;
+                                unsigned long long key1 = 0;
+                                ChunkKeyPairFp16(p, cs, embed, xp + f * kPolicy, g, c0, xp + f * kPolicy, g,
+                                                 c1 < chunks_per_row ? c1 : c0, 1, t, key0, key1);
+                                key = key0 > key ? key0 : key;
+                                key = c1 < chunks_per_row && key1 > key ? key1 : key;
+                            }
+                        } else {
+                            for (int c = warp; c < chunks_per_row; c += kWarps) {
+                                const unsigned long long k = ChunkKey(p, cs, xp + f * kPolicy, 1, tail, g, c, t);
+                                key = k > key ? k : key;
+                            }
                         }
                         FoldKeys(fb_key + f, key);
                     }

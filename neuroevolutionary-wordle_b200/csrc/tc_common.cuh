@@ -47,6 +47,29 @@ __device__ __forceinline__ void BulkLoad(void *dst, const void *src, std::uint32
         : "memory");
 }
 
+// Three-input maximum (one sm_100 instruction).
+__device__ __forceinline__ float Max3(float a, float b, float c) {
+    float d;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+
+// Maximum of v[base .. base + 31] in 16 three-input steps.
+__device__ __forceinline__ float Max32(const float (&v)[64], int base) {
+    float m[12];
+#pragma unroll
+    for (int j = 0; j < 10; ++j) {
+        m[j] = Max3(v[base + 3 * j], v[base + 3 * j + 1], v[base + 3 * j + 2]);
+    }
+    m[10] = v[base + 30];
+    m[11] = v[base + 31];
+    const float a = Max3(m[0], m[1], m[2]);
+    const float b = Max3(m[3], m[4], m[5]);
+    const float c = Max3(m[6], m[7], m[8]);
+    const float d = Max3(m[9], m[10], m[11]);
+    return fmaxf(Max3(a, b, c), d);
+}
+
 // Insert x (chunk id xi) into the descending list v[0..3].
 __device__ __forceinline__ void InsertTop4(float (&v)[kTopK], int (&id)[kTopK], float x, int xi) {
 #pragma unroll
@@ -101,6 +124,65 @@ __device__ __forceinline__ unsigned long long ChunkKey(const EvalParams &p, cons
         masked |= cs.guess[u][g] == code;
     }
     return masked ? 0ull : PackKey(s, a);
+}
+
+// Action a's row of a 16-bit embedding table (64 values in eight 16-byte pieces of the K-major operand tile layout,
+// 128 actions per 16 KB tile).
+__device__ __forceinline__ void LoadEmbedRow(const std::uint8_t *embed, std::uint32_t a, uint4 (&e)[8]) {
+    const std::uint8_t *erow = embed + static_cast<std::size_t>(a >> 7) * (128 * kPolicy * 2) +
+                               umma::TileOffset(a & 127u, 0, kPolicy);
+#pragma unroll
+    for (int kg = 0; kg < 8; ++kg) {
+        e[kg] = __ldg(reinterpret_cast<const uint4 *>(erow + kg * 128));
+    }
+}
+
+// Exact keys of this lane's action in two (game, 32-action chunk) tasks, read from an FP16 embedding table. The
+// FP16 table holds every embedding value exactly (the fixed features are small integers, the tail rows are the
+// genome's own FP16 values), so each FP32 chain -- fma(p_k, e_k, s) for k = 0..63 in ascending order, the plain
+// form's and the reference's (output_embedding.hpp:98-119) -- gives ExactScore's bits. Both tasks' rows and codes
+// are loaded before either chain starts, and the two chains run interleaved. key1 is computed for every lane; the
+// caller ignores it when it has no second task.
+__device__ __forceinline__ void ChunkKeyPairFp16(const EvalParams &p, const ChunkState &cs, const std::uint8_t *embed,
+                                                 const float *pv0, int g0, int chunk0, const float *pv1, int g1,
+                                                 int chunk1, int ld, int turns, unsigned long long &key0,
+                                                 unsigned long long &key1) {
+    const std::uint32_t lane = threadIdx.x & 31;
+    const std::uint32_t a0 = static_cast<std::uint32_t>(chunk0) * 32u + lane;
+    const std::uint32_t a1 = static_cast<std::uint32_t>(chunk1) * 32u + lane;
+    const bool v0 = a0 < p.action_count;
+    const bool v1 = a1 < p.action_count;
+    uint4 e0[8];
+    uint4 e1[8];
+    LoadEmbedRow(embed, v0 ? a0 : 0u, e0);
+    LoadEmbedRow(embed, v1 ? a1 : 0u, e1);
+    const std::uint32_t code0 = v0 ? __ldg(p.codes + a0) : 0u;
+    const std::uint32_t code1 = v1 ? __ldg(p.codes + a1) : 0u;
+    float s0 = 0.0f;
+    float s1 = 0.0f;
+#pragma unroll
+    for (int kg = 0; kg < 8; ++kg) {
+        const std::uint32_t w0[4] = {e0[kg].x, e0[kg].y, e0[kg].z, e0[kg].w};
+        const std::uint32_t w1[4] = {e1[kg].x, e1[kg].y, e1[kg].z, e1[kg].w};
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int k = kg * 8 + 2 * i;
+            const float2 f0 = __half22float2(*reinterpret_cast<const __half2 *>(&w0[i]));
+            const float2 f1 = __half22float2(*reinterpret_cast<const __half2 *>(&w1[i]));
+            s0 = __fmaf_rn(pv0[k * ld], f0.x, s0);
+            s1 = __fmaf_rn(pv1[k * ld], f1.x, s1);
+            s0 = __fmaf_rn(pv0[(k + 1) * ld], f0.y, s0);
+            s1 = __fmaf_rn(pv1[(k + 1) * ld], f1.y, s1);
+        }
+    }
+    bool m0 = !v0;
+    bool m1 = !v1;
+    for (int u = 0; u < turns; ++u) {
+        m0 |= cs.guess[u][g0] == code0;
+        m1 |= cs.guess[u][g1] == code1;
+    }
+    key0 = m0 ? 0ull : PackKey(s0, a0);
+    key1 = m1 ? 0ull : PackKey(s1, a1);
 }
 
 // Folds a warp's keys (the masked argmax) into *best_key.
