@@ -80,6 +80,7 @@ struct nwg_runtime {
     std::size_t tc_tables_bytes = 0;
     std::size_t last_table_pitch = 0;  // of the tables the last tensor-core evaluation built (0: none)
     std::uint8_t *trunk_tables = nullptr;
+    std::uint8_t *xt_tables = nullptr;  // exact trunk tables of the FP32 forms (ExactTrunkTablePitch per individual)
     float margin_tau = 1.0e-3f;
     std::uint32_t wait_limit = kDefaultWaitLimit;  // bounded mbarrier waits of the tensor-core kernels
     // a generation prepared for assembly (evaluated and planned; nwg_prepare_generation / checkpoint restore)
@@ -445,7 +446,8 @@ void FreeRuntime(nwg_runtime *rt) {
                            rt->slot_used,  rt->status,       rt->summary,     rt->shards,      rt->cell_offsets,
                            rt->cell_words, rt->local_words,  rt->chunk_start, rt->score_sum,   rt->steps,
                            rt->won_sum,
-                           rt->scratch,    rt->tc_tables,    rt->trunk_tables, rt->band_parent_table};
+                           rt->scratch,    rt->tc_tables,    rt->trunk_tables, rt->band_parent_table,
+                           rt->xt_tables};
     for (void *p : device_ptrs) {
         if (p != nullptr) {
             cudaFree(p);
@@ -489,6 +491,24 @@ cudaError_t RecordEvent(cudaEvent_t event, cudaStream_t stream) {
 }
 
 // CTAs of the persistent evaluation kernels: the tuned count, never more than the scratch holds.
+// The FP32 forms' exact trunk tables, allocated on first use. Never while the runtime's stream is being captured
+// (an allocation would break the capture): that evaluation then stages the weights from the genome, with the same
+// results; so does one whose allocation fails.
+void EnsureExactTrunkTables(nwg_runtime *rt) {
+    if (rt->xt_tables != nullptr) {
+        return;
+    }
+    cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+    if (rt->stream != nullptr && cudaStreamIsCapturing(rt->stream, &capture) == cudaSuccess &&
+        capture != cudaStreamCaptureStatusNone) {
+        return;
+    }
+    if (cudaMalloc(&rt->xt_tables, rt->max_generation_size * ExactTrunkTablePitch()) != cudaSuccess) {
+        rt->xt_tables = nullptr;
+        (void)cudaGetLastError();
+    }
+}
+
 int EvalGrid(const nwg_runtime *rt) {
     return rt->eval_ctas > 0 && rt->eval_ctas < rt->scratch_ctas ? rt->eval_ctas : rt->scratch_ctas;
 }
@@ -571,6 +591,18 @@ int EvaluateImpl(nwg_runtime *rt, const nwg_runtime_word_counts *counts, const n
     p.trace_turns = static_cast<std::int32_t *>(turns);
     p.trace_scores = static_cast<float *>(scores);
     p.trace_policy = static_cast<float *>(policy);
+    // the FP32 chains of the plain and exact forms stream their weights from the exact trunk tables
+    const bool fp32_trunk = rt->form == NWG_FORM_FP32 || rt->form == NWG_FORM_TC_BF16 ||
+                            rt->form == NWG_FORM_TC_FP16 || selectable <= 128;
+    if (fp32_trunk) {
+        EnsureExactTrunkTables(rt);
+        if (rt->xt_tables != nullptr) {
+            NWG_TRY(LaunchBuildExactTrunkTables(rt->slab, rt->pitch, rt->cur_slots, population, rt->xt_tables,
+                                                rt->stream));
+            p.xt = rt->xt_tables;
+            p.xt_pitch = ExactTrunkTablePitch();
+        }
+    }
     // at <= 128 selectable actions every form scores on the reference's tensor-tile path, in the plain kernel
     if (rt->form == NWG_FORM_FP32 || selectable <= 128) {
         NWG_TRY(RecordEvent(rt->eval_begin, rt->stream));
@@ -1657,7 +1689,12 @@ int nwg_advance_graphed(nwg_runtime *rt, uint32_t generation_seed, const nwg_run
         rt->breed_warps = 8;
         return status;
     };
-    // capture: prepare (no callbacks, so it never waits on the device) and the assembly's device work
+    // capture: prepare (no callbacks, so it never waits on the device) and the assembly's device work; the FP32
+    // forms' exact trunk tables are allocated first, since nothing is allocated while capturing
+    if (rt->form == NWG_FORM_FP32 || rt->form == NWG_FORM_TC_BF16 || rt->form == NWG_FORM_TC_FP16 ||
+        rt->action_count <= 128) {
+        EnsureExactTrunkTables(rt);
+    }
     cudaGraph_t graph = nullptr;
     if (cudaStreamBeginCapture(rt->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
         return restore(kCudaFailure);

@@ -25,6 +25,7 @@
 #include <cstdint>
 
 #include "eval_common.cuh"
+#include "trunk_fp32.cuh"
 
 namespace nwg {
 namespace {
@@ -253,6 +254,8 @@ __device__ __forceinline__ void ScoreSmallActionSpace(const EvalParams &p, Chunk
     __syncthreads();
 }
 
+// kStreamed: the encoder and trunk stream their weights from the exact trunk tables (p.xt), else from the genome.
+template <bool kStreamed>
 __global__ void __launch_bounds__(kEvalThreads, 2) EvalFp32Kernel(const EvalParams p) {
     extern __shared__ __align__(16) float arena[];
     __shared__ ChunkState st;
@@ -269,10 +272,18 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalFp32Kernel(const EvalPara
         }
         const std::uint32_t ind = static_cast<std::uint32_t>(st.individual);
         const __half *gh = reinterpret_cast<const __half *>(p.slab + static_cast<std::size_t>(st.slot) * p.pitch);
+        const std::uint8_t *xt = kStreamed ? p.xt + static_cast<std::size_t>(ind) * p.xt_pitch : nullptr;
+        auto encode = [&](int u) {
+            if constexpr (kStreamed) {
+                EncodeRoundX(st, gh, xt, arena, scratch, u);
+            } else {
+                EncodeRound(st, gh, arena, scratch, u);
+            }
+        };
         SetupGames(p, st, gh, scratch);
         if (st.cls == 1 && CountActive(st) > 0) {
-            EncodeRound(st, gh, arena, scratch, 0);
-            EncodeRound(st, gh, arena, scratch, 1);
+            encode(0);
+            encode(1);
             encoded += tid == 0 ? 2ull * st.active : 0ull;
         }
         for (int step = 0; step < kMaxTurns; ++step) {
@@ -281,10 +292,14 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalFp32Kernel(const EvalPara
             }
             const int t = st.cls == 0 ? step : step + 2;  // turns already on every active grid
             if (step > 0) {
-                EncodeRound(st, gh, arena, scratch, t - 1);  // the turn appended by the previous decision
+                encode(t - 1);  // the turn appended by the previous decision
                 encoded += tid == 0 ? static_cast<unsigned long long>(st.active) : 0ull;
             }
-            TrunkForward(p, st, gh, arena, scratch, t, step, ind);
+            if constexpr (kStreamed) {
+                TrunkForwardX(p, st, gh, xt, arena, scratch, t, step, ind);
+            } else {
+                TrunkForward(p, st, gh, arena, scratch, t, step, ind);
+            }
             if (p.action_count <= static_cast<std::uint32_t>(kSmallActionSpace)) {
                 ScoreSmallActionSpace(p, st, gh, arena, t);
             } else {
@@ -536,16 +551,21 @@ cudaError_t LaunchEvalPrepare(const WordSource &source, std::uint32_t population
 }
 
 cudaError_t LaunchEvalFp32(const EvalParams &params, int cta_count, cudaStream_t stream) {
-    static std::atomic<unsigned long long> configured{0};
-    if (const cudaError_t e =
-            RaiseSharedLimit(EvalFp32Kernel, kArenaFloats * static_cast<int>(sizeof(float)), configured);
+    static std::atomic<unsigned long long> configured[2]{{0}, {0}};
+    const int bytes = kArenaFloats * static_cast<int>(sizeof(float));
+    if (const cudaError_t e = params.xt != nullptr ? RaiseSharedLimit(EvalFp32Kernel<true>, bytes, configured[1])
+                                                   : RaiseSharedLimit(EvalFp32Kernel<false>, bytes, configured[0]);
         e != cudaSuccess) {
         return e;
     }
     if (cta_count <= 0) {
         return cudaSuccess;
     }
-    EvalFp32Kernel<<<cta_count, kEvalThreads, kArenaFloats * sizeof(float), stream>>>(params);
+    if (params.xt != nullptr) {
+        EvalFp32Kernel<true><<<cta_count, kEvalThreads, bytes, stream>>>(params);
+    } else {
+        EvalFp32Kernel<false><<<cta_count, kEvalThreads, bytes, stream>>>(params);
+    }
     return cudaGetLastError();
 }
 

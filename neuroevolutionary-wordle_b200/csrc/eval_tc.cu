@@ -1,25 +1,27 @@
 // Fitness evaluation, tensor-core scoring form: action scores on tcgen05, decisions re-scored exactly.
 //
-// Same chunk structure, encoder and FP32 trunk as the plain form (eval_common.cuh); only the scoring
-// phase differs. Per game step and chunk of up to 128 games:
+// Same chunk structure, encoder and FP32 trunk as the plain form (eval_common.cuh, or trunk_fp32.cuh when the
+// exact trunk tables are built); only the scoring phase differs. Per game step and chunk of up to 128 games:
 //   1. the FP32 policy vectors are rounded to 16-bit (BF16, or FP16) into a K-major operand tile;
 //   2. the individual's embedding table, kept as a 16-bit copy in the tensor-core layout
 //      (BuildTcTablesKernel), streams through shared memory 128 actions at a time by bulk copies;
-//   3. one thread issues tcgen05.mma (M = 128 games, N = 128 actions, K = 64) into one of two TMEM
-//      accumulators while all eight warps read the other one back (tcgen05.ld) and keep, per game, the
-//      four largest 32-action chunk maxima;
+//   3. tcgen05.mma (M = 128 games, N = 128 actions, K = 64) fills two TMEM accumulators in turn; all eight warps
+//      read a buffer back (tcgen05.ld) and keep, per game, the four largest 32-action chunk maxima, and the last
+//      warp to read a buffer refills its stage and issues the tile two ahead into it;
 //   4. every chunk whose maximum lies within 2 * eps of the best chunk free of guessed words is re-scored
 //      in FP32 with the plain form's own fused-multiply-add chain, and the game's guess is the exact FP32
 //      argmax (ties to the lower index, guessed words masked).
-//      eps bounds |tensor-core score - FP32 score|: eps = kappa * sum_k |p_k| * max_a |e_ak|, with kappa
-//      covering the 16-bit rounding of p (and of e for BF16) and both FP32 accumulations. When the four
-//      tracked chunks cannot prove that no other chunk reaches the window, the game is re-scored over
-//      every action. The guesses are therefore identical to the plain form's.
+//      eps bounds |tensor-core score - FP32 score|. FP16 operands: sum_k |fp16(p_k) - p_k| max_a |e_ak| (the
+//      embeddings are exact in FP16) plus both 64-term FP32 accumulations; BF16 operands: kappa sum_k |p_k|
+//      max_a |e_ak|, kappa covering both roundings and the accumulations. When the four tracked chunks cannot
+//      prove that no other chunk reaches the window, the game is re-scored over every action. The guesses are
+//      therefore identical to the plain form's.
 // Every mbarrier wait is bounded; a wait that gives up records NWG_TIMEOUT and the kernel winds down.
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
 #include "tc_common.cuh"
+#include "trunk_fp32.cuh"
 
 namespace nwg {
 namespace {
@@ -74,7 +76,7 @@ struct TcParams {
 // Failure protocol: a wait that gives up (q.wait_limit polls, or earlier once another thread has recorded a failure)
 // marks its thread dead (`alive`) and the CTA failed; a dead thread issues nothing and no copy or MMA is issued once
 // the CTA has failed, so every barrier phase still gets exactly one copy or commit, and the kernel's wind-down waits
-// for the copies issued on each barrier (counted) and for thread 0's MMAs.
+// for the copies issued on each barrier (counted) and for every issuing warp's MMAs.
 template <bool kFp16>
 __device__ __forceinline__ void ScoreTensorCores(const TcParams &q, ChunkState &cs, TcState &ts, const __half *gh,
                                                  float *arena, int t, std::uint32_t &load_phase,
@@ -266,13 +268,23 @@ __device__ __forceinline__ void ScoreTensorCores(const TcParams &q, ChunkState &
             return m;
         };
         float s_sum = 0.0f;
+        float s_dev = 0.0f;
         bool finite = true;
         for (int k = 0; k < kPolicy; ++k) {
             const float pk = pv[k * kLd + g];
             finite &= fabsf(pk) < (kFp16 ? 60000.0f : 3.0e38f);
             s_sum = __fmaf_rn(fabsf(pk), emax[k], s_sum);
+            if constexpr (kFp16) {
+                // the operand's own rounding error: p and its FP16 value are within a factor of two of each
+                // other (or the FP16 value is 0), so the difference is exact
+                s_dev = __fmaf_rn(fabsf(__half2float(__float2half_rn(pk)) - pk), emax[k], s_dev);
+            }
         }
-        const float eps = q.kappa * s_sum * 1.0001f;
+        // |tensor-core score - FP32 score| <= sum_k |p~_k - p_k| |e_ak| + both 64-term FP32 accumulations. FP16 operands
+        // hold every embedding exactly, so the first term is s_dev (the actual rounding of this game's policy) and
+        // the accumulations are covered by 2e-5 sum_k |p_k| max_a |e_ak| (64 x 2^-23 = 7.6e-6 each, tensor core
+        // and FP32 chain). BF16 operands also round the embeddings: kappa bounds both roundings relative to |p||e|.
+        const float eps = kFp16 ? (s_dev + 2.0e-5f * s_sum) * 1.0001f : q.kappa * s_sum * 1.0001f;
         bool full = !finite || !(eps < INFINITY);
         float top = -INFINITY;
         for (int h = 0; h < 2; ++h) {
@@ -412,7 +424,8 @@ __device__ __forceinline__ void ScoreTensorCores(const TcParams &q, ChunkState &
     __syncthreads();
 }
 
-template <bool kFp16>
+// kStreamed: the FP32 encoder and trunk stream their weights from the exact trunk tables (q.base.xt).
+template <bool kFp16, bool kStreamed>
 __global__ void __launch_bounds__(kEvalThreads, 2) EvalTcKernel(const TcParams q) {
     extern __shared__ __align__(1024) float arena[];
     __shared__ ChunkState cs;
@@ -460,10 +473,18 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTcKernel(const TcParams q
         }
         const std::uint32_t ind = static_cast<std::uint32_t>(cs.individual);
         const __half *gh = reinterpret_cast<const __half *>(p.slab + static_cast<std::size_t>(cs.slot) * p.pitch);
+        const std::uint8_t *xt = kStreamed ? p.xt + static_cast<std::size_t>(ind) * p.xt_pitch : nullptr;
+        auto encode = [&](int u) {
+            if constexpr (kStreamed) {
+                EncodeRoundX(cs, gh, xt, arena, scratch, u);
+            } else {
+                EncodeRound(cs, gh, arena, scratch, u);
+            }
+        };
         SetupGames(p, cs, gh, scratch);
         if (cs.cls == 1 && CountActive(cs) > 0) {
-            EncodeRound(cs, gh, arena, scratch, 0);
-            EncodeRound(cs, gh, arena, scratch, 1);
+            encode(0);
+            encode(1);
             encoded += tid == 0 ? 2ull * cs.active : 0ull;
         }
         for (int step = 0; step < kMaxTurns; ++step) {
@@ -472,10 +493,14 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTcKernel(const TcParams q
             }
             const int t = cs.cls == 0 ? step : step + 2;
             if (step > 0) {
-                EncodeRound(cs, gh, arena, scratch, t - 1);
+                encode(t - 1);
                 encoded += tid == 0 ? static_cast<unsigned long long>(cs.active) : 0ull;
             }
-            TrunkForward(p, cs, gh, arena, scratch, t, step, ind);
+            if constexpr (kStreamed) {
+                TrunkForwardX(p, cs, gh, xt, arena, scratch, t, step, ind);
+            } else {
+                TrunkForward(p, cs, gh, arena, scratch, t, step, ind);
+            }
             ScoreTensorCores<kFp16>(q, cs, ts, gh, arena, t, load_phase, acc_phase, alive);
             if (ts.failed) {
                 break;
@@ -645,10 +670,17 @@ cudaError_t LaunchEvalTc(const EvalParams &params, const std::uint8_t *tables, s
                          bool fp16, unsigned long long *tc_counters, int cta_count, cudaStream_t stream,
                          std::uint32_t wait_limit) {
     const int arena_bytes = kArenaFloats * static_cast<int>(sizeof(float));
-    static std::atomic<unsigned long long> configured[2]{{0}, {0}};
-    if (const cudaError_t e = fp16 ? RaiseSharedLimit(EvalTcKernel<true>, arena_bytes, configured[1])
-                                   : RaiseSharedLimit(EvalTcKernel<false>, arena_bytes, configured[0]);
-        e != cudaSuccess) {
+    static std::atomic<unsigned long long> configured[4]{{0}, {0}, {0}, {0}};
+    const bool streamed = params.xt != nullptr;
+    cudaError_t e = cudaSuccess;
+    if (fp16) {
+        e = streamed ? RaiseSharedLimit(EvalTcKernel<true, true>, arena_bytes, configured[3])
+                     : RaiseSharedLimit(EvalTcKernel<true, false>, arena_bytes, configured[1]);
+    } else {
+        e = streamed ? RaiseSharedLimit(EvalTcKernel<false, true>, arena_bytes, configured[2])
+                     : RaiseSharedLimit(EvalTcKernel<false, false>, arena_bytes, configured[0]);
+    }
+    if (e != cudaSuccess) {
         return e;
     }
     if (cta_count <= 0) {
@@ -663,9 +695,15 @@ cudaError_t LaunchEvalTc(const EvalParams &params, const std::uint8_t *tables, s
     q.tc_counters = tc_counters;
     q.wait_limit = wait_limit;
     if (fp16) {
-        EvalTcKernel<true><<<cta_count, kEvalThreads, arena_bytes, stream>>>(q);
+        if (streamed) {
+            EvalTcKernel<true, true><<<cta_count, kEvalThreads, arena_bytes, stream>>>(q);
+        } else {
+            EvalTcKernel<true, false><<<cta_count, kEvalThreads, arena_bytes, stream>>>(q);
+        }
+    } else if (streamed) {
+        EvalTcKernel<false, true><<<cta_count, kEvalThreads, arena_bytes, stream>>>(q);
     } else {
-        EvalTcKernel<false><<<cta_count, kEvalThreads, arena_bytes, stream>>>(q);
+        EvalTcKernel<false, false><<<cta_count, kEvalThreads, arena_bytes, stream>>>(q);
     }
     return cudaGetLastError();
 }

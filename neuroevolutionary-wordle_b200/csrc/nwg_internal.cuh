@@ -82,6 +82,10 @@ struct EvalParams {
     float *trace_scores;              // [population * trace_episodes]
     float *trace_policy;              // [population * trace_episodes * 6 * 64]
     std::uint32_t trace_episodes;
+    // the per-individual exact trunk tables (LaunchBuildExactTrunkTables), or null: the FP32 forms then stage the
+    // weights from the genome itself
+    const std::uint8_t *xt;
+    std::size_t xt_pitch;
 };
 
 std::size_t EvalScratchFloatsPerCta();
@@ -93,6 +97,12 @@ cudaError_t LaunchEvalFp32(const EvalParams &params, int cta_count, cudaStream_t
 cudaError_t LaunchFinalizeFitness(const std::uint32_t *score_sum, const std::uint32_t *local_words,
                                   std::uint32_t population, float *fitness, std::uint32_t *evaluation_counts,
                                   std::uint8_t *has_fitness, int *status, cudaStream_t stream);
+
+// Per-individual exact trunk tables (trunk_table.cu): the encoder and trunk weights as FP32 [input][output] blocks for
+// the FP32 forms' streamed policy path.
+std::size_t ExactTrunkTablePitch();
+cudaError_t LaunchBuildExactTrunkTables(const std::uint8_t *slab, std::size_t pitch, const std::uint32_t *slots,
+                                        std::uint32_t population, std::uint8_t *tables, cudaStream_t stream);
 
 // ---- fitness evaluation, tensor-core scoring form ----
 std::size_t TcTablePitch(std::uint32_t action_count);
