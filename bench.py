@@ -708,7 +708,8 @@ def run_ours(args) -> None:
 
     rank, world, local = dist_setup(args.gpus)
     nwg = importlib.import_module("neuroevolutionary-wordle_b200")
-    wl = {"full": nwg.workload.FULL, "medium": nwg.workload.MEDIUM, "small": nwg.workload.SMALL}[args.workload]
+    wl = {"full": nwg.workload.FULL, "quarter": nwg.workload.QUARTER, "medium": nwg.workload.MEDIUM,
+          "small": nwg.workload.SMALL}[args.workload]
     if world > 1:
         run_bands(args, nwg, torch, wl, rank, world, local)
         return
@@ -952,7 +953,8 @@ def run_reference(args) -> None:
         print(json.dumps({"impl": "reference", "unavailable": "the reference's CPU path has no widening run to time; "
                           "its arm is measured on the full workload"}))
         return
-    wl = {"full": nwg_workload.FULL, "medium": nwg_workload.MEDIUM, "small": nwg_workload.SMALL}[args.workload]
+    wl = {"full": nwg_workload.FULL, "quarter": nwg_workload.QUARTER, "medium": nwg_workload.MEDIUM,
+          "small": nwg_workload.SMALL}[args.workload]
     if O.ref_host() is None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref_host.so was not built"}))
         return
@@ -1020,7 +1022,7 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["full", "medium", "small", "growth"], default="full",
+    ap.add_argument("--workload", choices=["full", "quarter", "medium", "small", "growth"], default="full",
                     help="growth: the batching form (16,384 individuals, uneven shards, widening action space)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--form", choices=sorted(FORMS), default="tc-fp16",

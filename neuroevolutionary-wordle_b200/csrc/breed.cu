@@ -206,8 +206,243 @@ __device__ void MutateRun(__half *values, std::uint32_t count, Stream &s, float 
     s.cached_pair = cached_word & 0x7FFFFFFFu;
 }
 
+// ---- window-parallel mutation walk ----
+//
+// The serial walk's only state between draw positions is (offset into the next positions, cached normal held), so
+// a run is cut into 128-position windows, one per lane, 32 windows per step: each lane draws its window's
+// uniforms, turns them into a 128-bit hit mask and walks it from the two entry states with no position taken
+// (cached or not; a window whose first positions were taken by the previous window's last normal pair walks the
+// same way unless one of those positions is a hit, which the chain then walks again). A serial chain of 32
+// shuffles picks every window's true entry state, a prefix sum of the windows' value counts gives
+// each window its first value index, and every lane then walks its own window once more, drawing the normal
+// pairs of its hits and applying them. The draws, their order and their arithmetic are the serial walk's.
+
+constexpr unsigned kFullMask = 0xffffffffu;
+constexpr std::uint32_t kWindowRunMin = 4096;  // shorter runs take the serial walk
+
+// curand_uniform is non-decreasing in the generator's 32-bit output x, so (curand_uniform < p) <=> (x < threshold).
+// Valid for 0 < p < 1 when the largest output's uniform is not below p (ok reports that).
+__device__ std::uint32_t UniformThreshold(float p, bool &ok) {
+    ok = !(_curand_uniform(0xFFFFFFFFu) < p);
+    if (!(_curand_uniform(0u) < p)) {
+        return 0u;
+    }
+    std::uint32_t lo = 0u, hi = 0xFFFFFFFFu;  // uniform(lo) < p <= uniform(hi)
+    while (hi - lo > 1u) {
+        const std::uint32_t mid = lo + (hi - lo) / 2u;
+        if (_curand_uniform(mid) < p) {
+            lo = mid;
+        } else {
+            hi = mid;
+        }
+    }
+    return hi;
+}
+
+// First hit at or after window offset r (0 <= r < 128); 128 when none.
+__device__ __forceinline__ int NextHit(unsigned long long lo, unsigned long long hi, int r) {
+    const unsigned long long xlo = r < 64 ? (lo & (~0ull << (r & 63))) : 0ull;
+    const unsigned long long xhi = r < 64 ? hi : (hi & (~0ull << ((r - 64) & 63)));
+    return xlo != 0ull ? __ffsll(static_cast<long long>(xlo)) - 1
+                       : (xhi != 0ull ? 63 + __ffsll(static_cast<long long>(xhi)) : 128);
+}
+
+// Walks one window from entry state (e positions taken, cached c): every miss and every hit takes one position
+// and one value; a hit without a cached normal also takes the next two positions for a fresh pair. Returns the
+// exit state (positions of the next window taken + 3 * cached), the values walked, and 1 + the window offset
+// of the last fresh pair (0: none drawn).
+__device__ __forceinline__ void WalkWindow(unsigned long long lo, unsigned long long hi, int e, bool c,
+                                           std::uint32_t &exit_state, std::uint32_t &walked,
+                                           std::uint32_t &last_fresh) {
+    int r = e;
+    int n = 0;
+    int lf = 0;
+    while (r < 128) {
+        const int h = NextHit(lo, hi, r);
+        if (h >= 128) {
+            n += 128 - r;
+            r = 128;
+            break;
+        }
+        n += h - r + 1;
+        if (c) {
+            c = false;
+            r = h + 1;
+        } else {
+            c = true;
+            lf = h + 2;
+            r = h + 3;
+        }
+    }
+    exit_state = static_cast<std::uint32_t>(r - 128) + (c ? 3u : 0u);
+    walked = static_cast<std::uint32_t>(n);
+    last_fresh = static_cast<std::uint32_t>(lf);
+}
+
+// The normal pair drawn at `pair`: the generator's curand_normal twice from that position.
+__device__ __forceinline__ float2 PairNormals(const Stream &s, unsigned long long pair) {
+    curandStatePhilox4_32_10_t state = StateAt(s, pair);
+    const float a = curand_normal(&state);
+    const float b = curand_normal(&state);
+    return make_float2(a, b);
+}
+
+__device__ void MutateRunWindows(__half *values, std::uint32_t count, Stream &s, std::uint32_t threshold, float sigma,
+                                 int lane) {
+    unsigned long long pos = s.position;      // lane 0's window starts here with no position taken
+    bool cached = s.cached;
+    unsigned long long pair = s.cached_pair;  // the pair whose second value is cached
+    std::uint32_t v_base = 0;
+    while (v_base < count) {
+        // the step's values lie in [v_base, v_base + 4096): their lines reach L2 while the hits are found
+        for (std::uint32_t line = v_base / 64u + static_cast<std::uint32_t>(lane); line <= (v_base + 4095u) / 64u;
+             line += 32u) {
+            if (line * 64u < count) {
+                asm volatile("prefetch.L2 [%0];" ::"l"(values + line * 64u));
+            }
+        }
+        const unsigned long long win = pos + 128ull * static_cast<unsigned>(lane);
+        const std::uint32_t delta = static_cast<std::uint32_t>(pos & 3ull);
+        // ---- pass 1: the window's hit mask, from 33 aligned four-output blocks ----
+        std::uint32_t raw0 = 0, raw1 = 0, raw2 = 0, raw3 = 0, raw4 = 0;
+        {
+            curandStatePhilox4_32_10_t state = StateAt(s, win - delta);
+#pragma unroll
+            for (int b = 0; b < 33; ++b) {
+                const uint4 x = curand4(&state);
+                const std::uint32_t nib = (x.x < threshold ? 1u : 0u) | (x.y < threshold ? 2u : 0u) |
+                                          (x.z < threshold ? 4u : 0u) | (x.w < threshold ? 8u : 0u);
+                const std::uint32_t bits = nib << (4 * (b & 7));
+                if (b < 8) {
+                    raw0 |= bits;
+                } else if (b < 16) {
+                    raw1 |= bits;
+                } else if (b < 24) {
+                    raw2 |= bits;
+                } else if (b < 32) {
+                    raw3 |= bits;
+                } else {
+                    raw4 |= bits;
+                }
+            }
+        }
+        const unsigned long long lo = static_cast<unsigned long long>(__funnelshift_r(raw0, raw1, delta)) |
+                                      (static_cast<unsigned long long>(__funnelshift_r(raw1, raw2, delta)) << 32);
+        const unsigned long long hi = static_cast<unsigned long long>(__funnelshift_r(raw2, raw3, delta)) |
+                                      (static_cast<unsigned long long>(__funnelshift_r(raw3, raw4, delta)) << 32);
+        // ---- the two entry states with no position taken: exits, values walked, last fresh pairs ----
+        // A window entered with e > 0 positions taken walks exactly like one entered with none when its first e
+        // positions are misses (then it only walks e values fewer); otherwise the chain walks it again.
+        std::uint32_t summary = static_cast<std::uint32_t>(lo & 3ull) << 6;  // hits among the first two positions
+        std::uint32_t walked01 = 0;
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            std::uint32_t x, n, f;
+            WalkWindow(lo, hi, 0, c != 0, x, n, f);
+            summary |= (x << (3 * c)) | (f << (8 + 8 * c));
+            walked01 |= n << (16 * c);
+        }
+        // ---- the chain: every window's entry state, values walked and the pair cached on entry ----
+        std::uint32_t state = cached ? 3u : 0u;
+        std::uint32_t my_state = 0, my_walked = 0;
+        unsigned long long my_pair = 0;
+        for (int l = 0; l < 32; ++l) {
+            const std::uint32_t w = __shfl_sync(kFullMask, summary, l);
+            const std::uint32_t e = state % 3u;
+            const std::uint32_t c = state / 3u;
+            std::uint32_t x, n, f;
+            if (e != 0u && ((w >> 6) & ((1u << e) - 1u)) != 0u) {
+                // a hit among the taken positions: walk window l from its own entry (rare; warp-uniform)
+                const unsigned long long lo_l = __shfl_sync(kFullMask, lo, l);
+                const unsigned long long hi_l = __shfl_sync(kFullMask, hi, l);
+                WalkWindow(lo_l, hi_l, static_cast<int>(e), c != 0u, x, n, f);
+            } else {
+                x = (w >> (3u * c)) & 7u;
+                f = (w >> (8u + 8u * c)) & 0xFFu;
+                n = ((walked01 >> (16u * c)) & 0xFFFFu) - e;  // meaningful on lane l only
+            }
+            if (lane == l) {
+                my_state = state;
+                my_pair = pair;
+                my_walked = n;
+            }
+            if (f != 0u) {
+                pair = pos + 128ull * static_cast<unsigned>(l) + (f - 1u);
+            }
+            state = x;
+        }
+        std::uint32_t inclusive = my_walked;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const std::uint32_t t = __shfl_up_sync(kFullMask, inclusive, d);
+            if (lane >= d) {
+                inclusive += t;
+            }
+        }
+        const std::uint32_t total = __shfl_sync(kFullMask, inclusive, 31);
+        const std::uint32_t v0 = v_base + (inclusive - my_walked);
+        // ---- pass 2: this window's hits get their normals ----
+        const std::uint32_t limit = min(count, v0 + my_walked);
+        int r = static_cast<int>(my_state % 3u);
+        bool c = my_state >= 3u;
+        unsigned long long lane_pair = my_pair;
+        bool have_second = false;
+        float second = 0.0f;
+        std::uint32_t v = v0;
+        while (v < limit) {
+            const int h = NextHit(lo, hi, r);
+            const std::uint32_t misses = static_cast<std::uint32_t>((h < 128 ? h : 128) - r);
+            if (misses >= limit - v) {
+                r += static_cast<int>(limit - v);
+                v = limit;
+                break;
+            }
+            v += misses;
+            float n;
+            if (c) {
+                if (!have_second) {
+                    second = PairNormals(s, lane_pair).y;
+                }
+                n = second;
+                have_second = false;
+                c = false;
+                r = h + 1;
+            } else {
+                lane_pair = win + static_cast<unsigned long long>(h + 1);
+                const float2 nn = PairNormals(s, lane_pair);
+                n = nn.x;
+                second = nn.y;
+                have_second = true;
+                c = true;
+                r = h + 3;
+            }
+            values[v] = __float2half(__fmaf_rn(sigma, n, __half2float(values[v])));
+            ++v;
+        }
+        // ---- the stream state after this step ----
+        const unsigned end_lanes = __ballot_sync(kFullMask, v0 < count && count <= v0 + my_walked);
+        if (end_lanes != 0u) {
+            const int L = __ffs(static_cast<int>(end_lanes)) - 1;
+            const unsigned long long end_pos = win + static_cast<unsigned long long>(r);
+            s.position = __shfl_sync(kFullMask, end_pos, L);
+            s.cached = __shfl_sync(kFullMask, c ? 1 : 0, L) != 0;
+            s.cached_pair = __shfl_sync(kFullMask, lane_pair, L);
+            __syncwarp();
+            return;
+        }
+        pos += 128ull * 32ull + state % 3u;
+        cached = state >= 3u;
+        v_base += total;
+    }
+    // count == 0 never reaches here with work done; the stream is unchanged
+    s.position = pos;
+    s.cached = cached;
+    s.cached_pair = pair;
+}
+
 __device__ void CopyRegion(std::uint8_t *__restrict__ dst, const std::uint8_t *__restrict__ src, std::size_t bytes,
                            int lane) {
+
     const std::size_t n16 = bytes / 16;
     uint4 *d = reinterpret_cast<uint4 *>(dst);
     const uint4 *s = reinterpret_cast<const uint4 *>(src);
@@ -235,7 +470,7 @@ __device__ void CopyRegion(std::uint8_t *__restrict__ dst, const std::uint8_t *_
 
 // kWarps children per CTA (one warp each); the child images do not depend on it.
 template <int kWarps>
-__global__ void __launch_bounds__(kWarps * 32) BreedKernel(const BreedParams p) {
+__global__ void __launch_bounds__(kWarps * 32, 32 / kWarps) BreedKernel(const BreedParams p) {
     __shared__ EventList events[kWarps];
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
@@ -297,8 +532,16 @@ __global__ void __launch_bounds__(kWarps * 32) BreedKernel(const BreedParams p) 
 
     // ---- policy mutation (genome_ops.cuh:153-167, :301-309): skipped entirely when p <= 0 or sigma <= 0 ----
     __half *values = reinterpret_cast<__half *>(out);
+    bool windows_ok = false;
+    const std::uint32_t threshold = p.mutation_probability > 0.0f && p.mutation_probability < 1.0f
+                                        ? UniformThreshold(p.mutation_probability, windows_ok)
+                                        : 0u;
     if (p.mutation_probability > 0.0f && p.mutation_sigma > 0.0f) {
-        MutateRun(values, kPolicyHalfs, s, p.mutation_probability, p.mutation_sigma, true, ev, lane);
+        if (windows_ok && kPolicyHalfs >= kWindowRunMin) {
+            MutateRunWindows(values, kPolicyHalfs, s, threshold, p.mutation_sigma, lane);
+        } else {
+            MutateRun(values, kPolicyHalfs, s, p.mutation_probability, p.mutation_sigma, true, ev, lane);
+        }
     }
 
     // ---- tail rows (genome_ops.cuh:344-376) ----
@@ -335,7 +578,11 @@ __global__ void __launch_bounds__(kWarps * 32) BreedKernel(const BreedParams p) 
     // ---- tail mutation (genome_ops.cuh:237-257, :378-384) ----
     const bool with_normals = p.mutation_sigma > 0.0f;
     if (p.row_scale_probability <= 0.0f) {
-        MutateRun(tc, a_count * kTailDim, s, p.mutation_probability, p.mutation_sigma, with_normals, ev, lane);
+        if (windows_ok && with_normals && a_count * kTailDim >= kWindowRunMin) {
+            MutateRunWindows(tc, a_count * kTailDim, s, threshold, p.mutation_sigma, lane);
+        } else {
+            MutateRun(tc, a_count * kTailDim, s, p.mutation_probability, p.mutation_sigma, with_normals, ev, lane);
+        }
     } else {
         for (std::uint32_t row = 0; row < a_count; ++row) {
             MutateRun(tc + row * kTailDim, kTailDim, s, p.mutation_probability, p.mutation_sigma, with_normals, ev,

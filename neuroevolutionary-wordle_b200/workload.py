@@ -86,5 +86,7 @@ class Workload:
 SMALL = Workload("p64_a512_s64", 64, 8, 512, 256, 64)
 # P=4096 on 64x64, 4,739 words, 256 secrets per cell from a 2,315-word subset.
 FULL = Workload("p4096_a4739_s256", 4096, 64, 4739, 2315, 256)
+# The same per-individual work on 1,024 individuals (32x32): seven children per SM, slabs of 680 MB each.
+QUARTER = Workload("p1024_a4739_s256", 1024, 32, 4739, 2315, 256)
 # The same per-individual work on 256 individuals (16x16): a profiling case whose slab (170 MB) still exceeds L2.
 MEDIUM = Workload("p256_a4739_s256", 256, 16, 4739, 2315, 256)
