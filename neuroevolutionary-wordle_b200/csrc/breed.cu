@@ -306,7 +306,8 @@ __device__ void MutateRunWindows(__half *values, std::uint32_t count, Stream &s,
         // ---- pass 1: the window's hit mask, from 33 aligned four-output blocks ----
         std::uint32_t raw0 = 0, raw1 = 0, raw2 = 0, raw3 = 0, raw4 = 0;
         {
-            curandStatePhilox4_32_10_t state = StateAt(s, win - delta);
+            // a block boundary (the mask keeps that visible), so curand4 returns whole blocks
+            curandStatePhilox4_32_10_t state = StateAt(s, (win - delta) & ~3ull);
 #pragma unroll
             for (int b = 0; b < 33; ++b) {
                 const uint4 x = curand4(&state);
@@ -381,43 +382,56 @@ __device__ void MutateRunWindows(__half *values, std::uint32_t count, Stream &s,
         }
         const std::uint32_t total = __shfl_sync(kFullMask, inclusive, 31);
         const std::uint32_t v0 = v_base + (inclusive - my_walked);
-        // ---- pass 2: this window's hits get their normals ----
+        // ---- pass 2: this window's hits get their normals, one fresh pair and its cached second per trip ----
         const std::uint32_t limit = min(count, v0 + my_walked);
         int r = static_cast<int>(my_state % 3u);
         bool c = my_state >= 3u;
         unsigned long long lane_pair = my_pair;
-        bool have_second = false;
-        float second = 0.0f;
         std::uint32_t v = v0;
-        while (v < limit) {
-            const int h = NextHit(lo, hi, r);
+        // Advances over the misses before the next hit; false when the lane's values end first.
+        auto to_next_hit = [&](int &h) {
+            h = NextHit(lo, hi, r);
             const std::uint32_t misses = static_cast<std::uint32_t>((h < 128 ? h : 128) - r);
             if (misses >= limit - v) {
                 r += static_cast<int>(limit - v);
                 v = limit;
-                break;
+                return false;
             }
             v += misses;
-            float n;
-            if (c) {
-                if (!have_second) {
-                    second = PairNormals(s, lane_pair).y;
-                }
-                n = second;
-                have_second = false;
-                c = false;
-                r = h + 1;
-            } else {
-                lane_pair = win + static_cast<unsigned long long>(h + 1);
-                const float2 nn = PairNormals(s, lane_pair);
-                n = nn.x;
-                second = nn.y;
-                have_second = true;
-                c = true;
-                r = h + 3;
-            }
+            return true;
+        };
+        auto apply = [&](float n) {
             values[v] = __float2half(__fmaf_rn(sigma, n, __half2float(values[v])));
             ++v;
+        };
+        int h = 0;
+        if (c && v < limit && to_next_hit(h)) {  // the window's first hit takes the pair cached on entry
+            apply(PairNormals(s, lane_pair).y);
+            c = false;
+            r = h + 1;
+        }
+        while (!c && v < limit && to_next_hit(h)) {
+            // both values of the pair are found and loaded before its normals are computed
+            const std::uint32_t v1 = v;
+            const float old1 = __half2float(values[v1]);
+            ++v;
+            lane_pair = win + static_cast<unsigned long long>(h + 1);
+            c = true;
+            r = h + 3;
+            std::uint32_t v2 = 0xFFFFFFFFu;
+            float old2 = 0.0f;
+            if (v < limit && to_next_hit(h)) {
+                v2 = v;
+                old2 = __half2float(values[v2]);
+                ++v;
+                c = false;
+                r = h + 1;
+            }
+            const float2 nn = PairNormals(s, lane_pair);
+            values[v1] = __float2half(__fmaf_rn(sigma, nn.x, old1));
+            if (v2 != 0xFFFFFFFFu) {
+                values[v2] = __float2half(__fmaf_rn(sigma, nn.y, old2));
+            }
         }
         // ---- the stream state after this step ----
         const unsigned end_lanes = __ballot_sync(kFullMask, v0 < count && count <= v0 + my_walked);
@@ -468,9 +482,10 @@ __device__ void CopyRegion(std::uint8_t *__restrict__ dst, const std::uint8_t *_
     }
 }
 
-// kWarps children per CTA (one warp each); the child images do not depend on it.
+// kWarps children per CTA (one warp each); the child images do not depend on it. Four-warp CTAs hold 28 children
+// per SM at 72 registers, so 4,096 children fit in one wave of 148 SMs.
 template <int kWarps>
-__global__ void __launch_bounds__(kWarps * 32, 32 / kWarps) BreedKernel(const BreedParams p) {
+__global__ void __launch_bounds__(kWarps * 32, kWarps == 4 ? 7 : 32 / kWarps) BreedKernel(const BreedParams p) {
     __shared__ EventList events[kWarps];
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
@@ -611,14 +626,14 @@ cudaError_t LaunchBreed(const BreedParams &params, cudaStream_t stream, int warp
         return cudaErrorInvalidValue;
     }
     switch (warps_per_cta) {
-        case 4:
-            BreedKernel<4><<<(params.child_count + 3) / 4, 4 * 32, 0, stream>>>(params);
+        case 8:
+            BreedKernel<8><<<(params.child_count + 7) / 8, 8 * 32, 0, stream>>>(params);
             break;
         case 16:
             BreedKernel<16><<<(params.child_count + 15) / 16, 16 * 32, 0, stream>>>(params);
             break;
         default:
-            BreedKernel<8><<<(params.child_count + 7) / 8, 8 * 32, 0, stream>>>(params);
+            BreedKernel<4><<<(params.child_count + 3) / 4, 4 * 32, 0, stream>>>(params);
             break;
     }
     return cudaGetLastError();

@@ -107,7 +107,7 @@ struct nwg_runtime {
     std::uint64_t last_episodes = 0;
     // launch shapes: CTAs of the persistent evaluation kernels (0: scratch_ctas) and children per breeding CTA
     int eval_ctas = 0;
-    int breed_warps = 8;
+    int breed_warps = 4;
     cudaEvent_t breed_begin = nullptr;
     cudaEvent_t breed_end = nullptr;
     // graphed generations (nwg_advance_graphed) and the online launch-shape tuning per (width, form)
@@ -1681,12 +1681,12 @@ int nwg_advance_graphed(nwg_runtime *rt, uint32_t generation_seed, const nwg_run
         rt->breed_warps = tune.breed_warps;
     } else {
         rt->eval_ctas = 0;
-        rt->breed_warps = 8;
+        rt->breed_warps = 4;
     }
     auto restore = [&](int status) {
         rt->stream = caller;
         rt->eval_ctas = 0;
-        rt->breed_warps = 8;
+        rt->breed_warps = 4;
         return status;
     };
     // capture: prepare (no callbacks, so it never waits on the device) and the assembly's device work; the FP32

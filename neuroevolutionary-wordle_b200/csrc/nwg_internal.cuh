@@ -171,7 +171,7 @@ struct BreedParams {
     int *status;
     std::uint32_t child_first;  // global index of child 0: its Philox subsequence (0 for a whole population)
 };
-cudaError_t LaunchBreed(const BreedParams &params, cudaStream_t stream, int warps_per_cta = 8);
+cudaError_t LaunchBreed(const BreedParams &params, cudaStream_t stream, int warps_per_cta = 4);
 
 // ---- output-embedding injection (action-space growth) ----
 cudaError_t LaunchInject(std::uint8_t *slab, std::size_t pitch, const std::uint32_t *child_slots,
