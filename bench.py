@@ -472,6 +472,13 @@ def roofline(form: str, steps: float, encoded: float, action_count: int, kernel_
     other forms). The bound is the pipe whose share takes longest at its measured peak."""
     flops = algorithmic_flops(int(steps), int(encoded), action_count)
     trunk = 2.0 * (9472.0 * encoded + 123136.0 * steps)
+    return roofline_of(form, flops, trunk, steps, kernel_ms, pk, fp32_peak, traffic)
+
+
+def roofline_of(form: str, flops: float, trunk: float, steps: float, kernel_ms: float, pk: dict, fp32_peak: float,
+                traffic) -> dict:
+    """roofline() from the work itself: `flops` in all, `trunk` of it on the FP32 pipe in the plain and exact forms
+    (a run over several action widths sums its generations' work)."""
     scoring = flops - trunk
     t = kernel_ms * 1e-3
     kernel = {"fp32": "EvalFp32Kernel", "tc-bf16": "EvalTcKernel<bf16>", "tc-fp16": "EvalTcKernel<fp16>",
@@ -792,7 +799,7 @@ def run_ours(args) -> None:
     batching = None
     if not args.no_growth and args.workload == "full":
         # config 3 names BF16 operands for the batching form
-        batching = growth_run(nwg, torch, "tc-trunk-bf16", args.tau, 0, local)
+        batching = growth_run(nwg, torch, "tc-trunk-bf16", args.tau, 0, local, world, extras=True)
         for k in ("total_steps", "total_s"):
             batching.pop(k)
         nwg.capi.upload_catalog(catalog)
@@ -843,7 +850,8 @@ def run_ours(args) -> None:
         rt.close()
 
 
-def growth_run(nwg, torch, form: str, tau: float, rank: int = 0, local: int = 0) -> dict:
+def growth_run(nwg, torch, form: str, tau: float, rank: int = 0, local: int = 0, world: int = 1,
+               extras: bool = False, cpu: bool = False) -> dict:
     """Batching form with uneven shards (the widening run): 16,384 individuals on a 128x128 grid, per-cell secret
     lists of floor(exp(U[ln 32, ln 1024])) words drawn from the first 1,024 catalog words, and the action space
     widened from 1,024 to 4,739 words in steps of 512 (the last step 131) over 50 generations. Every generation that
@@ -851,7 +859,9 @@ def growth_run(nwg, torch, form: str, tau: float, rank: int = 0, local: int = 0)
     generation breeds into the wider slab and injects the new rows directly. As in the reference, the generation
     byte budget is fixed at creation (16,384 genomes at 1,024 words), so each widening keeps the whole grid rows
     that still fit; the surviving cells keep their secret lists. Timed on the host with the device synchronised
-    around each generation; game steps are counted on the device. Returns this rank's totals and the line fields."""
+    around each generation; game steps are counted on the device. Returns this rank's totals and the line fields;
+    with `extras`, also the evaluation kernel's roofline over the whole run, the end-to-end metric at the final
+    width (host buffers) and, with `cpu`, the reference's CPU path on the final generation."""
     W, capi = nwg.workload, nwg.capi
     population, columns, start, final, step, generations = 16384, 128, 1024, 4739, 512, 50
     widths = list(range(start + step, final, step)) + [final]
@@ -876,6 +886,8 @@ def growth_run(nwg, torch, form: str, tau: float, rank: int = 0, local: int = 0)
     width = start
     per_width = {}
     total_steps, total_s = 0, 0.0
+    work = {"flops": 0.0, "trunk": 0.0, "kernel_ms": 0.0}
+    cur_offsets, cur_words = offsets, words
     with ClockSampler(local) as clocks:
         for g in range(generations):
             counts = capi.word_counts(training=start, action_space=width)
@@ -887,9 +899,13 @@ def growth_run(nwg, torch, form: str, tau: float, rank: int = 0, local: int = 0)
             rt.advance_graphed(seed=9000 + g, counts=counts, config=cfg, pending=pending)
             torch.cuda.synchronize()
             dt = time.perf_counter() - t0
-            steps = rt.stats().game_steps
+            st = rt.stats()
+            steps = st.game_steps
             total_steps += steps
             total_s += dt
+            work["flops"] += algorithmic_flops(steps, st.encoded_turns, width)
+            work["trunk"] += 2.0 * (9472.0 * st.encoded_turns + 123136.0 * steps)
+            work["kernel_ms"] += st.eval_kernel_ms
             row = per_width.setdefault(width, {"generations": 0, "game_steps": 0, "seconds": 0.0})
             row["generations"] += 1
             row["game_steps"] += steps
@@ -897,7 +913,8 @@ def growth_run(nwg, torch, form: str, tau: float, rank: int = 0, local: int = 0)
             if pending is not None:
                 width = widen_at[g]
                 n = len(rt.current_generation()["slots"])
-                rt.set_cell_words(offsets[:n + 1], words[:offsets[n]])
+                cur_offsets, cur_words = offsets[:n + 1], words[:offsets[n]]
+                rt.set_cell_words(cur_offsets, cur_words)
     tuning = {}
     for w in per_width:
         t = rt.launch_tuning(width=w)
@@ -905,8 +922,30 @@ def growth_run(nwg, torch, form: str, tau: float, rank: int = 0, local: int = 0)
                      "eval_ms": [round(x, 3) for x in t.eval_ms], "breed_ms": [round(x, 3) for x in t.breed_ms]}
     gi = rt.graph_info()
     final_population = len(rt.current_generation()["slots"])
+    more = {}
+    if extras:
+        stream = torch.cuda.current_stream()
+        pk = peaks()
+        fp32_peak = nwg.capi.measure_fp32_peak(stream.cuda_stream)
+        pk["fp32_source"] = "measured live by nwg_measure_fp32_peak (independent FFMA chains on every SM)"
+        line_roofline = roofline_of(form, work["flops"], work["trunk"], total_steps, work["kernel_ms"], pk,
+                                    fp32_peak, None)
+        for k in ("algorithmic_flop_per_launch", "game_steps_per_launch", "fp32_pipe_flop_per_launch",
+                  "tensor_flop_per_launch", "min_ms_at_peaks"):
+            if k in line_roofline:
+                line_roofline[k] /= generations
+        line_roofline["kernel_ms_per_launch"] = work["kernel_ms"] / generations
+        line_roofline["over"] = f"all {generations} generations (every width): work and kernel time summed, " \
+                                "per-launch fields their means"
+        counts = capi.word_counts(training=start, action_space=width)
+        e2e, _ = e2e_line(rt, torch, stream, world, cur_offsets, cur_words, counts, cfg, 9000 + generations, 3)
+        e2e["at"] = f"the final width ({width} words, {final_population} individuals), ungraphed advance"
+        more = {"roofline": line_roofline, "e2e": e2e}
+        if cpu:
+            more["cpu_baseline"] = cpu_baseline_on(rt, catalog, cur_offsets, cur_words, width,
+                                                   f"widening run at its final width ({width} words)")
     rt.close()
-    return {
+    return {**more,
         "total_steps": total_steps, "total_s": total_s, "generations": generations,
         "value": total_steps / total_s, "unit": "game-steps/s", "generations_per_s": generations / total_s,
         "ms_per_generation": 1e3 * total_s / generations, "dtype": DTYPES[form],
@@ -930,7 +969,8 @@ def run_growth(args) -> None:
 
     rank, world, local = dist_setup(args.gpus)
     nwg = importlib.import_module("neuroevolutionary-wordle_b200")
-    r = growth_run(nwg, torch, args.form, args.tau, rank, local)
+    r = growth_run(nwg, torch, args.form, args.tau, rank, local, world, extras=True,
+                   cpu=rank == 0 and world == 1 and not args.no_cpu_baseline)
     value = sum_over_ranks(float(r["total_steps"]), world) / max_over_ranks(r["total_s"], world)
     if rank == 0:
         print(json.dumps({
@@ -938,6 +978,8 @@ def run_growth(args) -> None:
             "steps": r["generations"], "warmup": 0, "ms_per_step": r["ms_per_generation"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": r["dtype"], "data": "synthetic", "impl": "ours",
             "generations_per_s": r["generations_per_s"], "config": r["config"], "per_width": r["per_width"],
+            "roofline": r.get("roofline"), "cpu_baseline": r.get("cpu_baseline"), "e2e": r.get("e2e"),
+            "gpu_launches": kernel_launches(args.form) * r["generations"],
             "launch_tuning": r["launch_tuning"], "graphs": r["graphs"], "clocks": r["clocks"],
         }), flush=True)
 
