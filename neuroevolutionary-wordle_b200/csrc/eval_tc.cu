@@ -49,6 +49,11 @@ constexpr int kOffWindow = kOffKeys + 2 * kChunkGames;  // per game: best tensor
 constexpr int kOffFull = kOffWindow + kChunkGames;    // games re-scored over every action
 constexpr int kOffEnd = kOffFull + kChunkGames;
 static_assert(kOffEnd <= kArenaFloats, "scoring buffers must fit in the arena");
+// FP16 operands: the policy vectors again as contiguous [game][64] rows for the exact re-scores (the embedding
+// stages' space, free once the tile loop ends)
+constexpr int kOffPvRows = kOffEnd;
+static_assert(kOffPvRows + kChunkGames * kPolicy <= kArenaFloats, "policy rows must fit in the arena");
+static_assert((kOffPvRows * 4) % 16 == 0, "policy rows are read 16 bytes at a time");
 static_assert((kOffKeys * 4) % 8 == 0, "64-bit keys need 8-byte alignment");
 
 struct TcState {
@@ -252,6 +257,13 @@ __device__ __forceinline__ void ScoreTensorCores(const TcParams &q, ChunkState &
     }
     __syncthreads();
 
+    if constexpr (kFp16) {
+        float *pv_rows = arena + kOffPvRows;
+        for (int idx = tid; idx < kChunkGames * kPolicy; idx += kEvalThreads) {
+            pv_rows[idx] = pv[(idx & (kPolicy - 1)) * kLd + (idx >> 6)];  // game idx / 64, value idx % 64
+        }
+    }
+
     // ---- candidate chunks per game ----
     const int turns_now = t;
     if (tid < kChunkGames && !cs.done[tid]) {
@@ -359,8 +371,9 @@ __device__ __forceinline__ void ScoreTensorCores(const TcParams &q, ChunkState &
             const int g1 = static_cast<int>(task1 >> 16);
             unsigned long long key0 = 0;
             unsigned long long key1 = 0;
-            ChunkKeyPairFp16(p, cs, embed, pv + g0, g0, static_cast<int>(task0 & 0xFFFFu), pv + g1, g1,
-                             static_cast<int>(task1 & 0xFFFFu), kLd, turns_now, key0, key1);
+            const float *pv_rows = arena + kOffPvRows;
+            ChunkKeyPairFp16<1>(p, cs, embed, pv_rows + g0 * kPolicy, g0, static_cast<int>(task0 & 0xFFFFu),
+                                pv_rows + g1 * kPolicy, g1, static_cast<int>(task1 & 0xFFFFu), turns_now, key0, key1);
             FoldKeys(best_key + g0, key0);
             if (k1 < tasks) {
                 FoldKeys(best_key + g1, key1);
@@ -400,8 +413,9 @@ __device__ __forceinline__ void ScoreTensorCores(const TcParams &q, ChunkState &
                 const int c1 = c0 + kWarps;
                 unsigned long long key0 = 0;
                 unsigned long long key1 = 0;
-                ChunkKeyPairFp16(p, cs, embed, pv + g, g, c0, pv + g, g, c1 < chunks_per_row ? c1 : c0, kLd,
-                                 turns_now, key0, key1);
+                const float *row = arena + kOffPvRows + g * kPolicy;
+                ChunkKeyPairFp16<1>(p, cs, embed, row, g, c0, row, g, c1 < chunks_per_row ? c1 : c0, turns_now, key0,
+                                    key1);
                 best = key0 > best ? key0 : best;
                 best = c1 < chunks_per_row && key1 > best ? key1 : best;
             }

@@ -1548,10 +1548,10 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
                         const int f1 = static_cast<int>(task1 >> 16);
                         unsigned long long key0 = 0;
                         unsigned long long key1 = 0;
-                        ChunkKeyPairFp16(p, cs, embed, xp + f0 * kPolicy, ts.fallback_games[b0 + f0],
-                                         static_cast<int>(task0 & 0xFFFFu), xp + f1 * kPolicy,
-                                         ts.fallback_games[b0 + f1], static_cast<int>(task1 & 0xFFFFu), 1, t, key0,
-                                         key1);
+                        ChunkKeyPairFp16<1>(p, cs, embed, xp + f0 * kPolicy, ts.fallback_games[b0 + f0],
+                                            static_cast<int>(task0 & 0xFFFFu), xp + f1 * kPolicy,
+                                            ts.fallback_games[b0 + f1], static_cast<int>(task1 & 0xFFFFu), t, key0,
+                                            key1);
                         FoldKeys(fb_key + f0, key0);
                         if (k1 < n_tasks) {
                             FoldKeys(fb_key + f1, key1);
@@ -1583,8 +1583,8 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTctKernel(const TctParams
                                 const int c1 = c0 + kWarps;
                                 unsigned long long key0 = 0;
                                 unsigned long long key1 = 0;
-                                ChunkKeyPairFp16(p, cs, embed, xp + f * kPolicy, g, c0, xp + f * kPolicy, g,
-                                                 c1 < chunks_per_row ? c1 : c0, 1, t, key0, key1);
+                                ChunkKeyPairFp16<1>(p, cs, embed, xp + f * kPolicy, g, c0, xp + f * kPolicy, g,
+                                                    c1 < chunks_per_row ? c1 : c0, t, key0, key1);
                                 key = key0 > key ? key0 : key;
                                 key = c1 < chunks_per_row && key1 > key ? key1 : key;
                             }

@@ -140,12 +140,14 @@ __device__ __forceinline__ void LoadEmbedRow(const std::uint8_t *embed, std::uin
 // Exact keys of this lane's action in two (game, 32-action chunk) tasks, read from an FP16 embedding table. The
 // FP16 table holds every embedding value exactly (the fixed features are small integers, the tail rows are the
 // genome's own FP16 values), so each FP32 chain -- fma(p_k, e_k, s) for k = 0..63 in ascending order, the plain
-// form's and the reference's (output_embedding.hpp:98-119) -- gives ExactScore's bits. Both tasks' rows and codes
+// form's and the reference's (output_embedding.hpp:98-119) -- gives ExactScore's bits. kPvLd is the stride of a
+// game's policy values (1: a contiguous, 16-byte aligned row, read four values per load). Both tasks' rows and codes
 // are loaded before either chain starts, and the two chains run interleaved. key1 is computed for every lane; the
 // caller ignores it when it has no second task.
+template <int kPvLd>
 __device__ __forceinline__ void ChunkKeyPairFp16(const EvalParams &p, const ChunkState &cs, const std::uint8_t *embed,
                                                  const float *pv0, int g0, int chunk0, const float *pv1, int g1,
-                                                 int chunk1, int ld, int turns, unsigned long long &key0,
+                                                 int chunk1, int turns, unsigned long long &key0,
                                                  unsigned long long &key1) {
     const std::uint32_t lane = threadIdx.x & 31;
     const std::uint32_t a0 = static_cast<std::uint32_t>(chunk0) * 32u + lane;
@@ -164,15 +166,33 @@ __device__ __forceinline__ void ChunkKeyPairFp16(const EvalParams &p, const Chun
     for (int kg = 0; kg < 8; ++kg) {
         const std::uint32_t w0[4] = {e0[kg].x, e0[kg].y, e0[kg].z, e0[kg].w};
         const std::uint32_t w1[4] = {e1[kg].x, e1[kg].y, e1[kg].z, e1[kg].w};
+        // the policy values k = 8 kg .. 8 kg + 7 of both games: two 16-byte loads each from a contiguous row
+        float q0[8];
+        float q1[8];
+        if constexpr (kPvLd == 1) {
+            const float4 x0 = *reinterpret_cast<const float4 *>(pv0 + kg * 8);
+            const float4 y0 = *reinterpret_cast<const float4 *>(pv0 + kg * 8 + 4);
+            const float4 x1 = *reinterpret_cast<const float4 *>(pv1 + kg * 8);
+            const float4 y1 = *reinterpret_cast<const float4 *>(pv1 + kg * 8 + 4);
+            q0[0] = x0.x, q0[1] = x0.y, q0[2] = x0.z, q0[3] = x0.w, q0[4] = y0.x, q0[5] = y0.y, q0[6] = y0.z,
+            q0[7] = y0.w;
+            q1[0] = x1.x, q1[1] = x1.y, q1[2] = x1.z, q1[3] = x1.w, q1[4] = y1.x, q1[5] = y1.y, q1[6] = y1.z,
+            q1[7] = y1.w;
+        } else {
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                q0[i] = pv0[(kg * 8 + i) * kPvLd];
+                q1[i] = pv1[(kg * 8 + i) * kPvLd];
+            }
+        }
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
-            const int k = kg * 8 + 2 * i;
             const float2 f0 = __half22float2(*reinterpret_cast<const __half2 *>(&w0[i]));
             const float2 f1 = __half22float2(*reinterpret_cast<const __half2 *>(&w1[i]));
-            s0 = __fmaf_rn(pv0[k * ld], f0.x, s0);
-            s1 = __fmaf_rn(pv1[k * ld], f1.x, s1);
-            s0 = __fmaf_rn(pv0[(k + 1) * ld], f0.y, s0);
-            s1 = __fmaf_rn(pv1[(k + 1) * ld], f1.y, s1);
+            s0 = __fmaf_rn(q0[2 * i], f0.x, s0);
+            s1 = __fmaf_rn(q1[2 * i], f1.x, s1);
+            s0 = __fmaf_rn(q0[2 * i + 1], f0.y, s0);
+            s1 = __fmaf_rn(q1[2 * i + 1], f1.y, s1);
         }
     }
     bool m0 = !v0;
