@@ -115,28 +115,48 @@ __device__ __forceinline__ void EncodeRoundX(ChunkState &st, const __half *gh, c
             acc[i][j] = b;
         }
     }
+    // the hidden layer's biases of the four quarters, read while the weights stream in
+    float bias_q[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        bias_q[q] = H2F(gh, kEncB1 + q * 32 + (tid & 31));
+    }
     CopyAsyncWaitAll();
+#pragma unroll
     for (int q = 0; q < 4; ++q) {
         __syncthreads();
         // hidden[o] = relu(b1[o] + w[o][letter features] + w[o][tile features]) in ascending feature order
         const int ol = tid & 31;
         const int o = q * 32 + ol;
-        const float bias = H2F(gh, kEncB1 + o);
-        for (int g = tid >> 5; g < kChunkGames; g += kEvalThreads / 32) {
-            const std::uint32_t code = st.guess[t][g];
-            const std::uint32_t tiles = st.tiles[t][g];
-            float h = bias;
+        const float bias = bias_q[q];
+        // Four games per pass (the warp's games w, w + 8, w + 16, w + 24, then w + 32 ...): their forty weight
+        // reads are issued before any of the pass's stores, which the compiler could not move them past, and
+        // the four ten-add chains interleave.
+        constexpr int kWarps = kEvalThreads / 32;
+        for (int g0 = tid >> 5; g0 < kChunkGames; g0 += 4 * kWarps) {
+            float h[4];
 #pragma unroll
-            for (int pos = 0; pos < kWordLength; ++pos) {
-                h = __fmaf_rn(__half2float(ws[(pos * kAlphabet + WordLetter(code, pos)) * kEncoderHidden + o]), 1.0f,
-                              h);
+            for (int j = 0; j < 4; ++j) {
+                const int g = g0 + j * kWarps;
+                const std::uint32_t code = st.guess[t][g];
+                const std::uint32_t tiles = st.tiles[t][g];
+                float hj = bias;
+#pragma unroll
+                for (int pos = 0; pos < kWordLength; ++pos) {
+                    hj = __fmaf_rn(__half2float(ws[(pos * kAlphabet + WordLetter(code, pos)) * kEncoderHidden + o]),
+                                   1.0f, hj);
+                }
+#pragma unroll
+                for (int pos = 0; pos < kWordLength; ++pos) {
+                    const int f = kWordLength * kAlphabet + pos * 3 + ((tiles >> (2 * pos)) & 3);
+                    hj = __fmaf_rn(__half2float(ws[f * kEncoderHidden + o]), 1.0f, hj);
+                }
+                h[j] = hj;
             }
 #pragma unroll
-            for (int pos = 0; pos < kWordLength; ++pos) {
-                const int f = kWordLength * kAlphabet + pos * 3 + ((tiles >> (2 * pos)) & 3);
-                h = __fmaf_rn(__half2float(ws[f * kEncoderHidden + o]), 1.0f, h);
+            for (int j = 0; j < 4; ++j) {
+                ah[ol * kLd + g0 + j * kWarps] = h[j] < 0.0f ? 0.0f : h[j];
             }
-            ah[ol * kLd + g] = h < 0.0f ? 0.0f : h;
         }
         __syncthreads();
         MmaChainLd<4>(acc, ah, kLd, be + q * 32 * kEncoderOut, kEncoderOut, 32, ty, tx);
@@ -220,6 +240,12 @@ __device__ __forceinline__ void TrunkForwardX(const EvalParams &p, ChunkState &s
         CopyRowsAsync(bbuf(b), 128, w2 + kc * kXfKc * kHidden1, kHidden1, kXfKc, 128);
         CopyAsyncCommit();
     };
+    // layer 3's biases, read while layer 2 runs
+    float b3[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        b3[j] = H2F(gh, kTrB3 + tx * 4 + j);
+    }
     // ---- trunk layer 2: h1 = relu(b2 + W2 . relu(layer-1)) ----
     float acc[8][8];
 #pragma unroll
@@ -276,10 +302,9 @@ __device__ __forceinline__ void TrunkForwardX(const EvalParams &p, ChunkState &s
     float pacc[8][4];
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-        const float b = H2F(gh, kTrB3 + tx * 4 + j);
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
-            pacc[i][j] = b;
+            pacc[i][j] = b3[j];
         }
     }
     __syncthreads();
