@@ -48,6 +48,13 @@ __device__ __forceinline__ float H2F(const __half *p, int i) { return __half2flo
 __device__ __forceinline__ int RowOf(int ty, int i) { return i < 4 ? ty * 4 + i : 64 + ty * 4 + (i - 4); }
 __device__ __forceinline__ int ColOf8(int tx, int j) { return j < 4 ? tx * 4 + j : 64 + tx * 4 + (j - 4); }
 
+// A thread's eight rows RowOf(ty, 0..7) of one column (col = the column's start, 16-byte aligned) as two 16-byte
+// stores: rows 4 ty .. 4 ty + 3 and 64 + 4 ty .. 64 + 4 ty + 3.
+__device__ __forceinline__ void StoreRows8(float *col, int ty, const float (&v)[8]) {
+    *reinterpret_cast<float4 *>(col + ty * 4) = make_float4(v[0], v[1], v[2], v[3]);
+    *reinterpret_cast<float4 *>(col + 64 + ty * 4) = make_float4(v[4], v[5], v[6], v[7]);
+}
+
 // acc[i][j] = fma(A[k][row i], B[k][col j], acc[i][j]) for k = 0..K-1 in ascending order.
 template <int TN>
 __device__ __forceinline__ void MmaChain(float (&acc)[8][TN], const float *As, const float *Bs, int ldb, int K,
@@ -309,12 +316,20 @@ __device__ __forceinline__ void EncodeRound(ChunkState &st, const __half *gh, fl
     }
     __syncthreads();
     float *enc = arena;  // [64][kLd] encoded turn, k-major
+    {
+        bool live[8];
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-        const bool live = !kMaskByTurns || t < st.turns[RowOf(ty, i)];
+        for (int i = 0; i < 8; ++i) {
+            live[i] = !kMaskByTurns || t < st.turns[RowOf(ty, i)];
+        }
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-            enc[(tx * 4 + j) * kLd + RowOf(ty, i)] = live ? acc[i][j] : 0.0f;
+            float v[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                v[i] = live[i] ? acc[i][j] : 0.0f;
+            }
+            StoreRows8(enc + (tx * 4 + j) * kLd, ty, v);
         }
     }
     // trunk layer 1: chains continue with inputs 1 + 64t .. 64 + 64t
@@ -406,12 +421,13 @@ __device__ __forceinline__ void TrunkForward(const EvalParams &p, ChunkState &st
     __syncthreads();
     float *h1 = arena;  // [128][kLd]
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
+    for (int j = 0; j < 8; ++j) {
+        float v[8];
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            const float v = acc[i][j];
-            h1[ColOf8(tx, j) * kLd + RowOf(ty, i)] = v < 0.0f ? 0.0f : v;
+        for (int i = 0; i < 8; ++i) {
+            v[i] = acc[i][j] < 0.0f ? 0.0f : acc[i][j];
         }
+        StoreRows8(h1 + ColOf8(tx, j) * kLd, ty, v);
     }
 
     // ---- trunk layer 3: policy = b3 + W3 . h1 ----
@@ -438,11 +454,13 @@ __device__ __forceinline__ void TrunkForward(const EvalParams &p, ChunkState &st
     __syncthreads();
     float *pv = arena;  // [64][kLd] policy vectors, k-major
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
+    for (int j = 0; j < 4; ++j) {
+        float v[8];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            pv[(tx * 4 + j) * kLd + RowOf(ty, i)] = pacc[i][j];
+        for (int i = 0; i < 8; ++i) {
+            v[i] = pacc[i][j];
         }
+        StoreRows8(pv + (tx * 4 + j) * kLd, ty, v);
     }
     __syncthreads();
     if (p.trace_policy != nullptr) {

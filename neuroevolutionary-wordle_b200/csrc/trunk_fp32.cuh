@@ -170,12 +170,20 @@ __device__ __forceinline__ void EncodeRoundX(ChunkState &st, const __half *gh, c
     CopyRowsAsync(arena + kXeB1, 128, w1 + 128, kHidden0, kEncoderOut, 128);
     CopyAsyncCommit();
     float *enc = arena + kXeEnc;  // [64][kLd] encoded turn, k-major
+    {
+        bool live[8];
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-        const bool live = !kMaskByTurns || t < st.turns[RowOf(ty, i)];
+        for (int i = 0; i < 8; ++i) {
+            live[i] = !kMaskByTurns || t < st.turns[RowOf(ty, i)];
+        }
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-            enc[(tx * 4 + j) * kLd + RowOf(ty, i)] = live ? acc[i][j] : 0.0f;
+            float v[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                v[i] = live[i] ? acc[i][j] : 0.0f;
+            }
+            StoreRows8(enc + (tx * 4 + j) * kLd, ty, v);
         }
     }
     for (int nh = 0; nh < 2; ++nh) {
@@ -291,12 +299,13 @@ __device__ __forceinline__ void TrunkForwardX(const EvalParams &p, ChunkState &s
     __syncthreads();
     float *h1 = arena;  // [128][kLd]
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
+    for (int j = 0; j < 8; ++j) {
+        float v[8];
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            const float v = acc[i][j];
-            h1[ColOf8(tx, j) * kLd + RowOf(ty, i)] = v < 0.0f ? 0.0f : v;
+        for (int i = 0; i < 8; ++i) {
+            v[i] = acc[i][j] < 0.0f ? 0.0f : acc[i][j];
         }
+        StoreRows8(h1 + ColOf8(tx, j) * kLd, ty, v);
     }
     // ---- trunk layer 3: policy = b3 + W3 . h1 ----
     float pacc[8][4];
@@ -312,11 +321,13 @@ __device__ __forceinline__ void TrunkForwardX(const EvalParams &p, ChunkState &s
     __syncthreads();
     float *pv = arena;  // [64][kLd] policy vectors, k-major
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
+    for (int j = 0; j < 4; ++j) {
+        float v[8];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            pv[(tx * 4 + j) * kLd + RowOf(ty, i)] = pacc[i][j];
+        for (int i = 0; i < 8; ++i) {
+            v[i] = pacc[i][j];
         }
+        StoreRows8(pv + (tx * 4 + j) * kLd, ty, v);
     }
     __syncthreads();
     if (p.trace_policy != nullptr) {
