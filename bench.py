@@ -1024,6 +1024,7 @@ def run_reference(args) -> None:
             steps_total += int(steps.sum())
     total_s = sum(times)
     value = steps_total / total_s
+    generation = cpu_generation_small(O, wl, catalog, offsets, words, threads) if args.workload == "small" else None
     print(json.dumps({
         "metric": "game-steps/s", "value": value, "unit": "game-steps/s", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * total_s / args.steps, "higher_is_better": True,
@@ -1036,7 +1037,70 @@ def run_reference(args) -> None:
                          "kind": "reference",
                          "sample": f"{sample} individuals per step, {steps_total} game steps timed"},
         "e2e": {"value": value, "unit": "game-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "cpu_generation": generation,
     }), flush=True)
+
+
+def cpu_generation_small(O, wl, catalog, offsets, words, threads: int) -> dict | None:
+    """One whole generation of the 64-individual configuration on the host cores: the reference's CPU evaluation of
+    every individual (libref_host, every host thread), then cellular rank selection and breeding of the 64 children
+    by the oracle's single-thread restatement (the reference has no host selection or breeding). The Philox draws
+    those two steps consume are recorded on the GPU by the generator itself beforehand (oracle/nwg_tape.cu) and are
+    not part of the host time."""
+    try:
+        import torch
+    except ImportError:
+        return None
+    if not torch.cuda.is_available():
+        return None
+    try:
+        tl = O.tape_lib()
+    except OSError:
+        return None
+    n, cols = wl.population, wl.columns
+    rows = n // cols
+    halfs = O.genome_halfs(wl.action_count)
+    rng = np.random.default_rng(5)
+    genomes = (rng.standard_normal((n, halfs)).astype(np.float32) * 0.05).astype(np.float16).view(np.uint16)
+    seed, gen_index, radius, exponent = 77, 1, wl.radius, 0.5
+    cfg = {"l1": 0.02, "l2": 0.01, "l3": 0.005, "p": wl.mutation_probability, "sigma": wl.mutation_sigma}
+    draws = torch.zeros(6 * n, dtype=torch.int32, device="cuda")
+    weights = torch.zeros(32, dtype=torch.float32, device="cuda")
+    assert tl.tape_selection_draws(seed, gen_index, n, draws.data_ptr()) == 1
+    assert tl.tape_pow_table(exponent, 32, weights.data_ptr()) == 1
+    d = draws.cpu().numpy().view(np.uint32).reshape(n, 6)
+    w = weights.cpu().numpy()
+    O.set_fma_mode(True)
+    t0 = time.perf_counter()
+    raw_fit, steps, _ = O.ref_host_evaluate(genomes, wl.action_count, catalog, offsets, words,
+                                            np.arange(n, dtype=np.uint32), threads)
+    t1 = time.perf_counter()
+    fitness = np.array([O.normalize_fitness(float(r), wl.secrets_per_cell) for r in raw_fit], np.float32)
+    pairs = [O.select_parent_pair(fitness, np.ones(n, np.uint8), rows, cols, rows, c, radius, d[c], w)
+             for c in range(n)]
+    t2 = time.perf_counter()
+    # each child's draws are recorded on the GPU just before its host breeding, which alone is timed
+    length = 3 * halfs + 64
+    raw = torch.zeros(length, dtype=torch.int32, device="cuda")
+    uni = torch.zeros(length, dtype=torch.float32, device="cuda")
+    nrm = torch.zeros(2 * length, dtype=torch.float32, device="cuda")
+    breed_s = 0.0
+    for c, (a, b) in enumerate(pairs):
+        assert tl.tape_positions(seed, (c + gen_index * 4099) & 0xFFFFFFFF, length, raw.data_ptr(), uni.data_ptr(),
+                                 nrm.data_ptr()) == 1
+        tape = dict(raw=raw.cpu().numpy().view(np.uint32), uniform=uni.cpu().numpy(), normal_pair=nrm.cpu().numpy())
+        tb = time.perf_counter()
+        child = O.breed_and_mutate(genomes[a], genomes[b], wl.action_count, tape, cfg)
+        breed_s += time.perf_counter() - tb
+        if child is None:
+            return None
+    total = (t2 - t0) + breed_s
+    t3 = t2 + breed_s
+    return {"generations_per_s": 1.0 / total, "seconds": total, "evaluate_s": t1 - t0, "select_s": t2 - t1,
+            "breed_s": t3 - t2, "game_steps": int(steps.sum()), "cores_evaluate": threads, "cores_select_breed": 1,
+            "what": f"{n} individuals on {rows}x{cols}, {wl.action_count} words, {wl.secrets_per_cell} secrets per "
+                    "cell: evaluation by the reference's host code, selection and breeding by the oracle's "
+                    "restatement from Philox draws recorded on the GPU beforehand (not timed)"}
 
 
 def launch_ranks(args) -> None:
