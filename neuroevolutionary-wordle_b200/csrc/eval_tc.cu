@@ -6,8 +6,9 @@
 //   2. the individual's embedding table, kept as a 16-bit copy in the tensor-core layout
 //      (BuildTcTablesKernel), streams through shared memory 128 actions at a time by bulk copies;
 //   3. tcgen05.mma (M = 128 games, N = 128 actions, K = 64) fills two TMEM accumulators in turn; all eight warps
-//      read a buffer back (tcgen05.ld) and keep, per game, the four largest 32-action chunk maxima, and the last
-//      warp to read a buffer refills its stage and issues the tile two ahead into it;
+//      read a buffer back (tcgen05.ld) and keep, per game, the four largest 32-action chunk maxima; the first warp
+//      to see a tile's MMAs complete refills its stage, and the last warp to read its buffer issues the tile two
+//      ahead into it;
 //   4. every chunk whose maximum lies within 2 * eps of the best chunk free of guessed words is re-scored
 //      in FP32 with the plain form's own fused-multiply-add chain, and the game's guess is the exact FP32
 //      argmax (ties to the lower index, guessed words masked).
@@ -62,6 +63,7 @@ struct TcState {
     std::uint64_t mbar_drain[kEvalThreads / 32];  // wind-down after a failure: each warp's MMAs have completed
     unsigned int loads_issued[kStages];  // bulk copies issued on each stage barrier (one per phase)
     std::uint32_t readers[2];            // warps that have read each accumulator buffer (8 per tile)
+    std::uint32_t waiters[2];            // warps that have seen each buffer's MMAs complete (8 per tile)
     int task_count;
     int full_count;
     std::uint32_t tmem_base;
@@ -181,10 +183,11 @@ __device__ __forceinline__ void ScoreTensorCores(const TcParams &q, ChunkState &
     umma::FenceProxyAsyncShared();
     __syncthreads();
 
-    // No block barrier inside the tile loop. Thread 0 issues tiles 0 and 1; after that, the last warp to read tile
-    // k's accumulator buffer (an arrival counter per buffer) refills tile k's embedding stage with tile k + kStages
-    // and issues tile k + 2 into the buffer it has just released, while the other warps read the other buffer. The
-    // stage parities advance alike in every thread, tile by tile.
+    // No block barrier inside the tile loop. Thread 0 issues tiles 0 and 1; after that, the first warp to see tile
+    // k's MMAs complete (an arrival counter per buffer) refills tile k's embedding stage with tile k + kStages, and
+    // the last warp to read tile k's accumulator buffer (a second counter) issues tile k + 2 into the buffer it has
+    // just released, while the other warps read the other buffer. The stage parities advance alike in every thread,
+    // tile by tile.
     for (int tile = 0; tile < 2 && tile < n_tiles; ++tile) {
         if (tid == 0) {
             wait_stage_and_issue(tile);
@@ -212,6 +215,14 @@ __device__ __forceinline__ void ScoreTensorCores(const TcParams &q, ChunkState &
             umma::Load64(ts.tmem_base + static_cast<std::uint32_t>(buf * kTileN + half * 64) +
                              (static_cast<std::uint32_t>(quadrant * 32) << 16),
                          v);
+            if (lane == 0) {
+                // the first warp to see tile's MMAs complete refills its embedding stage, a whole epilogue earlier
+                // than the buffer's last reader could
+                const std::uint32_t prior = atomicAdd(&ts.waiters[buf], 1u);
+                if ((prior & 7u) == 0u && acc_ok && tile + kStages < n_tiles) {
+                    issue_load(tile % kStages, tile + kStages);
+                }
+            }
             if (tile + 1 == n_tiles) {
 #pragma unroll
                 for (int j = 0; j < 64; ++j) {
@@ -234,13 +245,8 @@ __device__ __forceinline__ void ScoreTensorCores(const TcParams &q, ChunkState &
                          : "=r"(prior)
                          : "r"(umma::SmemAddress(&ts.readers[buf])), "r"(1u)
                          : "memory");
-            if ((prior & 7u) == 7u && acc_ok) {  // every warp has read tile's buffer; tile's MMAs have completed
-                if (tile + kStages < n_tiles) {
-                    issue_load(tile % kStages, tile + kStages);
-                }
-                if (tile + 2 < n_tiles) {
-                    wait_stage_and_issue(tile + 2);
-                }
+            if ((prior & 7u) == 7u && acc_ok && tile + 2 < n_tiles) {  // every warp has read tile's buffer
+                wait_stage_and_issue(tile + 2);
             }
         }
         if (tile + 2 < n_tiles) {
@@ -475,6 +481,8 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTcKernel(const TcParams q
         }
         ts.readers[0] = 0;
         ts.readers[1] = 0;
+        ts.waiters[0] = 0;
+        ts.waiters[1] = 0;
         ts.failed = 0;
     }
     umma::FenceBeforeSync();
