@@ -7,15 +7,16 @@
 //      in the reference's order (genome_ops.cuh:264-299, :344-376);
 //   2. the donor layers and tail rows are copied with coalesced 128-bit loads and stores, then the
 //      single-neuron / single-row / splice overrides are applied;
-//   3. the per-value mutation stream (genome_ops.cuh:153-167, :237-257) is walked 128 draw positions
-//      at a time: each lane computes four consecutive uniforms, a ballot finds the hits, the hit list
-//      is resolved in order (a fresh normal pair consumes two more draw positions and leaves its
-//      second value cached for the next hit, as the generator's normal does), and the lanes then apply
-//      the hits' normals in parallel, 32 queued hits at a time (each value's load issued before its normal
-//      is computed, so the read of the child image overlaps the generator's arithmetic).
+//   3. the per-value mutation stream (genome_ops.cuh:153-167, :237-257): a fresh normal pair consumes two
+//      more draw positions and leaves its second value cached for the next hit, as the generator's normal
+//      does. Runs of at least 4,096 values take the window-parallel walk (MutateRunWindows: every lane owns
+//      a 128-position window, 32 windows per step); shorter runs, mutation without normals and p >= 1 take
+//      the serial walk (MutateRun: 128 positions at a time for the whole warp, the hit list resolved in
+//      order, the normals applied 32 queued hits at a time).
 // Every uniform, 32-bit draw and normal is produced by the toolkit generator itself (curand_init at the
-// draw's position, then curand_uniform / curand / curand_normal), so the child image is bit-identical
-// to the reference's serial walk.
+// draw's position, then curand4 / curand_uniform / curand / curand_normal; a hit test compares the 32-bit
+// draw with the threshold curand_uniform maps to p), so the child image is bit-identical to the
+// reference's serial walk.
 #include <cuda_fp16.h>
 #include <curand_kernel.h>
 
