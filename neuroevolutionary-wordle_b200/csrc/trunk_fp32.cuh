@@ -228,7 +228,9 @@ constexpr int kXfA1 = kXfA0 + kXfKc * 128;
 constexpr int kXfB0 = kXfA1 + kXfKc * 128;
 constexpr int kXfB1 = kXfB0 + kXfKc * 128;
 constexpr int kXfW3 = kHidden1 * kLd;  // after h1 ([128][kLd])
+constexpr int kXfVirgin = kXfB1 + kXfKc * 128;  // [256] layer-1 outputs with no turn, between B1 and W3
 static_assert(kXfB1 + kXfKc * 128 <= kXfW3 && kXfW3 + kHidden1 * kPolicy <= kArenaFloats, "trunk arena");
+static_assert(kXfVirgin + kHidden0 <= kXfW3, "the no-turn layer-1 outputs fit before W3");
 
 // TrunkForward with streamed weights (same chains, same order): leaves the FP32 policy vectors in arena[0 .. kTile)
 // as [64 k][kLd games] and records them in the trace when one is requested.
@@ -266,6 +268,15 @@ __device__ __forceinline__ void TrunkForwardX(const EvalParams &p, ChunkState &s
     }
     CopyRowsAsync(arena + kXfW3, kPolicy, reinterpret_cast<const float *>(xt + kXtW3), kPolicy, kHidden1, kPolicy);
     issue(0, 0);
+    // no turn on the board: every game's layer-1 output is relu(b1 + W1[:, 0]), one value per output
+    float *virgin = arena + kXfVirgin;
+    if (t == 0) {
+        for (int o = tid; o < kHidden0; o += kEvalThreads) {
+            const float v = __fmaf_rn(H2F(gh, kTrW1 + o * kModelInput), 1.0f, H2F(gh, kTrB1 + o));
+            virgin[o] = v < 0.0f ? 0.0f : v;
+        }
+        __syncthreads();
+    }
     constexpr int kChunks = kHidden0 / kXfKc;
     for (int kc = 0; kc < kChunks; ++kc) {
         const int b = kc & 1;
@@ -281,13 +292,10 @@ __device__ __forceinline__ void TrunkForwardX(const EvalParams &p, ChunkState &s
                 x.w = x.w < 0.0f ? 0.0f : x.w;
                 *v = x;
             }
-        } else {  // no turn on the board: every game's layer-1 output is relu(b1 + W1[:, 0])
+        } else {
             for (int idx = tid; idx < kXfKc * kChunkGames; idx += kEvalThreads) {
                 const int k = idx >> 7;
-                const int g = idx & 127;
-                const int o = kc * kXfKc + k;
-                const float v = __fmaf_rn(H2F(gh, kTrW1 + o * kModelInput), 1.0f, H2F(gh, kTrB1 + o));
-                abuf(b)[k * 128 + g] = v < 0.0f ? 0.0f : v;
+                abuf(b)[k * 128 + (idx & 127)] = virgin[kc * kXfKc + k];
             }
         }
         __syncthreads();
