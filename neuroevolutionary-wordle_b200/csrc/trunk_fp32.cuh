@@ -115,47 +115,57 @@ __device__ __forceinline__ void EncodeRoundX(ChunkState &st, const __half *gh, c
             acc[i][j] = b;
         }
     }
-    // the hidden layer's biases of the four quarters, read while the weights stream in
-    float bias_q[4];
+    // Each lane owns two adjacent hidden outputs of a quarter (one 4-byte read of W_e1 gives both) and a half-warp
+    // one game, so a warp gathers two games at a time. Their biases are read while the weights stream in.
+    const int pair = tid & 15;
+    const int half_warp = (tid >> 4) & 1;
+    float bias_q[4][2];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-        bias_q[q] = H2F(gh, kEncB1 + q * 32 + (tid & 31));
+        bias_q[q][0] = H2F(gh, kEncB1 + q * 32 + 2 * pair);
+        bias_q[q][1] = H2F(gh, kEncB1 + q * 32 + 2 * pair + 1);
     }
     CopyAsyncWaitAll();
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
         __syncthreads();
         // hidden[o] = relu(b1[o] + w[o][letter features] + w[o][tile features]) in ascending feature order
-        const int ol = tid & 31;
-        const int o = q * 32 + ol;
-        const float bias = bias_q[q];
-        // Four games per pass (the warp's games w, w + 8, w + 16, w + 24, then w + 32 ...): their forty weight
-        // reads are issued before any of the pass's stores, which the compiler could not move them past, and
-        // the four ten-add chains interleave.
+        const int o0 = q * 32 + 2 * pair;
+        // Four games per pass (games 2 w + half, then + 16, + 32, + 48; then + 64 ...): their weight reads are
+        // issued before any of the pass's stores, which the compiler could not move them past, and the eight
+        // ten-add chains interleave.
         constexpr int kWarps = kEvalThreads / 32;
-        for (int g0 = tid >> 5; g0 < kChunkGames; g0 += 4 * kWarps) {
-            float h[4];
+        for (int g0 = 2 * (tid >> 5) + half_warp; g0 < kChunkGames; g0 += 8 * kWarps) {
+            float h[4][2];
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
-                const int g = g0 + j * kWarps;
+                const int g = g0 + j * 2 * kWarps;
                 const std::uint32_t code = st.guess[t][g];
                 const std::uint32_t tiles = st.tiles[t][g];
-                float hj = bias;
+                float h0 = bias_q[q][0];
+                float h1 = bias_q[q][1];
 #pragma unroll
                 for (int pos = 0; pos < kWordLength; ++pos) {
-                    hj = __fmaf_rn(__half2float(ws[(pos * kAlphabet + WordLetter(code, pos)) * kEncoderHidden + o]),
-                                   1.0f, hj);
+                    const int f = pos * kAlphabet + static_cast<int>(WordLetter(code, pos));
+                    const float2 w = __half22float2(*reinterpret_cast<const __half2 *>(ws + f * kEncoderHidden + o0));
+                    h0 = __fmaf_rn(w.x, 1.0f, h0);
+                    h1 = __fmaf_rn(w.y, 1.0f, h1);
                 }
 #pragma unroll
                 for (int pos = 0; pos < kWordLength; ++pos) {
                     const int f = kWordLength * kAlphabet + pos * 3 + ((tiles >> (2 * pos)) & 3);
-                    hj = __fmaf_rn(__half2float(ws[f * kEncoderHidden + o]), 1.0f, hj);
+                    const float2 w = __half22float2(*reinterpret_cast<const __half2 *>(ws + f * kEncoderHidden + o0));
+                    h0 = __fmaf_rn(w.x, 1.0f, h0);
+                    h1 = __fmaf_rn(w.y, 1.0f, h1);
                 }
-                h[j] = hj;
+                h[j][0] = h0;
+                h[j][1] = h1;
             }
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
-                ah[ol * kLd + g0 + j * kWarps] = h[j] < 0.0f ? 0.0f : h[j];
+                const int g = g0 + j * 2 * kWarps;
+                ah[(2 * pair) * kLd + g] = h[j][0] < 0.0f ? 0.0f : h[j][0];
+                ah[(2 * pair + 1) * kLd + g] = h[j][1] < 0.0f ? 0.0f : h[j][1];
             }
         }
         __syncthreads();
