@@ -83,6 +83,10 @@ BREED_CASES = {
     "every_value": dict(l1=0.0, l2=0.0, l3=0.0, p=1.0, sigma=0.02, row_scale=0.0),
     "no_sigma": dict(l1=0.3, l2=0.3, l3=0.3, p=0.2, sigma=0.0, row_scale=1.0),
     "no_mutation": dict(l1=0.1, l2=0.1, l3=1.0, p=0.0, sigma=0.02, row_scale=0.0),
+    # the window-parallel walk at its extremes: almost every position a hit (fresh pairs straddling nearly every
+    # window edge), and hits so rare that most 4,096-position steps have none
+    "dense_hits": dict(l1=0.02, l2=0.01, l3=0.005, p=0.9, sigma=0.02, row_scale=0.0),
+    "sparse_hits": dict(l1=0.02, l2=0.01, l3=0.005, p=2e-6, sigma=0.02, row_scale=0.0),
 }
 
 
