@@ -466,10 +466,11 @@ def kernel_launches(form: str) -> int:
 
 def roofline(form: str, steps: float, encoded: float, action_count: int, kernel_ms: float, pk: dict,
              fp32_peak: float, traffic) -> dict:
-    """The evaluation kernel against its bound. The per-step work is SURVEY 8(d)'s 2 * (E_new + 123,136 + 64 A)
-    FLOP: the encoder and trunk share (2 * (9,472 per encoded turn + 123,136 per step)) runs as FP32 FFMA chains in
-    the plain and exact forms, the scoring share (2 * 64 A per step) on CUDA cores (plain) or on tensor cores (the
-    other forms). The bound is the pipe whose share takes longest at its measured peak."""
+    """The evaluation kernel against its bound. The per-step work is 2 * (E_new + 123,136 + 64 A) FLOP (E_new =
+    9,472 per newly encoded turn): the encoder and trunk share (2 * (9,472 per encoded turn + 123,136 per step))
+    runs as FP32 FFMA chains in the plain and exact forms, the scoring share (2 * 64 A per step) on CUDA cores
+    (plain) or on tensor cores (the other forms). The bound is the pipe whose share takes longest at its measured
+    peak."""
     flops = algorithmic_flops(int(steps), int(encoded), action_count)
     trunk = 2.0 * (9472.0 * encoded + 123136.0 * steps)
     return roofline_of(form, flops, trunk, steps, kernel_ms, pk, fp32_peak, traffic)
