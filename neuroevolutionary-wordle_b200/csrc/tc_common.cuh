@@ -205,12 +205,13 @@ __device__ __forceinline__ void ChunkKeyPairFp16(const EvalParams &p, const Chun
     key1 = m1 ? 0ull : PackKey(s1, a1);
 }
 
-// Folds a warp's keys (the masked argmax) into *best_key.
+// Folds a warp's keys (the masked argmax) into *best_key: the warp's largest 64-bit key as two 32-bit maximum
+// reductions, the high words first, then the low words of the lanes that hold that high word.
 __device__ __forceinline__ void FoldKeys(unsigned long long *best_key, unsigned long long key) {
-    for (int off = 16; off > 0; off >>= 1) {
-        const unsigned long long other = __shfl_xor_sync(0xffffffffu, key, off);
-        key = other > key ? other : key;
-    }
+    const std::uint32_t hi = static_cast<std::uint32_t>(key >> 32);
+    const std::uint32_t top = __reduce_max_sync(0xffffffffu, hi);
+    const std::uint32_t lo = __reduce_max_sync(0xffffffffu, hi == top ? static_cast<std::uint32_t>(key) : 0u);
+    key = (static_cast<unsigned long long>(top) << 32) | lo;
     if ((threadIdx.x & 31) == 0 && key != 0) {
         atomicMax(best_key, key);
     }
