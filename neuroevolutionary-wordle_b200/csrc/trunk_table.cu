@@ -4,8 +4,9 @@
 // Every weight matrix is stored as [input][output] (the order the register-tiled FP32 micro-kernel reads B in), the
 // trunk's layer-1 weights split into its five 64-input turn slots (inputs 1 + 64u .. 64 + 64u; input 0, the virgin
 // flag, stays in the genome). The values are the genome's FP16 values converted to FP32 exactly (W_e1 stays FP16:
-// the encoder only gathers from it). Each CTA transposes 32 x 32 blocks through shared memory: rows of the genome
-// are read contiguously, rows of the table written contiguously.
+// the encoder only gathers from it). Each CTA transposes one 64 x 64 block through shared memory: rows of the
+// genome are read contiguously (the genome's rows have odd lengths, so two bytes at a time), rows of the table
+// written contiguously, 16 bytes per thread for the FP32 matrices.
 #include <cuda_fp16.h>
 
 #include "trunk_fp32.cuh"
@@ -41,14 +42,16 @@ __device__ __forceinline__ XtJob JobOf(int j) {
     return {kTrW3, kHidden1, kHidden1, kPolicy, kXtW3, 0};
 }
 
-// 32 x 32 blocks of each job in job order: W_e1 5 x 4, W_e2 4 x 2, five W1 slots 2 x 8 each, W2 8 x 4, W3 4 x 2.
+// 64 x 64 blocks of each job in job order: W_e1 3 x 2, W_e2 2 x 1, five W1 slots 1 x 4 each, W2 4 x 2, W3 2 x 1.
 constexpr int kXtJobs = 9;
-constexpr int kXtBlocks = 20 + 8 + 5 * 16 + 32 + 8;
+constexpr int kXtBlock = 64;
+constexpr int kXtBlocks = 6 + 2 + 5 * 4 + 8 + 2;
 
 __global__ void __launch_bounds__(256) BuildExactTrunkTablesKernel(const std::uint8_t *slab, std::size_t pitch,
                                                                    const std::uint32_t *slots, std::uint8_t *tables,
                                                                    std::size_t table_pitch) {
-    __shared__ float tile[32][33];
+    constexpr int kTileLd = kXtBlock + 1;
+    __shared__ float tile[kXtBlock * kTileLd];  // [output n][input k]
     const std::uint32_t ind = blockIdx.y;
     const __half *gh = reinterpret_cast<const __half *>(slab + static_cast<std::size_t>(slots[ind]) * pitch);
     std::uint8_t *table = tables + static_cast<std::size_t>(ind) * table_pitch;
@@ -57,30 +60,45 @@ __global__ void __launch_bounds__(256) BuildExactTrunkTablesKernel(const std::ui
     XtJob job = JobOf(0);
     for (; j < kXtJobs; ++j) {
         job = JobOf(j);
-        const int blocks = ((job.K + 31) / 32) * (job.N / 32);
+        const int blocks = ((job.K + kXtBlock - 1) / kXtBlock) * (job.N / kXtBlock);
         if (b < blocks) {
             break;
         }
         b -= blocks;
     }
-    const int kb = (b / (job.N / 32)) * 32;
-    const int nb = (b % (job.N / 32)) * 32;
-    for (int e = threadIdx.x; e < 32 * 32; e += blockDim.x) {
-        const int n = e >> 5;
-        const int k = e & 31;
-        tile[n][k] = kb + k < job.K ? __half2float(gh[job.src + (nb + n) * job.ld + kb + k]) : 0.0f;
+    const int kb = (b / (job.N / kXtBlock)) * kXtBlock;
+    const int nb = (b % (job.N / kXtBlock)) * kXtBlock;
+    const int rows = job.K - kb < kXtBlock ? job.K - kb : kXtBlock;  // inputs of this block
+    // every load of the block is issued before the first shared-memory store
+    float v[kXtBlock * kXtBlock / 256];
+#pragma unroll
+    for (int i = 0; i < kXtBlock * kXtBlock / 256; ++i) {
+        const int e = static_cast<int>(threadIdx.x) + i * 256;
+        const int n = e >> 6;
+        const int k = e & (kXtBlock - 1);
+        v[i] = k < rows ? __half2float(gh[job.src + (nb + n) * job.ld + kb + k]) : 0.0f;
+    }
+#pragma unroll
+    for (int i = 0; i < kXtBlock * kXtBlock / 256; ++i) {
+        const int e = static_cast<int>(threadIdx.x) + i * 256;
+        tile[(e >> 6) * kTileLd + (e & (kXtBlock - 1))] = v[i];
     }
     __syncthreads();
-    for (int e = threadIdx.x; e < 32 * 32; e += blockDim.x) {
-        const int k = e >> 5;
-        const int n = e & 31;
-        if (kb + k < job.K) {
-            const std::size_t idx = static_cast<std::size_t>(kb + k) * job.N + nb + n;
-            if (job.fp16) {
-                reinterpret_cast<__half *>(table + job.dst)[idx] = __float2half_rn(tile[n][k]);
-            } else {
-                reinterpret_cast<float *>(table + job.dst)[idx] = tile[n][k];
-            }
+    if (job.fp16) {
+        __half *out = reinterpret_cast<__half *>(table + job.dst);
+        for (int e = static_cast<int>(threadIdx.x); e < rows * kXtBlock; e += 256) {
+            const int k = e >> 6;
+            const int n = e & (kXtBlock - 1);
+            out[static_cast<std::size_t>(kb + k) * job.N + nb + n] = __float2half_rn(tile[n * kTileLd + k]);
+        }
+    } else {
+        float *out = reinterpret_cast<float *>(table + job.dst);
+        for (int e = static_cast<int>(threadIdx.x); e < rows * (kXtBlock / 4); e += 256) {
+            const int k = e >> 4;
+            const int n = (e & 15) * 4;
+            const float4 w = make_float4(tile[n * kTileLd + k], tile[(n + 1) * kTileLd + k],
+                                         tile[(n + 2) * kTileLd + k], tile[(n + 3) * kTileLd + k]);
+            *reinterpret_cast<float4 *>(out + static_cast<std::size_t>(kb + k) * job.N + nb + n) = w;
         }
     }
 }
