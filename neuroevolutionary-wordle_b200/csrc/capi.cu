@@ -613,7 +613,7 @@ int EvaluateImpl(nwg_runtime *rt, const nwg_runtime_word_counts *counts, const n
         rt->last_table_pitch = TcTablePitch(static_cast<std::uint32_t>(selectable));
         NWG_TRY(LaunchBuildTcTables(rt->slab, rt->pitch, rt->cur_slots, population, g_catalog.fixed_t,
                                     static_cast<std::uint32_t>(g_catalog.pad), static_cast<std::uint32_t>(selectable),
-                                    rt->tc_tables, fp16, rt->stream));
+                                    rt->tc_tables, fp16, true, rt->stream));
         NWG_TRY(LaunchBuildTrunkTables(rt->slab, rt->pitch, rt->cur_slots, population, rt->trunk_tables, fp16,
                                        rt->stream));
         NWG_TRY(RecordEvent(rt->eval_begin, rt->stream));
@@ -628,7 +628,7 @@ int EvaluateImpl(nwg_runtime *rt, const nwg_runtime_word_counts *counts, const n
         rt->last_table_pitch = TcTablePitch(static_cast<std::uint32_t>(selectable));
         NWG_TRY(LaunchBuildTcTables(rt->slab, rt->pitch, rt->cur_slots, population, g_catalog.fixed_t,
                                     static_cast<std::uint32_t>(g_catalog.pad), static_cast<std::uint32_t>(selectable),
-                                    rt->tc_tables, fp16, rt->stream));
+                                    rt->tc_tables, fp16, false, rt->stream));
         NWG_TRY(RecordEvent(rt->eval_begin, rt->stream));
         NWG_TRY(LaunchEvalTc(p, rt->tc_tables, TcTablePitch(static_cast<std::uint32_t>(selectable)), kappa, fp16,
                              rt->steps + 3, EvalGrid(rt), rt->stream, rt->wait_limit));

@@ -567,15 +567,16 @@ __global__ void __launch_bounds__(kEvalThreads, 2) EvalTcKernel(const TcParams q
 // fill whole 128-byte lines. The values also go to shared memory ([action][65], conflict-free both ways), where
 // thread (column, quarter) sums its quarter of the tile's actions (values and their squares, each operation
 // rounded on its own) in ascending order; the quarters are then combined in a fixed order, so every run gets the
-// same bits.
-template <bool kFp16>
-__global__ void __launch_bounds__(256) BuildTcTablesKernel(const std::uint8_t *slab, std::size_t pitch,
+// same bits. kMoments false (the scoring form, which reads no moments) skips them: each thread keeps the maxima of
+// its 32 columns in registers, and a warp and then the CTA reduce them once at the end (a maximum is order-free).
+template <bool kFp16, bool kMoments>
+__global__ void __launch_bounds__(256, kMoments ? 4 : 3) BuildTcTablesKernel(const std::uint8_t *slab, std::size_t pitch,
                                                            const std::uint32_t *slots, const float *fixed_t,
                                                            std::uint32_t action_pad, std::uint32_t action_count,
                                                            std::uint32_t tiles, std::uint8_t *tables,
                                                            std::size_t table_pitch) {
     constexpr int kLd = kPolicy + 1;
-    __shared__ float vals[kTileN * kLd];
+    __shared__ float vals[kMoments ? kTileN * kLd : 1];
     __shared__ float2 part_sum[4][kPolicy];
     __shared__ float part_max[4][kPolicy];
     const std::uint32_t ind = blockIdx.x;
@@ -588,6 +589,11 @@ __global__ void __launch_bounds__(256) BuildTcTablesKernel(const std::uint8_t *s
     const int col = t & (kPolicy - 1);
     const int quarter = t >> 6;  // actions 32 quarter .. 32 quarter + 31 of the tile
     float run_max = 0.0f;
+    float col_max[32];  // without moments: this thread's columns 32 part + j over its actions
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+        col_max[j] = 0.0f;
+    }
     for (std::uint32_t tile = 0; tile < tiles; ++tile) {
         const std::uint32_t a = tile * kTileN + static_cast<std::uint32_t>(a_local);
         const bool valid = a < action_count;
@@ -634,6 +640,13 @@ __global__ void __launch_bounds__(256) BuildTcTablesKernel(const std::uint8_t *s
             *reinterpret_cast<uint4 *>(out + umma::TileOffset(a_local, part * 32 + 8 * s, kPolicy)) =
                 make_uint4(w[0], w[1], w[2], w[3]);
         }
+        if constexpr (!kMoments) {
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+                col_max[j] = fmaxf(col_max[j], fabsf(v[j]));
+            }
+            continue;
+        }
 #pragma unroll
         for (int j = 0; j < 32; ++j) {
             vals[a_local * kLd + part * 32 + j] = v[j];
@@ -655,7 +668,27 @@ __global__ void __launch_bounds__(256) BuildTcTablesKernel(const std::uint8_t *s
                             ((part_sum[0][t].y + part_sum[1][t].y) + part_sum[2][t].y) + part_sum[3][t].y);
         }
     }
-    part_max[quarter][col] = run_max;
+    if constexpr (!kMoments) {
+        // warp maxima of each column (the warp's 32 actions share `part`), then the four warps of each part
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+            float m = col_max[j];
+#pragma unroll
+            for (int d = 16; d > 0; d >>= 1) {
+                m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, d));
+            }
+            col_max[j] = m;
+        }
+        const int w = (t >> 5) & 3;  // the warp within its part
+        if ((t & 31) == 0) {
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+                part_max[w][part * 32 + j] = col_max[j];
+            }
+        }
+    } else {
+        part_max[quarter][col] = run_max;
+    }
     __syncthreads();
     if (t < kPolicy) {
         reinterpret_cast<float *>(table)[t] =
@@ -672,18 +705,25 @@ std::size_t TcTablePitch(std::uint32_t action_count) {
 
 cudaError_t LaunchBuildTcTables(const std::uint8_t *slab, std::size_t pitch, const std::uint32_t *slots,
                                 std::uint32_t population, const float *fixed_t, std::uint32_t action_pad,
-                                std::uint32_t action_count, std::uint8_t *tables, bool fp16, cudaStream_t stream) {
+                                std::uint32_t action_count, std::uint8_t *tables, bool fp16, bool with_moments,
+                                cudaStream_t stream) {
     if (population == 0) {
         return cudaSuccess;
     }
     const std::size_t table_pitch = TcTablePitch(action_count);
     const std::uint32_t tiles = (action_count + kTileN - 1) / kTileN;
-    if (fp16) {
-        BuildTcTablesKernel<true><<<population, 256, 0, stream>>>(slab, pitch, slots, fixed_t, action_pad,
-                                                                  action_count, tiles, tables, table_pitch);
+    if (fp16 && with_moments) {
+        BuildTcTablesKernel<true, true><<<population, 256, 0, stream>>>(slab, pitch, slots, fixed_t, action_pad,
+                                                                        action_count, tiles, tables, table_pitch);
+    } else if (fp16) {
+        BuildTcTablesKernel<true, false><<<population, 256, 0, stream>>>(slab, pitch, slots, fixed_t, action_pad,
+                                                                         action_count, tiles, tables, table_pitch);
+    } else if (with_moments) {
+        BuildTcTablesKernel<false, true><<<population, 256, 0, stream>>>(slab, pitch, slots, fixed_t, action_pad,
+                                                                         action_count, tiles, tables, table_pitch);
     } else {
-        BuildTcTablesKernel<false><<<population, 256, 0, stream>>>(slab, pitch, slots, fixed_t, action_pad,
-                                                                   action_count, tiles, tables, table_pitch);
+        BuildTcTablesKernel<false, false><<<population, 256, 0, stream>>>(slab, pitch, slots, fixed_t, action_pad,
+                                                                          action_count, tiles, tables, table_pitch);
     }
     return cudaGetLastError();
 }

@@ -108,7 +108,8 @@ cudaError_t LaunchBuildExactTrunkTables(const std::uint8_t *slab, std::size_t pi
 std::size_t TcTablePitch(std::uint32_t action_count);
 cudaError_t LaunchBuildTcTables(const std::uint8_t *slab, std::size_t pitch, const std::uint32_t *slots,
                                 std::uint32_t population, const float *fixed_t, std::uint32_t action_pad,
-                                std::uint32_t action_count, std::uint8_t *tables, bool fp16, cudaStream_t stream);
+                                std::uint32_t action_count, std::uint8_t *tables, bool fp16, bool with_moments,
+                                cudaStream_t stream);
 // Polls of a bounded mbarrier wait in the tensor-core evaluation kernels before it gives up with NWG_TIMEOUT.
 constexpr std::uint32_t kDefaultWaitLimit = 1u << 26;
 cudaError_t LaunchEvalTc(const EvalParams &params, const std::uint8_t *tables, std::size_t table_pitch, float kappa,

@@ -4,7 +4,8 @@ Per individual: the header (max |e_ak| over the selectable actions, per column),
 letter-count features from the catalog, -1 for an absent letter, then the genome's 38 tail values) rounded to
 FP16 or BF16 in the K-major core-matrix layout with zero rows past the last action, and per 128-action tile the
 column sums and sums of squares: each quarter of 32 actions summed in ascending order in float32 with every
-operation rounded on its own, then the quarters added left to right.
+operation rounded on its own, then the quarters added left to right. The scoring forms (1/2) read no moments and
+their build skips them, so for those forms the header and the embedding tiles are compared.
 """
 import numpy as np
 import pytest
@@ -79,8 +80,9 @@ def test_score_table_matches_restatement(form, action_count, selectable):
     counts = G.nwg.capi.word_counts(training=selectable, action_space=selectable)
     rt.evaluate(counts)
     slots = rt.current_generation()["slots"]
+    compared = 256 + (selectable + 127) // 128 * 16384 if form in (1, 2) else None
     for i in range(population):
         got = rt.score_table(i)
         want = _expected(rt.download_slot(int(slots[i])), catalog, selectable, KIND[form])
-        assert got.tobytes() == want, f"individual {i}"
+        assert got.tobytes()[:compared] == want[:compared], f"individual {i}"
     rt.close()
