@@ -645,27 +645,27 @@ __global__ void __launch_bounds__(256, kMoments ? 4 : 3) BuildTcTablesKernel(con
             for (int j = 0; j < 32; ++j) {
                 col_max[j] = fmaxf(col_max[j], fabsf(v[j]));
             }
-            continue;
-        }
+        } else {
 #pragma unroll
-        for (int j = 0; j < 32; ++j) {
-            vals[a_local * kLd + part * 32 + j] = v[j];
-        }
-        __syncthreads();
-        float sum = 0.0f;
-        float sum_sq = 0.0f;
-        for (int i = 0; i < 32; ++i) {
-            const float x = vals[(quarter * 32 + i) * kLd + col];
-            sum = __fadd_rn(sum, x);
-            sum_sq = __fadd_rn(sum_sq, __fmul_rn(x, x));
-            run_max = fmaxf(run_max, fabsf(x));
-        }
-        part_sum[quarter][col] = make_float2(sum, sum_sq);
-        __syncthreads();
-        if (t < kPolicy) {
-            moments[tile * kPolicy + t] =
-                make_float2(((part_sum[0][t].x + part_sum[1][t].x) + part_sum[2][t].x) + part_sum[3][t].x,
-                            ((part_sum[0][t].y + part_sum[1][t].y) + part_sum[2][t].y) + part_sum[3][t].y);
+            for (int j = 0; j < 32; ++j) {
+                vals[a_local * kLd + part * 32 + j] = v[j];
+            }
+            __syncthreads();
+            float sum = 0.0f;
+            float sum_sq = 0.0f;
+            for (int i = 0; i < 32; ++i) {
+                const float x = vals[(quarter * 32 + i) * kLd + col];
+                sum = __fadd_rn(sum, x);
+                sum_sq = __fadd_rn(sum_sq, __fmul_rn(x, x));
+                run_max = fmaxf(run_max, fabsf(x));
+            }
+            part_sum[quarter][col] = make_float2(sum, sum_sq);
+            __syncthreads();
+            if (t < kPolicy) {
+                moments[tile * kPolicy + t] =
+                    make_float2(((part_sum[0][t].x + part_sum[1][t].x) + part_sum[2][t].x) + part_sum[3][t].x,
+                                ((part_sum[0][t].y + part_sum[1][t].y) + part_sum[2][t].y) + part_sum[3][t].y);
+            }
         }
     }
     if constexpr (!kMoments) {
